@@ -1,0 +1,241 @@
+/*
+ * kds.h -- C ABI of the B200-native KD-SLAM registration path (libkds.so).
+ *
+ * This library replaces, for one CUDA device, the reference's registration hot path:
+ * surfel KD-tree build, greedy nearest-surfel descent, symmetric surfel-to-surfel ICP,
+ * continuous-time CT-ICP with per-leaf deskew, and the Gauss-Newton H,b reduction and
+ * solve.  Each entry point names the reference interface it stands in for (paths are
+ * relative to the reference project, kd/ = kd_slam2/src/lib/kd_slam/).
+ *
+ * Conventions
+ *  - Every function returns an int status (KDS_OK = 0, negative on error); none exits
+ *    the process (the reference's CUDA_CHECK calls exit(), kd/cuda/cuda_common.h:30-35).
+ *  - Poses are 3x4 row-major [R | t] (12 doubles), world <- body, as Eigen::Isometry3.
+ *  - Velocities are [v_x v_y v_z w_x w_y w_z] (decoupled body velocity, kd/cticp/cticp_.h:135-138).
+ *  - `stream` arguments take a cudaStream_t; NULL selects the per-thread default stream.
+ *  - Handles are not thread-safe; distinct handles may be used from distinct threads.
+ *  - The caller owns trees; aligners hold non-owning references to them
+ *    (kd/icp/tree_aligner_base_.h:49-50) and own their device workspaces.
+ */
+#ifndef KDS_H
+#define KDS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  KDS_OK = 0,
+  KDS_ERR_INVALID_ARG = -1,
+  KDS_ERR_CUDA = -2,
+  KDS_ERR_OOM = -3,
+  KDS_ERR_TREE_REJECTED = -4, /* makeTree returned nullptr: too few points or good leaves */
+  KDS_ERR_RANGE = -5,         /* coordinate or timestamp outside the supported range */
+  KDS_ERR_BAD_TREE = -6,      /* malformed node array */
+  KDS_ERR_STATE = -7,         /* aligner used without fixed/moving tree */
+  KDS_ERR_TIMEOUT = -8,       /* a bounded device-side wait gave up */
+  KDS_ERR_ADMISSION = -9,     /* server refused a request (memory budget) */
+  KDS_ERR_NO_DEVICE = -10,
+  KDS_ERR_CAPACITY = -11      /* a fixed-size buffer is too small for the request */
+};
+
+enum { KDS_ICP = 0, KDS_CTICP = 1 };
+enum { KDS_MEM_HOST = 0, KDS_MEM_DEVICE = 1 };
+
+typedef struct kds_tree kds_tree;
+typedef struct kds_aligner kds_aligner;
+
+/* Human-readable text of the last error on the calling thread. */
+const char* kds_last_error(void);
+
+/* Replaces lib/kd_slam_cuda_init.cu:3-6 (cudaSetDeviceFlags in a .so constructor):
+ * selects the device and, if blocking_sync != 0, sets cudaDeviceScheduleBlockingSync
+ * before the context exists.  Optional; first use of any entry point initialises. */
+int kds_init(int32_t device, int32_t blocking_sync);
+
+/* ------------------------------------------------------------------------------
+ * Tree
+ * ------------------------------------------------------------------------------ */
+
+/* TreeGenerator_ PARAMs (kd/tree/tree_generator_.h:18-25), same names and defaults. */
+typedef struct {
+  int32_t propagate_normal;         /* false */
+  int32_t tree_min_good_leaves;     /* 10 */
+  int32_t leaf_min_points;          /* 5 */
+  int32_t leaf_max_points;          /* 30 */
+  float leaf_density;               /* 100 */
+  float leaf_min_normal_incidence;  /* 0.1 */
+  float leaf_eigenvalue_threshold;  /* 1e-3 (read but unused, as in the reference) */
+  float leaf_normal_eigenratio;     /* 0.1 */
+  float prune_min_normal_incidence; /* 0.1: IsGoodLeafPredicate_ default, kd/tree/tree_predicates_.h:15 */
+  int32_t max_level;                /* 48: depth cap (the reference has none) */
+} kds_tree_params;
+
+void kds_tree_params_default(kds_tree_params* p);
+
+typedef struct {
+  int64_t num_nodes;
+  int64_t num_leaves;
+  int64_t num_points;
+  int64_t num_unpruned;
+  double ts_start; /* Tree_::_ts_start */
+  int32_t accepted;
+  int32_t depth;
+} kds_tree_info;
+
+/* Replaces TreeGenerator_::makeTree (kd/tree/tree_generator_impl_.h:7-19) and the
+ * TreeCPU_ build + prune + BFS relabel it runs (kd/tree/tree_cpu_.h:61-90,172-207),
+ * built on the GPU.  xyz: n*3 floats, stamps: n doubles or NULL (all zero).
+ * mem: KDS_MEM_HOST (copied to the device inside) or KDS_MEM_DEVICE.
+ * Returns KDS_ERR_TREE_REJECTED (and *out = NULL) where makeTree returns nullptr. */
+int kds_tree_build(const float* xyz, const double* stamps, int64_t n, int32_t mem, const kds_tree_params* p,
+                   void* stream, kds_tree** out);
+
+/* Replaces Tree_CUDAfromCPU_ (kd/tree/tree_cuda_impl_.h:197-222): uploads a node
+ * array in the Node_ field order (kd/tree/node_.h:33-43), BFS numbered, node 0 the
+ * root.  dts_mean/dts_cov/start/end may be NULL.  Leaves = nodes with no children. */
+int kds_tree_import(const float* mean, const float* dir, const double* dts_mean, const double* dts_cov,
+                    const int64_t* idx_start, const int64_t* idx_end, const int32_t* left, const int32_t* right,
+                    int64_t num_nodes, double ts_start, kds_tree** out);
+
+int kds_tree_get_info(const kds_tree* t, kds_tree_info* info);
+
+/* Device-to-host copy of the tree (any pointer may be NULL).  leaves: num_leaves node
+ * indices (Tree_::_leaves_indices_ptr); perm: num_points input indices in final order. */
+int kds_tree_export(const kds_tree* t, float* mean, float* dir, double* dts_mean, double* dts_cov, int64_t* idx_start,
+                    int64_t* idx_end, int32_t* left, int32_t* right, int32_t* level, int64_t* leaves, int64_t* perm);
+
+/* Replaces TreeCUDA_::applyVelocitiesInPlace / applyIsometryInPlace
+ * (kd/tree/tree_cuda_impl_.h:132-173): per-node morph mean <- R(w dts) mean + v dts,
+ * dir <- R dir, or a rigid transform of every node. */
+int kds_tree_apply_velocities(kds_tree* t, const float v[6], int32_t skip_leaves, void* stream);
+int kds_tree_apply_isometry(kds_tree* t, const float X[12], void* stream);
+
+/* Replaces TreeCUDA_::extractCompressedLeaves (kd/tree/tree_cuda_impl_.h:42-112):
+ * writes [mean, dir] per leaf (6 floats), optionally morphed by v (may be NULL). */
+int kds_tree_extract_compressed_leaves(const kds_tree* t, const float* v6, float* out, void* stream);
+
+void kds_tree_free(kds_tree* t);
+
+/* ------------------------------------------------------------------------------
+ * Aligners: ICPB2003D / CTICPB2003D (in place of ICPCUDA3D / CTICPCUDA3D)
+ * ------------------------------------------------------------------------------ */
+
+/* TreeAlignerBase_ PARAMs (kd/icp/tree_aligner_base_.h:39-47), CTICP_ velocity_damping
+ * (kd/cticp/cticp_.h:61) and ICPTerminationCriteriaScore_ (kd/icp/icp_stats_.h:84-102). */
+typedef struct {
+  float kernel_threshold;        /* 0.1 */
+  float damping;                 /* 1 */
+  float max_error;               /* 1 */
+  float min_normal_cos;          /* cos(25 deg) */
+  int32_t min_good_measurements; /* 10 */
+  int32_t max_iterations;        /* 20 */
+  float velocity_damping;        /* 100 (CT only) */
+  int32_t term_crit;             /* 0: none (nullptr), 1: ICPTerminationCriteriaScore */
+  float d_pert;                  /* 1e-3 */
+  float d_score;                 /* 1e-3 */
+} kds_aligner_params;
+
+void kds_aligner_params_default(kds_aligner_params* p);
+
+/* ICPStats_ (kd/icp/icp_stats_.h:10-21), same field order. */
+typedef struct {
+  int32_t num_inliers, num_outliers, num_bad, num_err_normal, num_err_fn;
+  float chi2, chi2_kernelized, pert_pose_norm, pert_vel_norm;
+} kds_stats;
+
+int kds_aligner_create(int32_t type, const kds_aligner_params* p, kds_aligner** out);
+int kds_aligner_set_params(kds_aligner* a, const kds_aligner_params* p);
+int kds_aligner_set_stream(kds_aligner* a, void* stream);
+/* setFixed / setMoving (kd/icp/tree_aligner_base_.h:52-53): non-owning. */
+int kds_aligner_set_fixed(kds_aligner* a, const kds_tree* fixed);
+int kds_aligner_set_moving(kds_aligner* a, const kds_tree* moving);
+/* setX/getX/setFixedX (:87-89), setVelocities/velocities/resetMovingState (:93-95). */
+int kds_aligner_set_x(kds_aligner* a, const double X[12]);
+int kds_aligner_get_x(const kds_aligner* a, double X[12]);
+int kds_aligner_set_fixed_x(kds_aligner* a, const double X[12]);
+int kds_aligner_set_velocities(kds_aligner* a, const double v[6]);
+int kds_aligner_get_velocities(const kds_aligner* a, double v[6]);
+int kds_aligner_set_fixed_velocities(kds_aligner* a, const double v[6]);
+int kds_aligner_reset_moving_state(kds_aligner* a);
+/* setPosePrior (:127-133); info all-zero disables the prior. */
+int kds_aligner_set_pose_prior(kds_aligner* a, const double X_ref[12], const double Z[12], const double info[36]);
+/* _fixed_forest / makeFixedEntry (:57-76,136): with entries present, oneRound sums
+ * H,b,stats over them (kd/icp/icp_impl_.h:55-71). */
+int kds_aligner_add_fixed_entry(kds_aligner* a, const kds_tree* fixed, const double X[12]);
+int kds_aligner_clear_fixed_forest(kds_aligner* a);
+
+/* compute (kd/icp/tree_aligner_base_.h:100-115): the whole Gauss-Newton loop runs on
+ * the device (one kernel per iteration, one host sync at the end).  *result is the
+ * reference's return value: -i on a failed round i, i on early termination, else
+ * max_iterations. */
+int kds_aligner_compute(kds_aligner* a, int32_t stats_mode, int32_t* result);
+/* oneRound (kd/icp/icp_impl_.h:52-90, kd/cticp/cticp_impl_.h:47-92); *ok = 0/1. */
+int kds_aligner_one_round(kds_aligner* a, int32_t stats_mode, int32_t* ok);
+/* buildQuadraticForm (kd/icp/icp_impl_.h:23-27) and, for CT, buildQuadraticFormDual
+ * (kd/cticp/cticp_impl_.h:41-45): H, b and stats at the current state, no update. */
+int kds_aligner_build_quadratic_form(kds_aligner* a, int32_t stats_mode);
+int kds_aligner_build_quadratic_form_dual(kds_aligner* a, int32_t stats_mode);
+/* Public fields H, b, dx (D = 6 for ICP, 12 for CT; row-major D*D). */
+int kds_aligner_get_hb(const kds_aligner* a, double* H, double* b, double* dx);
+/* H_dual_vel_B, b_dual_vel_B, H_dual_cross_pose_vel_B, H_dual_cross_vel_AB
+ * (kd/cticp/cticp_.h:183-186), row-major 6x6 / 6. */
+int kds_aligner_get_dual(const kds_aligner* a, double H_vel_B[36], double b_vel_B[6], double H_cross_pose_vel_B[36],
+                         double H_cross_vel_AB[36]);
+/* getPoseHessian (ICP: H; CT: Schur complement, kd/cticp/cticp_.h:169-177). */
+int kds_aligner_get_pose_hessian(const kds_aligner* a, double H6[36]);
+int kds_aligner_get_stats(const kds_aligner* a, kds_stats* s);
+/* stats_log of the last compute (kd/icp/tree_aligner_base_.h:135). */
+int kds_aligner_get_stats_log(const kds_aligner* a, kds_stats* log, int32_t cap, int32_t* n);
+/* One linearization at explicit float caches (Xm, Xf, Xmf: 3x 12 floats) and
+ * velocities: per-leaf fixed-leaf index (-1 when the descent ends at a pruned child)
+ * and status (0 inlier, 1 outlier, 2 bad, 3 err_normal, 4 err_fn), plus H, b, stats.
+ * Exposes quadraticTerm's correspondences for parity checks. */
+int kds_aligner_linearize_debug(kds_aligner* a, const float caches[36], const float v[6], const float fixed_v[6],
+                                int32_t kind, int32_t stats_mode, int32_t* match, int32_t* status, double* H,
+                                double* b, kds_stats* stats);
+void kds_aligner_free(kds_aligner* a);
+
+/* ------------------------------------------------------------------------------
+ * Batched alignment: many independent (moving, fixed) pairs in one launch per
+ * Gauss-Newton iteration -- the multi-view bundle-adjustment linearisations
+ * (MultiViewICPFactor_::compute, kd/map/multiview_icp_factor_impl_.h:10-62) and
+ * whole alignments of uneven sizes.
+ * ------------------------------------------------------------------------------ */
+enum { KDS_JOB_COMPUTE = 0, KDS_JOB_LINEARIZE = 1, KDS_JOB_LINEARIZE_DUAL = 2 };
+
+typedef struct {
+  int32_t type;   /* KDS_ICP / KDS_CTICP */
+  int32_t mode;   /* KDS_JOB_* */
+  int32_t stats_mode;
+  int32_t pad_;
+  const kds_tree* fixed;
+  const kds_tree* moving;
+  kds_aligner_params params;
+  double X[12];        /* in: initial guess; out: estimate */
+  double fixed_X[12];
+  double v[6];         /* in/out (CT) */
+  double fixed_v[6];
+  /* outputs */
+  int32_t result;
+  int32_t iterations;
+  kds_stats stats;
+  double H[144];       /* D*D, D = 6 or 12 */
+  double b[12];
+  double H_vel_B[36], b_vel_B[6], H_cross_pose_vel_B[36], H_cross_vel_AB[36]; /* dual */
+} kds_job;
+
+typedef struct kds_batch kds_batch;
+int kds_batch_create(kds_batch** out);
+/* Runs all jobs; with use_graph != 0 the launches are captured once into a CUDA
+ * graph and replayed while the job set keeps its shape. */
+int kds_batch_run(kds_batch* b, kds_job* jobs, int32_t num_jobs, int32_t use_graph, void* stream);
+void kds_batch_free(kds_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KDS_H */

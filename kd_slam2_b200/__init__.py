@@ -1,0 +1,412 @@
+"""B200-native KD-SLAM registration path: Python mirror of the reference's aligner API.
+
+The classes here wrap the C ABI of libkds.so (include/kds.h) and follow the method and
+parameter names of the reference types they stand in for:
+
+  TreeGeneratorB2003D  ~ TreeGenerator3D   (kd/tree/tree_generator_.h:10-47)
+  ICPB2003D            ~ ICPCUDA3D / ICPCPU3D   (kd/icp/tree_aligner_base_.h:25-161)
+  CTICPB2003D          ~ CTICPCUDA3D / CTICPCPU3D (kd/cticp/cticp_.h:20-261)
+
+Poses are 3x4 numpy arrays [R | t] (world <- body); velocities are [v; w].
+All compute runs on the GPU; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import abi as L
+from .abi import KdsError
+
+class _Lazy:
+    """Loads libkds.so on first use, so that `python -m kd_slam2_b200.build` can run
+    before the library exists.  A missing library raises ImportError at that point."""
+
+    def __getattr__(self, name):
+        real = L.load()
+        globals()["_lib"] = real
+        return getattr(real, name)
+
+
+_lib = _Lazy()
+
+
+def lib():
+    """The loaded libkds.so (ctypes.CDLL)."""
+    global _lib
+    if isinstance(_lib, _Lazy):
+        _lib = L.load()
+    return _lib
+
+
+def _check(rc: int, where: str) -> None:
+    if rc != L.KDS_OK:
+        raise KdsError(rc, where, (_lib.kds_last_error() or b"").decode())
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data
+
+
+def _pose12(X) -> np.ndarray:
+    X = np.asarray(X, dtype=np.float64)
+    if X.shape == (4, 4):
+        X = X[:3]
+    return np.ascontiguousarray(X.reshape(12))
+
+
+def identity() -> np.ndarray:
+    X = np.zeros((3, 4))
+    X[:, :3] = np.eye(3)
+    return X
+
+
+def init(device: int = 0, blocking_sync: bool = False) -> None:
+    _check(_lib.kds_init(device, 1 if blocking_sync else 0), "kds_init")
+
+
+# ---------------------------------------------------------------------------- trees
+class Tree:
+    """A surfel KD-tree resident on the GPU (Tree_ / TreeCUDA_, kd/tree/tree_.h:15-56)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def __del__(self):
+        self.free()
+
+    def free(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.kds_tree_free(self._h)
+            self._h = C.c_void_p(None)
+
+    @property
+    def info(self) -> L.TreeInfo:
+        inf = L.TreeInfo()
+        _check(_lib.kds_tree_get_info(self._h, C.byref(inf)), "kds_tree_get_info")
+        return inf
+
+    @property
+    def num_nodes(self) -> int:
+        return self.info.num_nodes
+
+    @property
+    def num_leaves(self) -> int:
+        return self.info.num_leaves
+
+    def export(self) -> dict:
+        inf = self.info
+        n, nl, npnt = inf.num_nodes, inf.num_leaves, inf.num_points
+        out = {
+            "mean": np.zeros((n, 3), np.float32), "dir": np.zeros((n, 3), np.float32),
+            "dts_mean": np.zeros(n), "dts_cov": np.zeros(n),
+            "start": np.zeros(n, np.int64), "end": np.zeros(n, np.int64),
+            "left": np.zeros(n, np.int32), "right": np.zeros(n, np.int32), "level": np.zeros(n, np.int32),
+            "leaves": np.zeros(nl, np.int64), "perm": np.zeros(npnt, np.int64),
+        }
+        _check(_lib.kds_tree_export(self._h, *(out[k].ctypes.data for k in (
+            "mean", "dir", "dts_mean", "dts_cov", "start", "end", "left", "right", "level", "leaves")),
+            out["perm"].ctypes.data if npnt else None), "kds_tree_export")
+        out["ts_start"] = inf.ts_start
+        return out
+
+    @staticmethod
+    def import_nodes(mean, dir, left, right, dts_mean=None, dts_cov=None, start=None, end=None,
+                     ts_start: float = 0.0) -> "Tree":
+        """Tree_CUDAfromCPU_: uploads a BFS-ordered node array (Node_ fields)."""
+        mean = np.ascontiguousarray(mean, np.float32)
+        dir = np.ascontiguousarray(dir, np.float32)
+        left = np.ascontiguousarray(left, np.int32)
+        right = np.ascontiguousarray(right, np.int32)
+        dm = None if dts_mean is None else np.ascontiguousarray(dts_mean, np.float64)
+        dc = None if dts_cov is None else np.ascontiguousarray(dts_cov, np.float64)
+        s0 = None if start is None else np.ascontiguousarray(start, np.int64)
+        e0 = None if end is None else np.ascontiguousarray(end, np.int64)
+        h = C.c_void_p()
+        _check(_lib.kds_tree_import(mean.ctypes.data, dir.ctypes.data, _ptr(dm), _ptr(dc), _ptr(s0), _ptr(e0),
+                                    left.ctypes.data, right.ctypes.data, len(mean), ts_start, C.byref(h)),
+               "kds_tree_import")
+        return Tree(h.value)
+
+    def apply_velocities_in_place(self, v, skip_leaves: bool = False) -> None:
+        vv = np.ascontiguousarray(v, np.float32)
+        _check(_lib.kds_tree_apply_velocities(self._h, vv.ctypes.data, 1 if skip_leaves else 0, None),
+               "kds_tree_apply_velocities")
+
+    def apply_isometry_in_place(self, X) -> None:
+        XX = np.ascontiguousarray(_pose12(X), np.float32)
+        _check(_lib.kds_tree_apply_isometry(self._h, XX.ctypes.data, None), "kds_tree_apply_isometry")
+
+    def extract_compressed_leaves(self, v=None) -> np.ndarray:
+        out = np.zeros((self.num_leaves, 6), np.float32)
+        vv = None if v is None else np.ascontiguousarray(v, np.float32)
+        _check(_lib.kds_tree_extract_compressed_leaves(self._h, _ptr(vv), out.ctypes.data, None),
+               "kds_tree_extract_compressed_leaves")
+        return out
+
+
+class TreeGeneratorB2003D:
+    """TreeGenerator3D with the same PARAM names and defaults; builds on the GPU."""
+
+    def __init__(self, **params):
+        self.params = L.TreeParams()
+        _lib.kds_tree_params_default(C.byref(self.params))
+        for k, v in params.items():
+            if not hasattr(self.params, k):
+                raise AttributeError(f"TreeGeneratorB2003D has no parameter {k}")
+            setattr(self.params, k, v)
+
+    def make_tree(self, xyz, stamps=None, device: bool = False, stream=None) -> Tree | None:
+        """makeTree: returns None where the reference returns nullptr."""
+        if device:
+            n = int(xyz.shape[0])
+            px, ps, mem = int(xyz.data_ptr()), (int(stamps.data_ptr()) if stamps is not None else None), L.KDS_MEM_DEVICE
+        else:
+            xyz = np.ascontiguousarray(xyz, np.float32)
+            st = None if stamps is None else np.ascontiguousarray(stamps, np.float64)
+            n, px, ps, mem = len(xyz), xyz.ctypes.data, _ptr(st), L.KDS_MEM_HOST
+        h = C.c_void_p()
+        rc = _lib.kds_tree_build(px, ps, n, mem, C.byref(self.params), stream, C.byref(h))
+        if rc == L.KDS_ERR_TREE_REJECTED:
+            return None
+        _check(rc, "kds_tree_build")
+        return Tree(h.value)
+
+
+# ---------------------------------------------------------------------------- aligners
+class _AlignerBase:
+    TYPE = L.KDS_ICP
+    D = 6
+
+    def __init__(self, **params):
+        self.params = L.AlignerParams()
+        _lib.kds_aligner_params_default(C.byref(self.params))
+        for k, v in params.items():
+            self.set_param(k, v)
+        h = C.c_void_p()
+        _check(_lib.kds_aligner_create(self.TYPE, C.byref(self.params), C.byref(h)), "kds_aligner_create")
+        self._h = h
+        self._keep = []
+        self.stats_log: list[dict] = []
+
+    def set_param(self, k, v):
+        if k == "term_crit" and isinstance(v, dict):
+            self.params.term_crit = 1
+            self.params.d_pert = v.get("d_pert", 1e-3)
+            self.params.d_score = v.get("d_score", 1e-3)
+            return
+        if not hasattr(self.params, k):
+            raise AttributeError(f"{type(self).__name__} has no parameter {k}")
+        setattr(self.params, k, v)
+        if getattr(self, "_h", None) is not None:
+            _check(_lib.kds_aligner_set_params(self._h, C.byref(self.params)), "kds_aligner_set_params")
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.kds_aligner_free(self._h)
+            self._h = C.c_void_p(None)
+
+    def set_fixed(self, t: Tree) -> None:
+        self._fixed = t
+        _check(_lib.kds_aligner_set_fixed(self._h, t.handle), "kds_aligner_set_fixed")
+
+    def set_moving(self, t: Tree) -> None:
+        self._moving = t
+        _check(_lib.kds_aligner_set_moving(self._h, t.handle), "kds_aligner_set_moving")
+
+    def set_x(self, X) -> None:
+        _check(_lib.kds_aligner_set_x(self._h, _pose12(X).ctypes.data), "kds_aligner_set_x")
+
+    def get_x(self) -> np.ndarray:
+        X = np.zeros(12)
+        _check(_lib.kds_aligner_get_x(self._h, X.ctypes.data), "kds_aligner_get_x")
+        return X.reshape(3, 4)
+
+    def set_fixed_x(self, X) -> None:
+        _check(_lib.kds_aligner_set_fixed_x(self._h, _pose12(X).ctypes.data), "kds_aligner_set_fixed_x")
+
+    def set_velocities(self, v) -> None:
+        vv = np.ascontiguousarray(v, np.float64)
+        _check(_lib.kds_aligner_set_velocities(self._h, vv.ctypes.data), "kds_aligner_set_velocities")
+
+    def velocities(self) -> np.ndarray:
+        v = np.zeros(6)
+        _check(_lib.kds_aligner_get_velocities(self._h, v.ctypes.data), "kds_aligner_get_velocities")
+        return v
+
+    def set_fixed_velocities(self, v) -> None:
+        vv = np.ascontiguousarray(v, np.float64)
+        _check(_lib.kds_aligner_set_fixed_velocities(self._h, vv.ctypes.data), "kds_aligner_set_fixed_velocities")
+
+    def reset_moving_state(self) -> None:
+        _check(_lib.kds_aligner_reset_moving_state(self._h), "kds_aligner_reset_moving_state")
+
+    def set_pose_prior(self, X_ref=None, Z=None, info=None) -> None:
+        X_ref = identity() if X_ref is None else X_ref
+        Z = identity() if Z is None else Z
+        info = np.zeros((6, 6)) if info is None else np.asarray(info, np.float64)
+        inf = np.ascontiguousarray(info.reshape(36))
+        _check(_lib.kds_aligner_set_pose_prior(self._h, _pose12(X_ref).ctypes.data, _pose12(Z).ctypes.data,
+                                               inf.ctypes.data), "kds_aligner_set_pose_prior")
+
+    def add_fixed_entry(self, t: Tree, X) -> None:
+        """makeFixedEntry + _fixed_forest insertion."""
+        self._keep.append(t)
+        _check(_lib.kds_aligner_add_fixed_entry(self._h, t.handle, _pose12(X).ctypes.data),
+               "kds_aligner_add_fixed_entry")
+
+    def clear_fixed_forest(self) -> None:
+        self._keep.clear()
+        _check(_lib.kds_aligner_clear_fixed_forest(self._h), "kds_aligner_clear_fixed_forest")
+
+    def compute(self, stats_mode: bool = False) -> int:
+        r = C.c_int32()
+        _check(_lib.kds_aligner_compute(self._h, 1 if stats_mode else 0, C.byref(r)), "kds_aligner_compute")
+        log = (L.Stats * 64)()
+        n = C.c_int32()
+        _check(_lib.kds_aligner_get_stats_log(self._h, log, 64, C.byref(n)), "kds_aligner_get_stats_log")
+        self.stats_log = [log[i].as_dict() for i in range(min(n.value, 64))]
+        return r.value
+
+    def one_round(self, stats_mode: bool = False) -> bool:
+        ok = C.c_int32()
+        _check(_lib.kds_aligner_one_round(self._h, 1 if stats_mode else 0, C.byref(ok)), "kds_aligner_one_round")
+        return bool(ok.value)
+
+    def build_quadratic_form(self, stats_mode: bool = False) -> None:
+        _check(_lib.kds_aligner_build_quadratic_form(self._h, 1 if stats_mode else 0),
+               "kds_aligner_build_quadratic_form")
+
+    def _hb(self):
+        D = self.D
+        H, b, dx = np.zeros(D * D), np.zeros(D), np.zeros(D)
+        _check(_lib.kds_aligner_get_hb(self._h, H.ctypes.data, b.ctypes.data, dx.ctypes.data), "kds_aligner_get_hb")
+        return H.reshape(D, D), b, dx
+
+    @property
+    def H(self) -> np.ndarray:
+        return self._hb()[0]
+
+    @property
+    def b(self) -> np.ndarray:
+        return self._hb()[1]
+
+    @property
+    def dx(self) -> np.ndarray:
+        return self._hb()[2]
+
+    @property
+    def stats(self) -> dict:
+        s = L.Stats()
+        _check(_lib.kds_aligner_get_stats(self._h, C.byref(s)), "kds_aligner_get_stats")
+        return s.as_dict()
+
+    def get_pose_hessian(self) -> np.ndarray:
+        H = np.zeros(36)
+        _check(_lib.kds_aligner_get_pose_hessian(self._h, H.ctypes.data), "kds_aligner_get_pose_hessian")
+        return H.reshape(6, 6)
+
+    def linearize_debug(self, caches36, v=None, fixed_v=None, kind=None, stats_mode=False):
+        """One linearization at explicit float caches (Xm, Xf, Xmf): per-leaf matches and status."""
+        n = self._moving.num_leaves
+        kind = (0 if self.TYPE == L.KDS_ICP else 1) if kind is None else kind
+        D = 6 if kind == 0 else 12
+        c = np.ascontiguousarray(caches36, np.float32)
+        vv = None if v is None else np.ascontiguousarray(v, np.float32)
+        fv = None if fixed_v is None else np.ascontiguousarray(fixed_v, np.float32)
+        match = np.zeros(n, np.int32)
+        status = np.zeros(n, np.int32)
+        H, b = np.zeros(D * D), np.zeros(D)
+        st = L.Stats()
+        _check(_lib.kds_aligner_linearize_debug(self._h, c.ctypes.data, _ptr(vv), _ptr(fv), kind,
+                                                1 if stats_mode else 0, match.ctypes.data, status.ctypes.data,
+                                                H.ctypes.data, b.ctypes.data, C.byref(st)),
+               "kds_aligner_linearize_debug")
+        return match, status, H.reshape(D, D), b, st.as_dict()
+
+
+class ICPB2003D(_AlignerBase):
+    TYPE = L.KDS_ICP
+    D = 6
+
+
+class CTICPB2003D(_AlignerBase):
+    TYPE = L.KDS_CTICP
+    D = 12
+
+    def __init__(self, **params):
+        params.setdefault("velocity_damping", 100.0)
+        super().__init__(**params)
+
+    def build_quadratic_form_dual(self, stats_mode: bool = False) -> None:
+        _check(_lib.kds_aligner_build_quadratic_form_dual(self._h, 1 if stats_mode else 0),
+               "kds_aligner_build_quadratic_form_dual")
+
+    def dual(self) -> dict:
+        a, b, c, d = np.zeros(36), np.zeros(6), np.zeros(36), np.zeros(36)
+        _check(_lib.kds_aligner_get_dual(self._h, a.ctypes.data, b.ctypes.data, c.ctypes.data, d.ctypes.data),
+               "kds_aligner_get_dual")
+        return {"H_dual_vel_B": a.reshape(6, 6), "b_dual_vel_B": b,
+                "H_dual_cross_pose_vel_B": c.reshape(6, 6), "H_dual_cross_vel_AB": d.reshape(6, 6)}
+
+
+# ---------------------------------------------------------------------------- batches
+class Batch:
+    """Many independent alignments / linearizations per launch (kds_batch_run)."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        _check(_lib.kds_batch_create(C.byref(h)), "kds_batch_create")
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.kds_batch_free(self._h)
+            self._h = C.c_void_p(None)
+
+    def run(self, jobs, use_graph: bool = True, stream=None):
+        arr = (L.Job * len(jobs))(*jobs)
+        _check(_lib.kds_batch_run(self._h, arr, len(jobs), 1 if use_graph else 0, stream), "kds_batch_run")
+        return arr
+
+
+def make_job(kind: int, fixed: Tree, moving: Tree, params: L.AlignerParams, X=None, fixed_X=None, v=None,
+             fixed_v=None, mode: int = L.KDS_JOB_COMPUTE, stats_mode: bool = False) -> L.Job:
+    j = L.Job()
+    j.type = kind
+    j.mode = mode
+    j.stats_mode = 1 if stats_mode else 0
+    j.fixed = fixed.handle.value
+    j.moving = moving.handle.value
+    j.params = params
+    j.X[:] = list(_pose12(identity() if X is None else X))
+    j.fixed_X[:] = list(_pose12(identity() if fixed_X is None else fixed_X))
+    j.v[:] = list(np.zeros(6) if v is None else np.asarray(v, np.float64))
+    j.fixed_v[:] = list(np.zeros(6) if fixed_v is None else np.asarray(fixed_v, np.float64))
+    return j
+
+
+def aligner_params(**kw) -> L.AlignerParams:
+    p = L.AlignerParams()
+    _lib.kds_aligner_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def tree_params(**kw) -> L.TreeParams:
+    p = L.TreeParams()
+    _lib.kds_tree_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+__all__ = ["Tree", "TreeGeneratorB2003D", "ICPB2003D", "CTICPB2003D", "Batch", "make_job", "aligner_params",
+           "tree_params", "identity", "init", "KdsError"]

@@ -1,0 +1,186 @@
+"""ctypes declarations of libkds.so (include/kds.h).
+
+The library is loaded from this package directory.  There is no fallback: if the
+shared object is missing or fails to load, importing fails with an error that says
+how to build it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libkds.so")
+
+KDS_OK = 0
+KDS_ERR_INVALID_ARG = -1
+KDS_ERR_CUDA = -2
+KDS_ERR_OOM = -3
+KDS_ERR_TREE_REJECTED = -4
+KDS_ERR_RANGE = -5
+KDS_ERR_BAD_TREE = -6
+KDS_ERR_STATE = -7
+KDS_ERR_TIMEOUT = -8
+KDS_ERR_ADMISSION = -9
+KDS_ERR_NO_DEVICE = -10
+KDS_ERR_CAPACITY = -11
+
+KDS_ICP = 0
+KDS_CTICP = 1
+KDS_MEM_HOST = 0
+KDS_MEM_DEVICE = 1
+KDS_JOB_COMPUTE = 0
+KDS_JOB_LINEARIZE = 1
+KDS_JOB_LINEARIZE_DUAL = 2
+
+
+class TreeParams(C.Structure):
+    _fields_ = [
+        ("propagate_normal", C.c_int32),
+        ("tree_min_good_leaves", C.c_int32),
+        ("leaf_min_points", C.c_int32),
+        ("leaf_max_points", C.c_int32),
+        ("leaf_density", C.c_float),
+        ("leaf_min_normal_incidence", C.c_float),
+        ("leaf_eigenvalue_threshold", C.c_float),
+        ("leaf_normal_eigenratio", C.c_float),
+        ("prune_min_normal_incidence", C.c_float),
+        ("max_level", C.c_int32),
+    ]
+
+
+class TreeInfo(C.Structure):
+    _fields_ = [
+        ("num_nodes", C.c_int64),
+        ("num_leaves", C.c_int64),
+        ("num_points", C.c_int64),
+        ("num_unpruned", C.c_int64),
+        ("ts_start", C.c_double),
+        ("accepted", C.c_int32),
+        ("depth", C.c_int32),
+    ]
+
+
+class AlignerParams(C.Structure):
+    _fields_ = [
+        ("kernel_threshold", C.c_float),
+        ("damping", C.c_float),
+        ("max_error", C.c_float),
+        ("min_normal_cos", C.c_float),
+        ("min_good_measurements", C.c_int32),
+        ("max_iterations", C.c_int32),
+        ("velocity_damping", C.c_float),
+        ("term_crit", C.c_int32),
+        ("d_pert", C.c_float),
+        ("d_score", C.c_float),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("num_inliers", C.c_int32),
+        ("num_outliers", C.c_int32),
+        ("num_bad", C.c_int32),
+        ("num_err_normal", C.c_int32),
+        ("num_err_fn", C.c_int32),
+        ("chi2", C.c_float),
+        ("chi2_kernelized", C.c_float),
+        ("pert_pose_norm", C.c_float),
+        ("pert_vel_norm", C.c_float),
+    ]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class Job(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("mode", C.c_int32),
+        ("stats_mode", C.c_int32),
+        ("pad_", C.c_int32),
+        ("fixed", C.c_void_p),
+        ("moving", C.c_void_p),
+        ("params", AlignerParams),
+        ("X", C.c_double * 12),
+        ("fixed_X", C.c_double * 12),
+        ("v", C.c_double * 6),
+        ("fixed_v", C.c_double * 6),
+        ("result", C.c_int32),
+        ("iterations", C.c_int32),
+        ("stats", Stats),
+        ("H", C.c_double * 144),
+        ("b", C.c_double * 12),
+        ("H_vel_B", C.c_double * 36),
+        ("b_vel_B", C.c_double * 6),
+        ("H_cross_pose_vel_B", C.c_double * 36),
+        ("H_cross_vel_AB", C.c_double * 36),
+    ]
+
+
+# Every entry point declared in include/kds.h: name -> (restype, argtypes)
+_P = C.c_void_p
+_I32 = C.c_int32
+_I64 = C.c_int64
+SIGNATURES = {
+    "kds_last_error": (C.c_char_p, []),
+    "kds_init": (C.c_int, [_I32, _I32]),
+    "kds_tree_params_default": (None, [C.POINTER(TreeParams)]),
+    "kds_tree_build": (C.c_int, [_P, _P, _I64, _I32, C.POINTER(TreeParams), _P, C.POINTER(_P)]),
+    "kds_tree_import": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _I64, C.c_double, C.POINTER(_P)]),
+    "kds_tree_get_info": (C.c_int, [_P, C.POINTER(TreeInfo)]),
+    "kds_tree_export": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "kds_tree_apply_velocities": (C.c_int, [_P, _P, _I32, _P]),
+    "kds_tree_apply_isometry": (C.c_int, [_P, _P, _P]),
+    "kds_tree_extract_compressed_leaves": (C.c_int, [_P, _P, _P, _P]),
+    "kds_tree_free": (None, [_P]),
+    "kds_aligner_params_default": (None, [C.POINTER(AlignerParams)]),
+    "kds_aligner_create": (C.c_int, [_I32, C.POINTER(AlignerParams), C.POINTER(_P)]),
+    "kds_aligner_set_params": (C.c_int, [_P, C.POINTER(AlignerParams)]),
+    "kds_aligner_set_stream": (C.c_int, [_P, _P]),
+    "kds_aligner_set_fixed": (C.c_int, [_P, _P]),
+    "kds_aligner_set_moving": (C.c_int, [_P, _P]),
+    "kds_aligner_set_x": (C.c_int, [_P, _P]),
+    "kds_aligner_get_x": (C.c_int, [_P, _P]),
+    "kds_aligner_set_fixed_x": (C.c_int, [_P, _P]),
+    "kds_aligner_set_velocities": (C.c_int, [_P, _P]),
+    "kds_aligner_get_velocities": (C.c_int, [_P, _P]),
+    "kds_aligner_set_fixed_velocities": (C.c_int, [_P, _P]),
+    "kds_aligner_reset_moving_state": (C.c_int, [_P]),
+    "kds_aligner_set_pose_prior": (C.c_int, [_P, _P, _P, _P]),
+    "kds_aligner_add_fixed_entry": (C.c_int, [_P, _P, _P]),
+    "kds_aligner_clear_fixed_forest": (C.c_int, [_P]),
+    "kds_aligner_compute": (C.c_int, [_P, _I32, C.POINTER(_I32)]),
+    "kds_aligner_one_round": (C.c_int, [_P, _I32, C.POINTER(_I32)]),
+    "kds_aligner_build_quadratic_form": (C.c_int, [_P, _I32]),
+    "kds_aligner_build_quadratic_form_dual": (C.c_int, [_P, _I32]),
+    "kds_aligner_get_hb": (C.c_int, [_P, _P, _P, _P]),
+    "kds_aligner_get_dual": (C.c_int, [_P, _P, _P, _P, _P]),
+    "kds_aligner_get_pose_hessian": (C.c_int, [_P, _P]),
+    "kds_aligner_get_stats": (C.c_int, [_P, C.POINTER(Stats)]),
+    "kds_aligner_get_stats_log": (C.c_int, [_P, C.POINTER(Stats), _I32, C.POINTER(_I32)]),
+    "kds_aligner_linearize_debug": (C.c_int, [_P, _P, _P, _P, _I32, _I32, _P, _P, _P, _P, C.POINTER(Stats)]),
+    "kds_aligner_free": (None, [_P]),
+    "kds_batch_create": (C.c_int, [C.POINTER(_P)]),
+    "kds_batch_run": (C.c_int, [_P, C.POINTER(Job), _I32, _I32, _P]),
+    "kds_batch_free": (None, [_P]),
+}
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    if not os.path.exists(path):
+        raise ImportError(
+            f"libkds.so not found at {path}; build it with `python -m kd_slam2_b200.build` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+class KdsError(RuntimeError):
+    def __init__(self, code: int, where: str, text: str):
+        super().__init__(f"{where}: status {code}: {text}")
+        self.code = code

@@ -1,0 +1,846 @@
+// Fused ICP / CT-ICP linearization and on-device Gauss-Newton.
+//
+// One launch = one Gauss-Newton iteration for every job of a batch.  A job is one
+// alignment (ICP_::compute / CTICP_::compute, kd/icp/tree_aligner_base_.h:100-115)
+// or one buildQuadraticForm; it has one moving leaf set and one or more fixed
+// entries (the _fixed_forest of kd/icp/icp_impl_.h:55-71).  The grid is a flat list of
+// tiles (job, entry, 128 moving leaves); each block:
+//   1. runs quadraticTerm for its leaves (kd/icp/icp_impl_.h:102-152,
+//      kd/cticp/cticp_impl_.h:105-293): optional CT warp, greedy descent through the
+//      fixed tree, gates, symmetric error, Jacobian, robust weight -- the gating path in
+//      exact single roundings so matches and masks equal the CPU oracle bit for bit;
+//   2. reduces gamma*J^T J and gamma*J^T e over its leaves warp-cooperatively: each
+//      lane owns a few of the D(D+1)/2+D entries and sums them over the warp's 32
+//      leaves with Kahan compensation; warps are combined in FP64 into one block
+//      partial (no per-leaf workspace, replacing ICP_kernel + ~2x14 _reduce1 passes,
+//      kd/icp/icp_cuda_impl_.cuh:68-132, kd/cuda/reduce_impl_.cuh:9-78);
+//   3. the last block of a job to finish sums the job's partials in tile order (FP64,
+//      deterministic: the result of a job does not depend on what else is in the
+//      batch), adds the pose prior, solves (H + damping) dx = -b by FP64 LDL^T, applies
+//      X <- expmap(dx) X, v += dx_v, runs the termination test and refreshes the
+//      float caches for the next launch.  No host round trip inside compute().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "kds_align.cuh"
+#include "kds_internal.cuh"
+
+namespace kds {
+
+__device__ __forceinline__ F3 cross3(F3 a, F3 b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float dot3f(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// M = A * B (3x3 row-major), relaxed rounding (Jacobian path only)
+__device__ __forceinline__ void mm3(const float* A, const float* B, float* C) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) C[i * 3 + j] = A[i * 3] * B[j] + A[i * 3 + 1] * B[3 + j] + A[i * 3 + 2] * B[6 + j];
+}
+__device__ __forceinline__ F3 mv3(const float* A, F3 p) {
+  return f3(A[0] * p.x + A[1] * p.y + A[2] * p.z, A[3] * p.x + A[4] * p.y + A[5] * p.z,
+            A[6] * p.x + A[7] * p.y + A[8] * p.z);
+}
+
+// Pieces of dRxp (kd/utils/geometry_3d_impl_.h:143-174) shared by both of its calls:
+// R = rodrigues(w) and Q = n n^T + (R^T - I) S / angle, so that
+// d(R u)/dw = -R skew(u) Q.  small = angle < 1e-9 (then dR = -skew(u)).
+struct DRxp {
+  float R[9];
+  float Q[9];
+  bool small;
+};
+__device__ __forceinline__ void drxp_setup(F3 w, DRxp& d) {
+  float angle = sqrtf(dot3f(w, w));
+  d.small = angle < 1e-9f;
+  if (d.small) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) { d.R[i] = (i % 4 == 0) ? 1.f : 0.f; d.Q[i] = 0.f; }
+    return;
+  }
+  rodrigues_x(w, d.R);
+  float inv = 1.0f / angle;
+  F3 n = f3(w.x * inv, w.y * inv, w.z * inv);
+  float S[9] = {0.f, -n.z, n.y, n.z, 0.f, -n.x, -n.y, n.x, 0.f};
+  float RtmI[9] = {d.R[0] - 1.f, d.R[3], d.R[6], d.R[1], d.R[4] - 1.f, d.R[7], d.R[2], d.R[5], d.R[8] - 1.f};
+  float A[9];
+  mm3(RtmI, S, A);
+  float nn[3] = {n.x, n.y, n.z};
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) d.Q[i * 3 + j] = nn[i] * nn[j] + A[i * 3 + j] * inv;
+}
+// out = Ra * d(R u)/dw  (3x3)
+__device__ __forceinline__ void ra_drxp(const DRxp& d, const float* Ra, F3 u, float* out) {
+  float su[9] = {0.f, -u.z, u.y, u.z, 0.f, -u.x, -u.y, u.x, 0.f};
+  float dR[9];
+  if (d.small) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) dR[i] = -su[i];
+  } else {
+    float Rs[9], P[9];
+    mm3(d.R, su, Rs);
+    mm3(Rs, d.Q, P);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) dR[i] = -P[i];
+  }
+  mm3(Ra, dR, out);
+}
+
+// errorAndJacobianVelocityA (kd/d3/cticp_impl_.h:10-39) -> J[0..5]
+__device__ __forceinline__ void jac_vel_A(const float* Xm, F3 pa_l, F3 na_l, F3 pb_g, F3 nb_g, const float* va, float dt,
+                                          float* J) {
+  F3 tm = f3(va[0] * dt, va[1] * dt, va[2] * dt);
+  F3 wa = f3(va[3] * dt, va[4] * dt, va[5] * dt);
+  DRxp d;
+  drxp_setup(wa, d);
+  float Ra[9] = {Xm[0], Xm[1], Xm[2], Xm[4], Xm[5], Xm[6], Xm[8], Xm[9], Xm[10]};
+  F3 pam = mv3(d.R, pa_l);
+  pam = f3(pam.x + tm.x, pam.y + tm.y, pam.z + tm.z);
+  F3 nam = mv3(d.R, na_l);
+  F3 pag = mv3(Ra, pam);
+  pag = f3(pag.x + Xm[3], pag.y + Xm[7], pag.z + Xm[11]);
+  F3 nag = mv3(Ra, nam);
+  F3 n = f3(nag.x + nb_g.x, nag.y + nb_g.y, nag.z + nb_g.z);
+  F3 dp = f3(pag.x - pb_g.x, pag.y - pb_g.y, pag.z - pb_g.z);
+  float A[9], B[9];
+  ra_drxp(d, Ra, pa_l, A);
+  ra_drxp(d, Ra, na_l, B);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    J[c] = (n.x * Ra[c] + n.y * Ra[3 + c] + n.z * Ra[6 + c]) * dt;
+    J[3 + c] = (n.x * A[c] + n.y * A[3 + c] + n.z * A[6 + c] + dp.x * B[c] + dp.y * B[3 + c] + dp.z * B[6 + c]) * dt;
+  }
+}
+
+// errorAndJacobianVelocityB (kd/d3/cticp_impl_.h:43-73) -> J[0..5]
+__device__ __forceinline__ void jac_vel_B(const float* Xf, F3 pa_g, F3 na_g, F3 pb_l, F3 nb_l, const float* vb, float dt,
+                                          float* J) {
+  F3 tm = f3(vb[0] * dt, vb[1] * dt, vb[2] * dt);
+  F3 wb = f3(vb[3] * dt, vb[4] * dt, vb[5] * dt);
+  DRxp d;
+  drxp_setup(wb, d);
+  float Rb[9] = {Xf[0], Xf[1], Xf[2], Xf[4], Xf[5], Xf[6], Xf[8], Xf[9], Xf[10]};
+  F3 pbm = mv3(d.R, pb_l);
+  pbm = f3(pbm.x + tm.x, pbm.y + tm.y, pbm.z + tm.z);
+  F3 nbm = mv3(d.R, nb_l);
+  F3 pbg = mv3(Rb, pbm);
+  pbg = f3(pbg.x + Xf[3], pbg.y + Xf[7], pbg.z + Xf[11]);
+  F3 nbg = mv3(Rb, nbm);
+  F3 n = f3(na_g.x + nbg.x, na_g.y + nbg.y, na_g.z + nbg.z);
+  F3 dp = f3(pa_g.x - pbg.x, pa_g.y - pbg.y, pa_g.z - pbg.z);
+  float A[9], B[9];
+  ra_drxp(d, Rb, pb_l, A);
+  ra_drxp(d, Rb, nb_l, B);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    J[c] = -(n.x * Rb[c] + n.y * Rb[3 + c] + n.z * Rb[6 + c]) * dt;
+    J[3 + c] = (-(n.x * A[c] + n.y * A[3 + c] + n.z * A[6 + c]) + dp.x * B[c] + dp.y * B[3 + c] + dp.z * B[6 + c]) * dt;
+  }
+}
+
+enum { ST_INLIER = 0, ST_OUTLIER = 1, ST_BAD = 2, ST_ERR_NORMAL = 3, ST_ERR_FN = 4, ST_NONE = 5 };
+
+template <int KIND> struct KindDim;
+template <> struct KindDim<0> { static constexpr int D = 6; };
+template <> struct KindDim<1> { static constexpr int D = 12; };
+template <> struct KindDim<2> { static constexpr int D = 18; };
+
+template <int KIND>
+__device__ __forceinline__ void leaf_term(const CacheF& C, const DNode* F, int fnn, const float* fdts, float4 md,
+                                          float4 nr, const ParamsF& P, bool stats_mode, int& status, int& match,
+                                          float& e_out, float& gamma_out, float* J) {
+  constexpr int D = KindDim<KIND>::D;
+#pragma unroll
+  for (int i = 0; i < D; ++i) J[i] = 0.f;
+  e_out = 0.f;
+  gamma_out = 0.f;
+  F3 m = f3(md.x, md.y, md.z), n = f3(nr.x, nr.y, nr.z);
+  float dt = md.w;
+  F3 mw = m, nw = n;
+  if (KIND != 0) warp_x(C.v, dt, m, n, mw, nw);
+  F3 q = apply_iso_x(C.Xmf, mw);
+  // greedy descent (kd/icp/icp_impl_.h:116-121): no backtracking
+  int idx = fnn > 0 ? 0 : -1;
+  DNode nd;
+  while (idx >= 0) {
+    nd = load_node(F + idx);
+    int l = node_left(nd), r = node_right(nd);
+    if (l < 0 && r < 0) break;
+    bool side = dot3x(node_dir(nd), sub3x(q, node_mean(nd))) > 0.0f;
+    idx = side ? l : r;
+  }
+  match = idx;
+  if (idx < 0) { status = ST_BAD; return; }
+  F3 pf = node_mean(nd), nf = node_dir(nd);
+  F3 pm = apply_iso_x(C.Xm, mw);
+  F3 nm = apply_rot_x(C.Xm, nw);
+  F3 pfx = apply_iso_x(C.Xf, pf);
+  F3 nfx = apply_rot_x(C.Xf, nf);
+  // ICP_3D_Traits::errorAndJacobian (kd/d3/icp_.h:40-60)
+  if (dot3x(nfx, nm) < P.min_normal_cos) { status = ST_ERR_NORMAL; return; }
+  F3 ns = add3x(nm, nfx);
+  float e = dot3x(sub3x(pm, pfx), ns);
+  if (fabsf(e) > P.max_error) { status = ST_ERR_FN; return; }
+  F3 c1 = cross3(pm, nfx), c2 = cross3(pfx, nm);
+  J[0] = ns.x; J[1] = ns.y; J[2] = ns.z;
+  J[3] = c1.x + c2.x; J[4] = c1.y + c2.y; J[5] = c1.z + c2.z;
+  if (KIND != 0) jac_vel_A(C.Xm, m, n, pfx, nfx, C.v, dt, J + 6);
+  float chi2 = fm(e, e);
+  float kt = P.kernel_threshold;
+  float gamma;
+  if (KIND == 2) {
+    gamma = stats_mode ? 0.f : 1.f;
+    if (chi2 > kt) { status = ST_OUTLIER; gamma = __fsqrt_rn(__fdiv_rn(kt, chi2)); }
+    else status = ST_INLIER;
+    jac_vel_B(C.Xf, pm, nm, pf, nf, C.fv, fdts[idx], J + 12);
+  } else {
+    gamma = 1.f;
+    if (chi2 > kt) { status = ST_OUTLIER; gamma = stats_mode ? 0.f : __fsqrt_rn(__fdiv_rn(kt, chi2)); }
+    else status = ST_INLIER;
+  }
+  e_out = e;
+  gamma_out = gamma;
+}
+
+// entry k of the packed D(D+1)/2 + D vector -> (row, col); col == D means "e"
+__device__ __forceinline__ void entry_rc(int D, int k, int& r, int& c) {
+  int T = D * (D + 1) / 2;
+  if (k >= T) { r = k - T; c = D; return; }
+  int rr = 0, off = 0;
+  while (off + (D - rr) <= k) { off += D - rr; ++rr; }
+  r = rr;
+  c = rr + (k - off);
+}
+
+constexpr int kBlock = 128;
+constexpr int kWarps = kBlock / 32;
+constexpr int kMaxFS = 21;  // factor row stride (D + 2, padded to odd)
+
+template <int KIND>
+__device__ __forceinline__ void tile_body(const JobIn& Jn, const LinDev& L, const CacheF& C, const TileDev& T,
+                                          double* wpart /* [kWarps][kPStride] */, float* fac /* [kWarps][32][kMaxFS] */,
+                                          int32_t* dbg_match, int32_t* dbg_status) {
+  constexpr int D = KindDim<KIND>::D;
+  constexpr int M = D * (D + 1) / 2 + D;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = T.leaf_begin + threadIdx.x;
+  int status = ST_NONE, match = -1;
+  float e = 0.f, gamma = 0.f;
+  float J[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) J[k] = 0.f;
+  if (i < T.leaf_end) {
+    float4 md = __ldg(Jn.m_md + i);
+    float4 nr = __ldg(Jn.m_nrm + i);
+    leaf_term<KIND>(C, L.fnodes, L.f_num_nodes, L.fdts, md, nr, Jn.P, Jn.stats_mode != 0, status, match, e, gamma, J);
+    if (dbg_match) { dbg_match[i] = match; dbg_status[i] = status; }
+  }
+  bool contrib = status == ST_INLIER || status == ST_OUTLIER;
+  float* row = fac + (w * 32 + lane) * kMaxFS;
+#pragma unroll
+  for (int k = 0; k < D; ++k) row[k] = contrib ? J[k] : 0.f;
+  row[D] = contrib ? e : 0.f;
+  row[D + 1] = contrib ? gamma : 0.f;
+  // stats (ICPStats_::pack, kd/icp/icp_stats_.h:57-59)
+  unsigned full = 0xffffffffu;
+  int c_in = __popc(__ballot_sync(full, status == ST_INLIER));
+  int c_out = __popc(__ballot_sync(full, status == ST_OUTLIER));
+  int c_bad = __popc(__ballot_sync(full, status == ST_BAD));
+  int c_nrm = __popc(__ballot_sync(full, status == ST_ERR_NORMAL));
+  int c_fn = __popc(__ballot_sync(full, status == ST_ERR_FN));
+  double chi2 = contrib ? (double)fm(e, e) : 0.0;
+  double chi2k = contrib ? (double)fm(fm(e, e), gamma) : 0.0;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    chi2 += __shfl_xor_sync(full, chi2, off);
+    chi2k += __shfl_xor_sync(full, chi2k, off);
+  }
+  __syncwarp();
+  // warp-cooperative outer products: lane owns entries lane, lane+32, ...
+  const float* wf = fac + w * 32 * kMaxFS;
+  double* wp = wpart + w * kPStride;
+  for (int k = lane; k < M; k += 32) {
+    int r, c;
+    entry_rc(D, k, r, c);
+    float s = 0.f, comp = 0.f;
+#pragma unroll 8
+    for (int l = 0; l < 32; ++l) {
+      const float* fr = wf + l * kMaxFS;
+      float val = fr[r] * fr[c] * fr[D + 1];
+      float y = val - comp;
+      float t = s + y;
+      comp = (t - s) - y;
+      s = t;
+    }
+    wp[k] = (double)s - (double)comp;
+  }
+  if (lane == 0) {
+    wp[kPStats + 0] = c_in;
+    wp[kPStats + 1] = c_out;
+    wp[kPStats + 2] = c_bad;
+    wp[kPStats + 3] = c_nrm;
+    wp[kPStats + 4] = c_fn;
+    wp[kPStats + 5] = chi2;
+    wp[kPStats + 6] = chi2k;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 finalize (one thread) -- ICP_::oneRound / CTICP_::oneRound.
+__device__ void iso_mul_d(const double* A, const double* B, double* C) {
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j)
+      C[i * 4 + j] = A[i * 4] * B[j] + A[i * 4 + 1] * B[4 + j] + A[i * 4 + 2] * B[8 + j];
+    C[i * 4 + 3] = A[i * 4] * B[3] + A[i * 4 + 1] * B[7] + A[i * 4 + 2] * B[11] + A[i * 4 + 3];
+  }
+}
+__device__ void iso_inv_d(const double* A, double* B) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) B[i * 4 + j] = A[j * 4 + i];
+  for (int i = 0; i < 3; ++i) B[i * 4 + 3] = -(B[i * 4] * A[3] + B[i * 4 + 1] * A[7] + B[i * 4 + 2] * A[11]);
+}
+__device__ void rodrigues_d(const double* w, double* R) {
+  double a = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+  if (a < 1e-9) {
+    for (int i = 0; i < 9; ++i) R[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    return;
+  }
+  double n[3] = {w[0] / a, w[1] / a, w[2] / a};
+  double S[9] = {0, -n[2], n[1], n[2], 0, -n[0], -n[1], n[0], 0};
+  double s, c;
+  sincos(a, &s, &c);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s2 = S[i * 3] * S[j] + S[i * 3 + 1] * S[3 + j] + S[i * 3 + 2] * S[6 + j];
+      R[i * 3 + j] = ((i == j) ? 1.0 : 0.0) + s * S[i * 3 + j] + (1.0 - c) * s2;
+    }
+}
+__device__ void expmap_d(const double* v, double* X) {
+  double R[9];
+  rodrigues_d(v + 3, R);
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) X[i * 4 + j] = R[i * 3 + j];
+    X[i * 4 + 3] = v[i];
+  }
+}
+__device__ void logso3_d(const double* X, double* w) {
+  double tr = X[0] + X[5] + X[10];
+  double ca = fmin(1.0, fmax(-1.0, 0.5 * (tr - 1.0)));
+  double a = acos(ca);
+  double ax[3] = {X[9] - X[6], X[2] - X[8], X[4] - X[1]};
+  double f = (a < 1e-7) ? 0.5 : a / (2.0 * sin(a));
+  for (int i = 0; i < 3; ++i) w[i] = ax[i] * f;
+}
+// dPoseToPoseError (kd/utils/geometry_3d_impl_.h:125-140) in FP64
+__device__ void dpose_d(const double* ZXi, const double* Xm, double* e, double J[6][6]) {
+  double P[12];
+  iso_mul_d(ZXi, Xm, P);
+  for (int i = 0; i < 3; ++i) e[i] = P[i * 4 + 3];
+  logso3_d(P, e + 3);
+  double R[9] = {ZXi[0], ZXi[1], ZXi[2], ZXi[4], ZXi[5], ZXi[6], ZXi[8], ZXi[9], ZXi[10]};
+  double B[12][6];
+  for (int i = 0; i < 12; ++i) for (int j = 0; j < 6; ++j) B[i][j] = 0.0;
+  auto skewmul = [&](const double* v, double* out) {  // out = R * skew(v)
+    double S[9] = {0, -v[2], v[1], v[2], 0, -v[0], -v[1], v[0], 0};
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) out[i * 3 + j] = R[i * 3] * S[j] + R[i * 3 + 1] * S[3 + j] + R[i * 3 + 2] * S[6 + j];
+  };
+  double t[3] = {Xm[3], Xm[7], Xm[11]};
+  double RS[9];
+  skewmul(t, RS);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) { B[i][j] = R[i * 3 + j]; B[i][3 + j] = -RS[i * 3 + j]; }
+  for (int k = 0; k < 3; ++k) {
+    double col[3] = {Xm[k], Xm[4 + k], Xm[8 + k]};
+    skewmul(col, RS);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) B[3 + 3 * k + i][3 + j] = -RS[i * 3 + j];
+  }
+  // dlogSO3 of P's rotation (column-major coefficient order)
+  double ax[3] = {P[9] - P[6], P[2] - P[8], P[4] - P[1]};
+  double tr = P[0] + P[5] + P[10];
+  double ca = fmin(1.0, fmax(-1.0, 0.5 * (tr - 1.0)));
+  double a = acos(ca);
+  bool small = a < 1e-7;
+  double f = small ? 0.5 : a / (2.0 * sin(a));
+  double Js[3][9];
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 9; ++j) Js[i][j] = 0.0;
+  Js[0][5] = f; Js[0][7] = -f;
+  Js[1][6] = f; Js[1][2] = -f;
+  Js[2][1] = f; Js[2][3] = -f;
+  if (!small) {
+    double s = sin(a);
+    double c = (s - a * cos(a)) / (4.0 * s * s * s);
+    for (int k = 0; k < 3; ++k) { Js[k][0] -= c * ax[k]; Js[k][4] -= c * ax[k]; Js[k][8] -= c * ax[k]; }
+  }
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) {
+      double acc = 0.0;
+      if (i < 3) acc = B[i][j];
+      else for (int k = 0; k < 9; ++k) acc += Js[i - 3][k] * B[3 + k][j];
+      J[i][j] = acc;
+    }
+}
+
+// symmetric LDL^T with diagonal pivoting, n <= 12, in place on A (row-major)
+__device__ bool ldlt_solve_d(int n, double* A, const double* rhs, double* x) {
+  int perm[12];
+  double L[12][12], Dg[12], y[12];
+  for (int i = 0; i < n; ++i) {
+    perm[i] = i;
+    for (int j = 0; j < n; ++j) L[i][j] = (i == j) ? 1.0 : 0.0;
+  }
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double best = fabs(A[k * n + k]);
+    for (int i = k + 1; i < n; ++i)
+      if (fabs(A[i * n + i]) > best) { best = fabs(A[i * n + i]); p = i; }
+    if (p != k) {
+      for (int j = 0; j < n; ++j) { double tmp = A[k * n + j]; A[k * n + j] = A[p * n + j]; A[p * n + j] = tmp; }
+      for (int i = 0; i < n; ++i) { double tmp = A[i * n + k]; A[i * n + k] = A[i * n + p]; A[i * n + p] = tmp; }
+      for (int j = 0; j < k; ++j) { double tmp = L[k][j]; L[k][j] = L[p][j]; L[p][j] = tmp; }
+      int tp = perm[k]; perm[k] = perm[p]; perm[p] = tp;
+    }
+    double d = A[k * n + k];
+    Dg[k] = d;
+    if (d == 0.0) return false;
+    for (int i = k + 1; i < n; ++i) L[i][k] = A[i * n + k] / d;
+    for (int i = k + 1; i < n; ++i)
+      for (int j = k + 1; j <= i; ++j) {
+        A[i * n + j] = A[i * n + j] - L[i][k] * d * L[j][k];
+        A[j * n + i] = A[i * n + j];
+      }
+  }
+  for (int i = 0; i < n; ++i) y[i] = rhs[perm[i]];
+  for (int i = 0; i < n; ++i) {
+    double acc = y[i];
+    for (int j = 0; j < i; ++j) acc -= L[i][j] * y[j];
+    y[i] = acc;
+  }
+  for (int i = 0; i < n; ++i) y[i] /= Dg[i];
+  for (int i = n - 1; i >= 0; --i) {
+    double acc = y[i];
+    for (int j = i + 1; j < n; ++j) acc -= L[j][i] * y[j];
+    y[i] = acc;
+  }
+  for (int i = 0; i < n; ++i) x[perm[i]] = y[i];
+  return true;
+}
+
+__device__ void refresh_caches(const JobState& S, LinDev* lins, int lb, int lc) {
+  for (int l = lb; l < lb + lc; ++l) {
+    LinDev& L = lins[l];
+    double iXf[12], Xmf[12];
+    iso_inv_d(L.Xf, iXf);
+    iso_mul_d(iXf, S.X, Xmf);
+    for (int k = 0; k < 12; ++k) {
+      L.cache.Xm[k] = (float)S.X[k];
+      L.cache.Xf[k] = (float)L.Xf[k];
+      L.cache.Xmf[k] = (float)Xmf[k];
+    }
+    for (int k = 0; k < 6; ++k) {
+      L.cache.v[k] = (float)S.v[k];
+      L.cache.fv[k] = (float)L.fv[k];
+    }
+  }
+}
+
+__device__ __noinline__ void finalize(const JobIn& Jn, JobState& S, JobOut& O, kds_stats* log, LinDev* lins, const double* red) {
+  const int kind = Jn.kind;
+  const int Dk = kind == 0 ? 6 : (kind == 1 ? 12 : 18);
+  const int D = kind == 0 ? 6 : 12;
+  // unpack the upper triangle of the Dk x Dk system
+  double Hf[18 * 18], bf[18];
+  {
+    int k = 0;
+    for (int a = 0; a < Dk; ++a)
+      for (int c = a; c < Dk; ++c) { Hf[a * Dk + c] = red[k]; Hf[c * Dk + a] = red[k]; ++k; }
+    for (int a = 0; a < Dk; ++a) bf[a] = red[k++];
+  }
+  kds_stats st;
+  st.num_inliers = (int32_t)red[kPStats + 0];
+  st.num_outliers = (int32_t)red[kPStats + 1];
+  st.num_bad = (int32_t)red[kPStats + 2];
+  st.num_err_normal = (int32_t)red[kPStats + 3];
+  st.num_err_fn = (int32_t)red[kPStats + 4];
+  st.chi2 = (float)red[kPStats + 5];
+  st.chi2_kernelized = (float)red[kPStats + 6];
+  st.pert_pose_norm = 0.f;
+  st.pert_vel_norm = 0.f;
+  double H[144], b[12];
+  for (int a = 0; a < D; ++a) {
+    for (int c = 0; c < D; ++c) H[a * D + c] = Hf[a * Dk + c];
+    b[a] = bf[a];
+  }
+  if (kind == 2) {
+    for (int a = 0; a < 6; ++a) {
+      for (int c = 0; c < 6; ++c) {
+        O.H_vel_B[a * 6 + c] = Hf[(12 + a) * Dk + 12 + c];
+        O.H_cross_pose_vel_B[a * 6 + c] = Hf[a * Dk + 12 + c];
+        O.H_cross_vel_AB[a * 6 + c] = Hf[(6 + a) * Dk + 12 + c];
+      }
+      O.b_vel_B[a] = bf[12 + a];
+    }
+  }
+  const int it = S.iter;
+  if (Jn.mode != KDS_JOB_COMPUTE) {
+    for (int i = 0; i < D * D; ++i) O.H[i] = H[i];
+    for (int i = 0; i < D; ++i) O.b[i] = b[i];
+    O.stats = st;
+    O.result = 0;
+    O.iterations = 1;
+    S.done = 1;
+    return;
+  }
+  if (Jn.prior_enabled) {
+    double e6[6], Jp[6][6];
+    dpose_d(Jn.prior_ZXi, S.X, e6, Jp);
+    const double* Om = Jn.prior_info;
+    double OJ[6][6], Oe[6];
+    for (int i = 0; i < 6; ++i) {
+      for (int j = 0; j < 6; ++j) {
+        double a = 0;
+        for (int k = 0; k < 6; ++k) a += Om[i * 6 + k] * Jp[k][j];
+        OJ[i][j] = a;
+      }
+      double a = 0;
+      for (int k = 0; k < 6; ++k) a += Om[i * 6 + k] * e6[k];
+      Oe[i] = a;
+    }
+    for (int i = 0; i < 6; ++i) {
+      for (int j = 0; j < 6; ++j) {
+        double a = 0;
+        for (int k = 0; k < 6; ++k) a += Jp[k][i] * OJ[k][j];
+        H[i * D + j] += a;
+      }
+      double a = 0;
+      for (int k = 0; k < 6; ++k) a += Jp[k][i] * Oe[k];
+      b[i] += a;
+    }
+  }
+  for (int i = 0; i < D * D; ++i) O.H[i] = H[i];
+  for (int i = 0; i < D; ++i) O.b[i] = b[i];
+  O.iterations = it + 1;
+  if (st.num_inliers + st.num_outliers < Jn.P.min_good_measurements) {
+    if (log && it < kMaxLog) log[it] = st;
+    O.stats = st;
+    S.done = 1;
+    S.result = -it;
+    O.result = S.result;
+    return;
+  }
+  double A[144], rhs[12], dx[12];
+  for (int i = 0; i < D * D; ++i) A[i] = H[i];
+  for (int i = 0; i < D; ++i) {
+    A[i * D + i] += (i < 6) ? (double)Jn.P.damping : (double)Jn.P.velocity_damping;
+    rhs[i] = -b[i];
+  }
+  if (!ldlt_solve_d(D, A, rhs, dx))
+    for (int i = 0; i < D; ++i) dx[i] = 0.0;
+  double pp = 0.0, pv = 0.0;
+  for (int i = 0; i < 6; ++i) pp += dx[i] * dx[i];
+  st.pert_pose_norm = (float)sqrt(pp);
+  if (D == 12) {
+    for (int i = 6; i < 12; ++i) pv += dx[i] * dx[i];
+    st.pert_vel_norm = (float)sqrt(pv);
+  }
+  for (int i = 0; i < D; ++i) O.dx[i] = dx[i];
+  if (log && it < kMaxLog) log[it] = st;
+  O.stats = st;
+  if (!Jn.stats_mode) {
+    double dX[12], Xn[12];
+    expmap_d(dx, dX);
+    iso_mul_d(dX, S.X, Xn);
+    for (int i = 0; i < 12; ++i) S.X[i] = Xn[i];
+    if (D == 12)
+      for (int i = 0; i < 6; ++i) S.v[i] += dx[6 + i];
+  }
+  bool stop = false;
+  if (Jn.P.term_crit) {
+    // ICPTerminationCriteriaScore_::hasToStop (kd/icp/icp_stats_.h:91-101)
+    int nl = st.num_inliers + st.num_outliers + st.num_bad + st.num_err_normal + st.num_err_fn;
+    float ratio = nl ? (float)st.num_inliers / (float)nl : 0.f;
+    float score = ratio / (st.chi2_kernelized / (float)st.num_inliers + 1e-6f);
+    if (it > 0) {
+      bool pert_ok = st.pert_pose_norm < Jn.P.d_pert;
+      float dsc = score - S.prev_score;
+      bool score_ok = (dsc > 0.f) && ((double)dsc / ((double)S.prev_score + 1e-6) < (double)Jn.P.d_score);
+      if (pert_ok && score_ok) stop = true;
+    }
+    S.prev_score = score;
+  }
+  S.iter = it + 1;
+  if (stop) {
+    S.done = 1;
+    S.result = it;
+  } else if (S.iter >= S.max_iter) {
+    S.done = 1;
+    S.result = Jn.P.max_iterations;
+  }
+  O.result = S.result;
+  for (int i = 0; i < 12; ++i) O.X[i] = S.X[i];
+  for (int i = 0; i < 6; ++i) O.v[i] = S.v[i];
+  if (!S.done) refresh_caches(S, lins, Jn.lin_begin, Jn.lin_count);
+}
+
+// ---------------------------------------------------------------------------
+// The last block of a job: FP64 sum of the job's partials in tile order, then finalize.
+__device__ __noinline__ void job_tail(const JobIn& Jn, JobState& S, JobOut& O, kds_stats* log, LinDev* lins,
+                                      const double* partials, double* red, int M) {
+  for (int k = threadIdx.x; k < kPStride; k += blockDim.x) {
+    if (k >= M && k < kPStats) { red[k] = 0.0; continue; }
+    double acc = 0.0;
+    for (int t = Jn.tile_begin; t < Jn.tile_begin + Jn.tile_count; ++t) acc += __ldcg(partials + (size_t)t * kPStride + k);
+    red[k] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    finalize(Jn, S, O, log, lins, red);
+    S.arrive = 0u;
+  }
+}
+
+// One Gauss-Newton iteration over the tiles [tile0, tile0 + gridDim.x) of one kind.
+template <int KIND>
+__global__ void __launch_bounds__(kBlock, 4) k_linearize(const JobIn* __restrict__ jobs, JobState* states, JobOut* outs,
+                                                      kds_stats* logs, LinDev* lins, const TileDev* __restrict__ tiles,
+                                                      int tile0, double* partials, int32_t* dbg_match,
+                                                      int32_t* dbg_status) {
+  constexpr int D = KindDim<KIND>::D;
+  constexpr int M = D * (D + 1) / 2 + D;
+  __shared__ CacheF sC;
+  __shared__ float sfac[kWarps * 32 * kMaxFS];
+  __shared__ double swp[kWarps * kPStride];
+  __shared__ int s_last;
+  const int tile = tile0 + blockIdx.x;
+  const TileDev T = tiles[tile];
+  JobState& S = states[T.job];
+  if (*(volatile int32_t*)&S.done) return;
+  const JobIn& Jn = jobs[T.job];
+  const LinDev& L = lins[T.lin];
+  if (threadIdx.x < (int)(sizeof(CacheF) / 4))
+    reinterpret_cast<float*>(&sC)[threadIdx.x] = reinterpret_cast<const float*>(&L.cache)[threadIdx.x];
+  __syncthreads();
+  tile_body<KIND>(Jn, L, sC, T, swp, sfac, dbg_match, dbg_status);
+  __syncthreads();
+  double* P = partials + (size_t)tile * kPStride;
+  for (int k = threadIdx.x; k < kPStride; k += blockDim.x) {
+    if (k >= M && k < kPStats) continue;
+    double acc = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) acc += swp[w * kPStride + k];
+    P[k] = acc;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned prev = atomicAdd(&S.arrive, 1u);
+    s_last = (prev == (unsigned)(Jn.tile_count - 1)) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  job_tail(Jn, S, outs[T.job], logs ? logs + (size_t)T.job * kMaxLog : nullptr, lins, partials, swp, M);
+}
+
+// Resets control state, seeds state from the job inputs and writes the first caches.
+__global__ void k_init_jobs(const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins, int num_jobs) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= num_jobs) return;
+  const JobIn& Jn = jobs[j];
+  JobState& S = states[j];
+  for (int i = 0; i < 12; ++i) S.X[i] = Jn.X0[i];
+  for (int i = 0; i < 6; ++i) S.v[i] = Jn.v0[i];
+  S.iter = 0;
+  S.done = 0;
+  S.result = 0;
+  S.arrive = 0u;
+  S.prev_score = 0.f;
+  S.max_iter = Jn.stats_mode ? 1 : Jn.P.max_iterations;
+  JobOut& O = outs[j];
+  for (int i = 0; i < 12; ++i) O.X[i] = S.X[i];
+  for (int i = 0; i < 6; ++i) O.v[i] = S.v[i];
+  O.result = Jn.P.max_iterations;
+  O.iterations = 0;
+  if (Jn.tile_count == 0 || S.max_iter <= 0) {
+    // no moving leaves: the round sees zero measurements and fails at iteration 0
+    kds_stats z;
+    memset(&z, 0, sizeof(z));
+    O.stats = z;
+    for (int i = 0; i < 144; ++i) O.H[i] = 0.0;
+    for (int i = 0; i < 12; ++i) { O.b[i] = 0.0; O.dx[i] = 0.0; }
+    S.done = 1;
+    O.result = (Jn.mode == KDS_JOB_COMPUTE && S.max_iter > 0 && Jn.P.min_good_measurements > 0) ? 0
+                                                                                                  : Jn.P.max_iterations;
+    if (Jn.mode != KDS_JOB_COMPUTE) O.result = 0;
+    return;
+  }
+  if (!Jn.keep_cache) refresh_caches(S, lins, Jn.lin_begin, Jn.lin_count);
+}
+
+// ---------------------------------------------------------------------------
+// Host runner
+int Runner::reserve(int nj, int nl, int nt) {
+  if (nj <= cap_jobs && nl <= cap_lins && nt <= cap_tiles) return KDS_OK;
+  release();
+  cap_jobs = std::max(nj, 1);
+  cap_lins = std::max(nl, 1);
+  cap_tiles = std::max(nt, 1);
+  size_t bytes = sizeof(JobIn) * cap_jobs + sizeof(JobState) * cap_jobs + sizeof(JobOut) * cap_jobs +
+                 sizeof(kds_stats) * kMaxLog * cap_jobs + sizeof(LinDev) * cap_lins + sizeof(TileDev) * cap_tiles +
+                 sizeof(double) * kPStride * cap_tiles + 8 * 256;
+  cudaError_t e = cudaMalloc(&block, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    block = nullptr;
+    cap_jobs = cap_lins = cap_tiles = 0;
+    set_error("cudaMalloc of %zu bytes for the aligner workspace failed", bytes);
+    return KDS_ERR_OOM;
+  }
+  char* p = (char*)block;
+  auto carve = [&](size_t sz) {
+    char* r = p;
+    p += (sz + 255) & ~(size_t)255;
+    return (void*)r;
+  };
+  d_jobs = (JobIn*)carve(sizeof(JobIn) * cap_jobs);
+  d_states = (JobState*)carve(sizeof(JobState) * cap_jobs);
+  d_outs = (JobOut*)carve(sizeof(JobOut) * cap_jobs);
+  d_logs = (kds_stats*)carve(sizeof(kds_stats) * kMaxLog * cap_jobs);
+  d_lins = (LinDev*)carve(sizeof(LinDev) * cap_lins);
+  d_tiles = (TileDev*)carve(sizeof(TileDev) * cap_tiles);
+  d_partials = (double*)carve(sizeof(double) * kPStride * cap_tiles);
+  return KDS_OK;
+}
+
+void Runner::release() {
+  drop_graph();
+  if (block) cudaFree(block);
+  block = nullptr;
+  cap_jobs = cap_lins = cap_tiles = 0;
+}
+
+void Runner::drop_graph() {
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (graph) cudaGraphDestroy(graph);
+  gexec = nullptr;
+  graph = nullptr;
+  graph_key.clear();
+}
+
+// Builds the tile list and device inputs for `jobs` (host descriptions).
+int Runner::setup(const std::vector<JobIn>& jobs_in, const std::vector<LinDev>& lins_in, cudaStream_t s) {
+  h_jobs = jobs_in;
+  h_lins = lins_in;
+  h_tiles.clear();
+  for (int kind = 0; kind < 3; ++kind) {
+    kind_begin[kind] = (int)h_tiles.size();
+    for (size_t j = 0; j < h_jobs.size(); ++j) {
+      JobIn& Jn = h_jobs[j];
+      if (Jn.kind != kind) continue;
+      Jn.tile_begin = (int32_t)h_tiles.size();
+      for (int l = Jn.lin_begin; l < Jn.lin_begin + Jn.lin_count; ++l) {
+        for (int b = 0; b < Jn.m_num_leaves; b += kBlock) {
+          TileDev t;
+          t.job = (int32_t)j;
+          t.lin = l;
+          t.leaf_begin = b;
+          t.leaf_end = std::min(b + kBlock, Jn.m_num_leaves);
+          h_tiles.push_back(t);
+        }
+      }
+      Jn.tile_count = (int32_t)h_tiles.size() - Jn.tile_begin;
+    }
+    kind_count[kind] = (int)h_tiles.size() - kind_begin[kind];
+  }
+  int rc = reserve((int)h_jobs.size(), (int)h_lins.size(), (int)h_tiles.size());
+  if (rc) return rc;
+  num_jobs = (int)h_jobs.size();
+  num_tiles = (int)h_tiles.size();
+  KDS_CK(cudaMemcpyAsync(d_jobs, h_jobs.data(), sizeof(JobIn) * h_jobs.size(), cudaMemcpyHostToDevice, s));
+  KDS_CK(cudaMemcpyAsync(d_lins, h_lins.data(), sizeof(LinDev) * h_lins.size(), cudaMemcpyHostToDevice, s));
+  if (num_tiles)
+    KDS_CK(cudaMemcpyAsync(d_tiles, h_tiles.data(), sizeof(TileDev) * h_tiles.size(), cudaMemcpyHostToDevice, s));
+  return KDS_OK;
+}
+
+int Runner::max_launches() const {
+  int m = 0;
+  for (const JobIn& J : h_jobs) {
+    int it = (J.mode == KDS_JOB_COMPUTE) ? (J.stats_mode ? 1 : J.P.max_iterations) : 1;
+    m = std::max(m, it);
+  }
+  return m;
+}
+
+int Runner::enqueue(cudaStream_t s, int32_t* dbg_match, int32_t* dbg_status) {
+  if (num_jobs == 0) return KDS_OK;
+  k_init_jobs<<<(num_jobs + 127) / 128, 128, 0, s>>>(d_jobs, d_states, d_outs, d_lins, num_jobs);
+  int L = max_launches();
+  for (int i = 0; i < L; ++i) {
+    if (kind_count[0])
+      k_linearize<0><<<kind_count[0], kBlock, 0, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
+                                                      kind_begin[0], d_partials, dbg_match, dbg_status);
+    if (kind_count[1])
+      k_linearize<1><<<kind_count[1], kBlock, 0, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
+                                                      kind_begin[1], d_partials, dbg_match, dbg_status);
+    if (kind_count[2])
+      k_linearize<2><<<kind_count[2], kBlock, 0, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
+                                                      kind_begin[2], d_partials, dbg_match, dbg_status);
+  }
+  KDS_CK(cudaGetLastError());
+  return KDS_OK;
+}
+
+int Runner::run(cudaStream_t s, bool use_graph, int32_t* dbg_match, int32_t* dbg_status) {
+  if (!use_graph || dbg_match) return enqueue(s, dbg_match, dbg_status);
+  // graph key: everything the captured launches depend on
+  std::vector<int64_t> key;
+  key.push_back((int64_t)(uintptr_t)block);
+  key.push_back(num_jobs);
+  key.push_back(num_tiles);
+  key.push_back(max_launches());
+  for (int k = 0; k < 3; ++k) { key.push_back(kind_begin[k]); key.push_back(kind_count[k]); }
+  if (key != graph_key) {
+    drop_graph();
+    cudaStream_t cs;
+    KDS_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    int rc = KDS_OK;
+    if (e == cudaSuccess) {
+      rc = enqueue(cs, nullptr, nullptr);
+      e = cudaStreamEndCapture(cs, &graph);
+    }
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess || rc) {
+      graph = nullptr;
+      return rc ? rc : cuda_status(e, "graph capture", __FILE__, __LINE__);
+    }
+    KDS_CK(cudaGraphInstantiate(&gexec, graph, 0));
+    graph_key = key;
+  }
+  KDS_CK(cudaGraphLaunch(gexec, s));
+  return KDS_OK;
+}
+
+int Runner::fetch(cudaStream_t s, std::vector<JobOut>& outs, std::vector<kds_stats>* logs) {
+  outs.resize(num_jobs);
+  if (num_jobs == 0) return KDS_OK;
+  KDS_CK(cudaMemcpyAsync(outs.data(), d_outs, sizeof(JobOut) * num_jobs, cudaMemcpyDeviceToHost, s));
+  if (logs) {
+    logs->resize((size_t)num_jobs * kMaxLog);
+    KDS_CK(cudaMemcpyAsync(logs->data(), d_logs, sizeof(kds_stats) * kMaxLog * num_jobs, cudaMemcpyDeviceToHost, s));
+  }
+  KDS_CK(cudaStreamSynchronize(s));
+  return KDS_OK;
+}
+
+}  // namespace kds

@@ -1,0 +1,127 @@
+// Device-side job layout of the fused linearization kernel and its host runner.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "kds_internal.cuh"
+
+namespace kds {
+
+constexpr int kMaxLog = 64;      // per-job stats_log depth
+constexpr int kPStride = 200;    // doubles per tile partial: 189 entries (D = 18) + stats
+constexpr int kPStats = 192;     // offset of the 7 stats values inside a partial
+
+// Per-iteration float view of the state for one (job, fixed entry) pair: the
+// QuadraticTermCache of kd/icp/icp_.h:97-102 plus the velocities.
+struct CacheF {
+  float Xm[12];
+  float Xf[12];
+  float Xmf[12];
+  float v[6];
+  float fv[6];
+};
+
+struct ParamsF {
+  float kernel_threshold;
+  float damping;
+  float max_error;
+  float min_normal_cos;
+  int32_t min_good_measurements;
+  int32_t max_iterations;
+  float velocity_damping;
+  int32_t term_crit;
+  float d_pert;
+  float d_score;
+};
+
+// One fixed entry of a job (the FixedEntry of kd/icp/tree_aligner_base_.h:57-74).
+struct LinDev {
+  const DNode* fnodes;
+  const float* fdts;
+  int32_t f_num_nodes;
+  int32_t job;
+  double Xf[12];
+  double fv[6];
+  CacheF cache;  // written on the device
+};
+
+struct JobIn {
+  const float4* m_md;
+  const float4* m_nrm;
+  int32_t m_num_leaves;
+  int32_t kind;  // 0 ICP, 1 CT, 2 CT dual
+  int32_t mode;  // KDS_JOB_*
+  int32_t stats_mode;
+  int32_t lin_begin, lin_count;
+  int32_t tile_begin, tile_count;
+  ParamsF P;
+  int32_t prior_enabled;
+  int32_t keep_cache;  // 1: use the caches already in LinDev (explicit-cache linearization)
+  double prior_ZXi[12];
+  double prior_info[36];
+  double X0[12];
+  double v0[6];
+};
+
+struct JobState {
+  double X[12];
+  double v[6];
+  int32_t iter, done, result, max_iter;
+  unsigned int arrive;
+  float prev_score;
+};
+
+struct JobOut {
+  double X[12];
+  double v[6];
+  int32_t result;
+  int32_t iterations;
+  kds_stats stats;
+  double H[144];
+  double b[12];
+  double dx[12];
+  double H_vel_B[36], b_vel_B[6], H_cross_pose_vel_B[36], H_cross_vel_AB[36];
+};
+
+struct TileDev {
+  int32_t job;
+  int32_t lin;
+  int32_t leaf_begin;
+  int32_t leaf_end;
+};
+
+// Owns the device buffers of a batch of jobs and (optionally) a CUDA graph of its
+// launches: k_init_jobs followed by one k_linearize per Gauss-Newton iteration.
+struct Runner {
+  void* block = nullptr;
+  int cap_jobs = 0, cap_lins = 0, cap_tiles = 0;
+  JobIn* d_jobs = nullptr;
+  JobState* d_states = nullptr;
+  JobOut* d_outs = nullptr;
+  kds_stats* d_logs = nullptr;
+  LinDev* d_lins = nullptr;
+  TileDev* d_tiles = nullptr;
+  double* d_partials = nullptr;  // scratch: one kPStride partial per tile
+  std::vector<JobIn> h_jobs;
+  std::vector<LinDev> h_lins;
+  std::vector<TileDev> h_tiles;
+  int num_jobs = 0, num_tiles = 0;
+  int kind_begin[3] = {0, 0, 0}, kind_count[3] = {0, 0, 0};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<int64_t> graph_key;
+
+  int reserve(int nj, int nl, int nt);
+  void release();
+  void drop_graph();
+  int setup(const std::vector<JobIn>& jobs, const std::vector<LinDev>& lins, cudaStream_t s);
+  int max_launches() const;
+  int enqueue(cudaStream_t s, int32_t* dbg_match, int32_t* dbg_status);
+  int run(cudaStream_t s, bool use_graph, int32_t* dbg_match, int32_t* dbg_status);
+  int fetch(cudaStream_t s, std::vector<JobOut>& outs, std::vector<kds_stats>* logs);
+  ~Runner() { release(); }
+};
+
+}  // namespace kds

@@ -1,0 +1,248 @@
+"""ctypes binding of the CPU oracle (liborc.so) -- TEST INFRASTRUCTURE ONLY.
+
+Imported by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg, always
+as the checker or the timed CPU baseline, never as part of the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liborc.so")
+
+MODE_REF32, MODE_MIXED, MODE_FP64 = 0, 1, 2
+KIND_ICP, KIND_CT, KIND_CT_DUAL = 0, 1, 2
+
+
+class TreeParams(C.Structure):
+    _fields_ = [("propagate_normal", C.c_int32), ("tree_min_good_leaves", C.c_int32),
+                ("leaf_min_points", C.c_int32), ("leaf_max_points", C.c_int32), ("leaf_density", C.c_float),
+                ("leaf_min_normal_incidence", C.c_float), ("leaf_eigenvalue_threshold", C.c_float),
+                ("leaf_normal_eigenratio", C.c_float), ("prune_min_normal_incidence", C.c_float),
+                ("max_level", C.c_int32)]
+
+
+class AlignParams(C.Structure):
+    _fields_ = [("kernel_threshold", C.c_float), ("damping", C.c_float), ("max_error", C.c_float),
+                ("min_normal_cos", C.c_float), ("min_good_measurements", C.c_int32), ("max_iterations", C.c_int32),
+                ("velocity_damping", C.c_float), ("term_crit", C.c_int32), ("d_pert", C.c_float),
+                ("d_score", C.c_float)]
+
+
+class OStats(C.Structure):
+    _fields_ = [("num_inliers", C.c_int32), ("num_outliers", C.c_int32), ("num_bad", C.c_int32),
+                ("num_err_normal", C.c_int32), ("num_err_fn", C.c_int32), ("chi2", C.c_float),
+                ("chi2_kernelized", C.c_float), ("pert_pose_norm", C.c_float), ("pert_vel_norm", C.c_float)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class OPrior(C.Structure):
+    _fields_ = [("enabled", C.c_int32), ("X_ref", C.c_double * 12), ("Z", C.c_double * 12),
+                ("info", C.c_double * 36)]
+
+
+class OResult(C.Structure):
+    _fields_ = [("ret", C.c_int32), ("iterations", C.c_int32), ("H", C.c_double * 144), ("b", C.c_double * 12),
+                ("dx", C.c_double * 12), ("stats", OStats), ("log", OStats * 64)]
+
+
+def tree_params(**kw) -> TreeParams:
+    p = TreeParams(0, 10, 5, 30, 100.0, 0.1, 1e-3, 0.1, 0.1, 48)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def align_params(**kw) -> AlignParams:
+    p = AlignParams(0.1, 1.0, 1.0, float(np.float32(np.cos(25.0 / 180.0 * np.pi))), 10, 20, 100.0, 0, 1e-3, 1e-3)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+_LIB = None
+
+
+def load() -> C.CDLL:
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
+    lib = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    sig = {
+        "orc_tree_build": (P, [P, P, C.c_int64, C.POINTER(TreeParams)]),
+        "orc_tree_from_nodes": (P, [P, P, P, P, P, C.c_int64]),
+        "orc_tree_num_nodes": (C.c_int64, [P]),
+        "orc_tree_num_leaves": (C.c_int64, [P]),
+        "orc_tree_num_points": (C.c_int64, [P]),
+        "orc_tree_num_unpruned": (C.c_int64, [P]),
+        "orc_tree_accepted": (C.c_int32, [P]),
+        "orc_tree_ts_start": (C.c_double, [P]),
+        "orc_tree_export": (None, [P] * 12),
+        "orc_tree_free": (None, [P]),
+        "orc_align": (C.c_int32, [C.c_int32, C.c_int32, P, P, C.c_int32, P, C.POINTER(AlignParams),
+                                  C.POINTER(OPrior), P, P, P, C.c_int32, C.c_int32, C.POINTER(OResult)]),
+        "orc_linearize": (None, [C.c_int32, P, P, P, P, P, C.POINTER(AlignParams), C.c_int32, P, P, P, P,
+                                 C.POINTER(OStats)]),
+        "orc_sincosf": (None, [C.c_float, P, P]),
+        "orc_err_jac_vel_A": (None, [C.c_int32, P, P, P, P, P, P, P, P, C.c_double]),
+        "orc_err_jac_vel_B": (None, [C.c_int32, P, P, P, P, P, P, P, P, C.c_double]),
+        "orc_pose_to_pose_error": (None, [C.c_int32, P, P, P]),
+        "orc_dpose_to_pose_error": (None, [C.c_int32, P, P, P]),
+        "orc_expmap": (None, [C.c_int32, P, P]),
+        "orc_iso_mul": (None, [P, P, P]),
+        "orc_jacobi3": (None, [P, P, P]),
+        "orc_warp_leaf": (None, [P, C.c_float, P, P, P, P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _LIB = lib
+    return lib
+
+
+class OTree:
+    """Oracle tree handle (canonical build or a node array)."""
+
+    def __init__(self, h):
+        self.h = h
+
+    def __del__(self):
+        if self.h:
+            load().orc_tree_free(self.h)
+            self.h = None
+
+    @staticmethod
+    def build(xyz, stamps=None, params: TreeParams | None = None) -> "OTree":
+        lib = load()
+        xyz = np.ascontiguousarray(xyz, np.float32)
+        st = None if stamps is None else np.ascontiguousarray(stamps, np.float64)
+        p = params or tree_params()
+        h = lib.orc_tree_build(xyz.ctypes.data, None if st is None else st.ctypes.data, len(xyz), C.byref(p))
+        return OTree(h)
+
+    @staticmethod
+    def from_nodes(mean, dir, dts_mean, left, right) -> "OTree":
+        lib = load()
+        mean = np.ascontiguousarray(mean, np.float32)
+        dir = np.ascontiguousarray(dir, np.float32)
+        dm = np.ascontiguousarray(dts_mean, np.float64)
+        left = np.ascontiguousarray(left, np.int32)
+        right = np.ascontiguousarray(right, np.int32)
+        return OTree(lib.orc_tree_from_nodes(mean.ctypes.data, dir.ctypes.data, dm.ctypes.data, left.ctypes.data,
+                                             right.ctypes.data, len(mean)))
+
+    @property
+    def num_nodes(self) -> int:
+        return load().orc_tree_num_nodes(self.h)
+
+    @property
+    def num_leaves(self) -> int:
+        return load().orc_tree_num_leaves(self.h)
+
+    @property
+    def accepted(self) -> bool:
+        return bool(load().orc_tree_accepted(self.h))
+
+    def export(self) -> dict:
+        lib = load()
+        n, nl, npnt = self.num_nodes, self.num_leaves, lib.orc_tree_num_points(self.h)
+        out = {"mean": np.zeros((n, 3), np.float32), "dir": np.zeros((n, 3), np.float32),
+               "dts_mean": np.zeros(n), "dts_cov": np.zeros(n), "start": np.zeros(n, np.int64),
+               "end": np.zeros(n, np.int64), "left": np.zeros(n, np.int32), "right": np.zeros(n, np.int32),
+               "level": np.zeros(n, np.int32), "leaves": np.zeros(nl, np.int64), "perm": np.zeros(npnt, np.int64)}
+        lib.orc_tree_export(self.h, *(out[k].ctypes.data for k in ("mean", "dir", "dts_mean", "dts_cov", "start",
+                                                                    "end", "left", "right", "level", "leaves",
+                                                                    "perm")))
+        out["ts_start"] = lib.orc_tree_ts_start(self.h)
+        out["num_unpruned"] = lib.orc_tree_num_unpruned(self.h)
+        out["accepted"] = self.accepted
+        return out
+
+
+def align(kind: int, mode: int, fixed, moving: OTree, params: AlignParams, X0, v0=None, fixed_X=None,
+          fixed_v=None, prior=None, stats_mode: bool = False, num_threads: int = 1):
+    """Runs TreeAlignerBase_::compute.  fixed: OTree or list of (OTree, X) entries."""
+    lib = load()
+    if isinstance(fixed, OTree):
+        fixed = [(fixed, np.eye(3, 4) if fixed_X is None else fixed_X)]
+    hs = (C.c_void_p * len(fixed))(*[f.h for f, _ in fixed])
+    FX = np.ascontiguousarray(np.stack([np.asarray(x, np.float64).reshape(12) for _, x in fixed]))
+    X = np.ascontiguousarray(np.asarray(X0, np.float64).reshape(12)).copy()
+    v = np.zeros(6) if v0 is None else np.ascontiguousarray(v0, np.float64).copy()
+    fv = np.zeros(6) if fixed_v is None else np.ascontiguousarray(fixed_v, np.float64)
+    res = OResult()
+    pr = None
+    if prior is not None:
+        pr = OPrior()
+        pr.enabled = 1
+        pr.X_ref[:] = list(np.asarray(prior[0], np.float64).reshape(12))
+        pr.Z[:] = list(np.asarray(prior[1], np.float64).reshape(12))
+        pr.info[:] = list(np.asarray(prior[2], np.float64).reshape(36))
+    ret = lib.orc_align(kind, mode, hs, FX.ctypes.data, len(fixed), moving.h, C.byref(params),
+                        C.byref(pr) if pr is not None else None, X.ctypes.data, v.ctypes.data, fv.ctypes.data,
+                        1 if stats_mode else 0, num_threads, C.byref(res))
+    D = 6 if kind == KIND_ICP else 12
+    return {"ret": ret, "X": X.reshape(3, 4), "v": v, "iterations": res.iterations,
+            "H": np.array(res.H[:D * D]).reshape(D, D), "b": np.array(res.b[:D]), "dx": np.array(res.dx[:D]),
+            "stats": res.stats.as_dict(), "log": [res.log[i].as_dict() for i in range(min(res.iterations, 64))]}
+
+
+def linearize(kind: int, fixed: OTree, moving: OTree, caches36, params: AlignParams, v=None, fixed_v=None,
+              stats_mode: bool = False):
+    lib = load()
+    n = moving.num_leaves
+    c = np.ascontiguousarray(caches36, np.float32)
+    vv = np.zeros(6, np.float32) if v is None else np.ascontiguousarray(v, np.float32)
+    fv = np.zeros(6, np.float32) if fixed_v is None else np.ascontiguousarray(fixed_v, np.float32)
+    match = np.zeros(n, np.int32)
+    status = np.zeros(n, np.int32)
+    D = {KIND_ICP: 6, KIND_CT: 12, KIND_CT_DUAL: 18}[kind]
+    H = np.zeros(D * D)
+    b = np.zeros(D)
+    st = OStats()
+    lib.orc_linearize(kind, fixed.h, moving.h, c.ctypes.data, vv.ctypes.data, fv.ctypes.data, C.byref(params),
+                      1 if stats_mode else 0, match.ctypes.data, status.ctypes.data, H.ctypes.data, b.ctypes.data,
+                      C.byref(st))
+    return match, status, H.reshape(D, D), b, st.as_dict()
+
+
+def sincosf(x: float):
+    s, c = C.c_float(), C.c_float()
+    load().orc_sincosf(x, C.byref(s), C.byref(c))
+    return s.value, c.value
+
+
+def caches_from(X, Xf=None) -> np.ndarray:
+    """Float caches Xm, Xf, Xmf computed in double and rounded, as the product does."""
+    X = np.asarray(X, np.float64).reshape(3, 4)
+    Xf = np.eye(3, 4) if Xf is None else np.asarray(Xf, np.float64).reshape(3, 4)
+    R, t = Xf[:, :3], Xf[:, 3]
+    iXf = np.zeros((3, 4))
+    iXf[:, :3] = R.T
+    iXf[:, 3] = -(R.T @ t)
+    Xmf = np.zeros((3, 4))
+    Xmf[:, :3] = iXf[:, :3] @ X[:, :3]
+    Xmf[:, 3] = iXf[:, :3] @ X[:, 3] + iXf[:, 3]
+    return np.concatenate([X.reshape(12), Xf.reshape(12), Xmf.reshape(12)]).astype(np.float32)
+
+
+def warp_leaf(v6, dt, m, n):
+    lib = load()
+    v = np.ascontiguousarray(v6, np.float32)
+    m = np.ascontiguousarray(m, np.float32)
+    n = np.ascontiguousarray(n, np.float32)
+    mo = np.zeros(3, np.float32)
+    no = np.zeros(3, np.float32)
+    lib.orc_warp_leaf(v.ctypes.data, float(np.float32(dt)), m.ctypes.data, n.ctypes.data, mo.ctypes.data,
+                      no.ctypes.data)
+    return mo, no

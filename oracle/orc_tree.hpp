@@ -1,0 +1,47 @@
+// CPU oracle types -- TEST INFRASTRUCTURE ONLY (see orc_math.hpp for the parity status).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace orc {
+
+// TreeGenerator_ PARAMs (kd/tree/tree_generator_.h:18-25) plus the fixed prune incidence
+// of the default-constructed IsGoodLeafPredicate_ (kd/tree/tree_predicates_.h:15).
+struct TreeParams {
+  int32_t propagate_normal;
+  int32_t tree_min_good_leaves;
+  int32_t leaf_min_points;
+  int32_t leaf_max_points;
+  float leaf_density;
+  float leaf_min_normal_incidence;
+  float leaf_eigenvalue_threshold;  // read by the reference, never used
+  float leaf_normal_eigenratio;
+  float prune_min_normal_incidence;
+  int32_t max_level;
+};
+
+// Node_ (kd/tree/node_.h:18-48)
+struct Node {
+  float mean[3];
+  float dir[3];
+  double dts_mean;
+  double dts_cov;
+  int64_t start, end;
+  int32_t left, right;
+};
+
+struct Tree {
+  std::vector<Node> nodes;       // BFS order after prune
+  std::vector<int32_t> levels;   // depth of each node
+  std::vector<int64_t> leaves;   // leaf node indices, BFS order
+  std::vector<int64_t> perm;     // final point order: perm[i] = input index at position i
+  double ts_start = 0.0;
+  int64_t num_points = 0;
+  int64_t num_unpruned = 0;
+  bool accepted = false;
+};
+
+Tree build_tree(const float* xyz, const double* stamps, int64_t n, const TreeParams& P);
+void jacobi3(const double A[3][3], double ev[3], double V[3][3]);
+
+}  // namespace orc

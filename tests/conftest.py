@@ -1,0 +1,61 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the product kernels")
+
+
+def gpu_available() -> bool:
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def pytest_collection_modifyitems(config, items):
+    if gpu_available():
+        return
+    skip = pytest.mark.skip(reason="no CUDA device")
+    for it in items:
+        if "gpu" in it.keywords:
+            it.add_marker(skip)
+
+
+# ---------------------------------------------------------------- shared inputs
+@pytest.fixture(scope="session")
+def scene():
+    from kd_slam2_b200 import synth
+    return synth.scene(1001)
+
+
+def make_scan(boxes, seed, beams=16, cols=1024, elev=(-15.0, 15.0), pose=None, vel=None, noise=0.02):
+    from kd_slam2_b200 import synth
+    P = synth.pose((0.0, 0.0, 1.8)) if pose is None else pose
+    return synth.scan(boxes, P, vel=vel, beams=beams, cols=cols, elev=elev, seed=seed, noise=noise)
+
+
+def perturbation(rng, t_max=0.2, r_deg=2.0):
+    from kd_slam2_b200 import synth
+    d = rng.normal(size=3)
+    d /= np.linalg.norm(d)
+    a = rng.normal(size=3)
+    a /= np.linalg.norm(a)
+    return synth.pose(t_max * d, np.deg2rad(r_deg) * a)
+
+
+def pose_err(A, B):
+    """translation (m) and rotation (rad) difference of two 3x4 poses"""
+    A = np.asarray(A, np.float64).reshape(3, 4)
+    B = np.asarray(B, np.float64).reshape(3, 4)
+    dR = A[:, :3].T @ B[:, :3]
+    c = np.clip((np.trace(dR) - 1) / 2, -1, 1)
+    return float(np.linalg.norm(A[:, 3] - B[:, 3])), float(np.arccos(c))

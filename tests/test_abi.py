@@ -1,0 +1,72 @@
+"""The drop-in boundary: libkds.so loads without a GPU and exports every entry point
+declared in include/kds.h; the ctypes struct mirrors have the header's layout."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if not h.endswith(".h"):
+            continue
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(kds_\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    from kd_slam2_b200 import abi as _lib
+    lib = C.CDLL(_lib.LIB_PATH)
+    names = declared_functions()
+    assert len(names) >= 40
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # and every declared function has a ctypes signature in the binding
+    assert set(names) <= set(_lib.SIGNATURES), set(names) - set(_lib.SIGNATURES)
+
+
+def test_struct_layouts():
+    from kd_slam2_b200 import abi as L
+    assert C.sizeof(L.TreeParams) == 40
+    assert C.sizeof(L.AlignerParams) == 40
+    assert C.sizeof(L.Stats) == 36
+    # kds_job: 4 ints, 2 pointers, params, 36 doubles, 2 ints, stats, 144+12+36+6+36+36 doubles
+    assert L.Job.X.offset == 4 * 4 + 2 * 8 + 40
+    assert L.Job.result.offset == L.Job.X.offset + 36 * 8
+    assert L.Job.H.offset % 8 == 0
+
+
+def test_defaults_match_reference_params():
+    from kd_slam2_b200 import tree_params, aligner_params
+    import math
+    tp = tree_params()
+    # TreeGenerator_ PARAM defaults, kd/tree/tree_generator_.h:18-25
+    assert (tp.propagate_normal, tp.tree_min_good_leaves, tp.leaf_min_points, tp.leaf_max_points) == (0, 10, 5, 30)
+    assert tp.leaf_density == pytest.approx(100.0)
+    assert tp.leaf_min_normal_incidence == pytest.approx(0.1)
+    assert tp.leaf_normal_eigenratio == pytest.approx(0.1)
+    ap = aligner_params()
+    # TreeAlignerBase_ PARAM defaults, kd/icp/tree_aligner_base_.h:39-47; CT velocity_damping kd/cticp/cticp_.h:61
+    assert ap.kernel_threshold == pytest.approx(0.1)
+    assert ap.damping == pytest.approx(1.0)
+    assert ap.max_error == pytest.approx(1.0)
+    assert ap.min_normal_cos == pytest.approx(math.cos(25 / 180 * math.pi), rel=1e-7)
+    assert (ap.min_good_measurements, ap.max_iterations, ap.term_crit) == (10, 20, 0)
+    assert ap.velocity_damping == pytest.approx(100.0)
+
+
+def test_calls_without_a_device_fail_with_a_status_not_a_crash():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("device present")
+    from kd_slam2_b200 import abi as L, lib
+    h = C.c_void_p()
+    rc = lib().kds_aligner_create(0, None, C.byref(h))
+    assert rc == L.KDS_ERR_NO_DEVICE
+    assert b"device" in lib().kds_last_error()

@@ -1,0 +1,141 @@
+"""GPU tree build against the oracle: bit-exact node arrays, leaf lists and point order."""
+import numpy as np
+import pytest
+
+from conftest import make_scan
+from oracle import orc
+
+pytestmark = pytest.mark.gpu
+
+
+def build_both(xyz, st, **params):
+    import kd_slam2_b200 as kds
+    O = orc.OTree.build(xyz, st, orc.tree_params(**params))
+    G = kds.TreeGeneratorB2003D(**params).make_tree(xyz, st)
+    return O, G
+
+
+def assert_same_tree(O, G):
+    eo, eg = O.export(), G.export()
+    assert len(eo["mean"]) == len(eg["mean"])
+    for k in ("left", "right", "level", "start", "end", "leaves", "perm"):
+        assert np.array_equal(eo[k], eg[k]), k
+    for k in ("mean", "dir"):
+        assert np.array_equal(eo[k].view(np.uint32), eg[k].view(np.uint32)), k
+    for k in ("dts_mean", "dts_cov"):
+        assert np.array_equal(eo[k].view(np.uint64), eg[k].view(np.uint64)), k
+    assert eo["ts_start"] == eg["ts_start"]
+    assert G.info.num_unpruned == eo["num_unpruned"]
+
+
+@pytest.mark.parametrize("seed,beams,params", [
+    (2000, 16, dict(leaf_max_points=16)),
+    (2001, 16, dict(leaf_max_points=16, propagate_normal=1)),
+    (2002, 32, dict()),
+    (2003, 64, dict(leaf_max_points=16)),  # 65k points: large-node path
+    (2004, 16, dict(leaf_max_points=100, leaf_min_points=5, leaf_min_normal_incidence=0.2, propagate_normal=1,
+                    tree_min_good_leaves=50)),
+])
+def test_tree_build_bit_exact(scene, seed, beams, params):
+    xyz, st = make_scan(scene, seed, beams=beams, elev=(-15.0, 15.0) if beams <= 32 else (-22.5, 22.5))
+    O, G = build_both(xyz, st, **params)
+    assert O.accepted and G is not None
+    assert_same_tree(O, G)
+
+
+def test_tree_build_skewed_scan_with_stamps(scene):
+    from kd_slam2_b200 import synth
+    xyz, st = make_scan(scene, 2010, beams=32, vel=[10.0, 0, 0, 0, 0, np.deg2rad(30.0)])
+    st = st + 1234.5  # absolute stamps: dts relative to the first point
+    O, G = build_both(xyz, st, leaf_max_points=16)
+    assert_same_tree(O, G)
+
+
+def test_tree_without_stamps(scene):
+    xyz, _ = make_scan(scene, 2011)
+    O, G = build_both(xyz, None, leaf_max_points=16)
+    assert_same_tree(O, G)
+
+
+def test_rejected_trees_match_makeTree_nullptr(scene):
+    import kd_slam2_b200 as kds
+    # fewer points than leaf_min_points
+    xyz = np.zeros((3, 3), np.float32)
+    assert kds.TreeGeneratorB2003D().make_tree(xyz) is None
+    # a tiny patch: too few good leaves for tree_min_good_leaves
+    rng = np.random.default_rng(0)
+    xyz = (rng.normal(size=(200, 3)) * [1.0, 1.0, 0.01] + [10.0, 0, 0]).astype(np.float32)
+    O = orc.OTree.build(xyz, None, orc.tree_params(tree_min_good_leaves=50))
+    G = kds.TreeGeneratorB2003D(tree_min_good_leaves=50).make_tree(xyz)
+    assert not O.accepted and G is None
+
+
+def test_degenerate_inputs(scene):
+    """duplicated points and collinear runs: deterministic, same as the oracle"""
+    xyz, st = make_scan(scene, 2012)
+    dup = np.concatenate([xyz, xyz[:3000], np.repeat(xyz[:5], 40, axis=0)]).astype(np.float32)
+    std = np.concatenate([st, st[:3000], np.repeat(st[:5], 40)])
+    line = np.stack([np.linspace(5, 15, 500), np.full(500, 3.0), np.full(500, 0.5)], 1).astype(np.float32)
+    allp = np.concatenate([dup, line]).astype(np.float32)
+    alls = np.concatenate([std, np.zeros(500)])
+    O, G = build_both(allp, alls, leaf_max_points=16)
+    assert_same_tree(O, G)
+
+
+def test_out_of_range_input_is_rejected_with_status():
+    import kd_slam2_b200 as kds
+    xyz = np.zeros((100, 3), np.float32)
+    xyz[5] = [1e6, 0, 0]
+    with pytest.raises(kds.KdsError) as ei:
+        kds.TreeGeneratorB2003D().make_tree(xyz)
+    assert ei.value.code == kds.abi.KDS_ERR_RANGE
+
+
+def test_import_export_roundtrip(scene):
+    import kd_slam2_b200 as kds
+    xyz, st = make_scan(scene, 2013)
+    O = orc.OTree.build(xyz, st, orc.tree_params(leaf_max_points=16))
+    e = O.export()
+    T = kds.Tree.import_nodes(e["mean"], e["dir"], e["left"], e["right"], e["dts_mean"], e["dts_cov"], e["start"],
+                              e["end"], ts_start=e["ts_start"])
+    g = T.export()
+    for k in ("mean", "dir", "left", "right", "dts_mean", "dts_cov", "start", "end", "leaves"):
+        assert np.array_equal(e[k], g[k]), k
+    # malformed: child index pointing backwards
+    bad = e["left"].copy()
+    bad[5] = 1
+    with pytest.raises(kds.KdsError) as ei:
+        kds.Tree.import_nodes(e["mean"], e["dir"], bad, e["right"])
+    assert ei.value.code == kds.abi.KDS_ERR_BAD_TREE
+
+
+def test_morph_and_isometry_match_oracle(scene):
+    import kd_slam2_b200 as kds
+    xyz, st = make_scan(scene, 2014, vel=[5.0, 0.5, 0, 0.01, 0, 0.4])
+    G = kds.TreeGeneratorB2003D(leaf_max_points=16).make_tree(xyz, st)
+    e0 = G.export()
+    v = np.array([5.0, 0.5, 0.1, 0.01, -0.02, 0.4], np.float32)
+    G.apply_velocities_in_place(v)
+    e1 = G.export()
+    for i in range(0, len(e0["mean"]), 7):
+        mo, no = orc.warp_leaf(v, np.float32(e0["dts_mean"][i]), e0["mean"][i], e0["dir"][i])
+        assert np.array_equal(mo.view(np.uint32), e1["mean"][i].view(np.uint32))
+        assert np.array_equal(no.view(np.uint32), e1["dir"][i].view(np.uint32))
+    # leaves only skipped when asked
+    G2 = kds.TreeGeneratorB2003D(leaf_max_points=16).make_tree(xyz, st)
+    G2.apply_velocities_in_place(v, skip_leaves=True)
+    e2 = G2.export()
+    assert np.array_equal(e2["mean"][e2["leaves"]], e0["mean"][e0["leaves"]])
+    # rigid transform: applyIsometry_ row loop
+    from kd_slam2_b200 import synth
+    X = synth.pose((1.0, -2.0, 0.3), (0.1, 0.2, -0.3)).astype(np.float32)
+    G3 = kds.TreeGeneratorB2003D(leaf_max_points=16).make_tree(xyz, st)
+    G3.apply_isometry_in_place(X)
+    e3 = G3.export()
+    m = e0["mean"][10]
+    ref = np.float32(X[:, 3])
+    for c in range(3):
+        ref = (ref + (X[:, c] * m[c]).astype(np.float32)).astype(np.float32)
+    assert np.array_equal(ref.view(np.uint32), e3["mean"][10].view(np.uint32))
+    L = G3.extract_compressed_leaves()
+    assert np.array_equal(L[:, :3], e3["mean"][e3["leaves"]])

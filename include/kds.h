@@ -51,6 +51,10 @@ typedef struct kds_aligner kds_aligner;
 /* Human-readable text of the last error on the calling thread. */
 const char* kds_last_error(void);
 
+/* Number of CUDA kernels libkds has launched in this process (launch accounting; no
+ * reference counterpart).  Launches replayed from a CUDA graph count once per replay. */
+int64_t kds_launch_count(void);
+
 /* Replaces lib/kd_slam_cuda_init.cu:3-6 (cudaSetDeviceFlags in a .so constructor):
  * selects the device and, if blocking_sync != 0, sets cudaDeviceScheduleBlockingSync
  * before the context exists.  Optional; first use of any entry point initialises. */
@@ -94,6 +98,13 @@ typedef struct {
 int kds_tree_build(const float* xyz, const double* stamps, int64_t n, int32_t mem, const kds_tree_params* p,
                    void* stream, kds_tree** out);
 
+/* Batched form of kds_tree_build: num_trees clouds stored back to back (cloud r is
+ * points [offsets[r], offsets[r+1]) of xyz/stamps; offsets[0] = 0) built in one
+ * level-synchronous pass.  out[r] / status[r] per cloud (KDS_OK or
+ * KDS_ERR_TREE_REJECTED); the return value reports failures of the whole call. */
+int kds_tree_build_batch(const float* xyz, const double* stamps, const int64_t* offsets, int32_t num_trees,
+                         int32_t mem, const kds_tree_params* p, void* stream, kds_tree** out, int32_t* status);
+
 /* Replaces Tree_CUDAfromCPU_ (kd/tree/tree_cuda_impl_.h:197-222): uploads a node
  * array in the Node_ field order (kd/tree/node_.h:33-43), BFS numbered, node 0 the
  * root.  dts_mean/dts_cov/start/end may be NULL.  Leaves = nodes with no children. */
@@ -118,6 +129,9 @@ int kds_tree_apply_isometry(kds_tree* t, const float X[12], void* stream);
  * writes [mean, dir] per leaf (6 floats), optionally morphed by v (may be NULL). */
 int kds_tree_extract_compressed_leaves(const kds_tree* t, const float* v6, float* out, void* stream);
 
+/* Releases the tree's device memory to the stream-ordered pool on the stream it was
+ * built on.  As with TreeCUDA_'s destructor, no work using the tree may be pending on
+ * other streams. */
 void kds_tree_free(kds_tree* t);
 
 /* ------------------------------------------------------------------------------
@@ -197,6 +211,15 @@ int kds_aligner_get_stats_log(const kds_aligner* a, kds_stats* log, int32_t cap,
 int kds_aligner_linearize_debug(kds_aligner* a, const float caches[36], const float v[6], const float fixed_v[6],
                                 int32_t kind, int32_t stats_mode, int32_t* match, int32_t* status, double* H,
                                 double* b, kds_stats* stats);
+/* Measurement hooks (no reference counterpart).  With profiling on, compute() records a
+ * CUDA event pair around every linearization launch on the aligner's stream, inside the
+ * graph when one is used; get_profile returns the mean launch duration of the last
+ * compute in milliseconds.  count_touched_nodes returns the number of distinct
+ * fixed-tree nodes that the descents of the moving leaves visit at the current state
+ * (the fixed-tree term of the algorithmic-bytes model). */
+int kds_aligner_set_profiling(kds_aligner* a, int32_t on);
+int kds_aligner_get_profile(const kds_aligner* a, double* mean_ms, int32_t* launches);
+int kds_aligner_count_touched_nodes(kds_aligner* a, int64_t* count);
 void kds_aligner_free(kds_aligner* a);
 
 /* ------------------------------------------------------------------------------

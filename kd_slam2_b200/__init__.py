@@ -178,6 +178,24 @@ class TreeGeneratorB2003D:
         _check(rc, "kds_tree_build")
         return Tree(h.value)
 
+    def make_trees(self, clouds, stream=None) -> list:
+        """Builds one tree per (xyz, stamps) cloud in a single batched pass; None entries
+        where makeTree would return nullptr."""
+        xyz = np.ascontiguousarray(np.concatenate([np.asarray(c[0], np.float32).reshape(-1, 3) for c in clouds]))
+        has_st = any(c[1] is not None for c in clouds)
+        st = None
+        if has_st:
+            st = np.ascontiguousarray(np.concatenate(
+                [np.zeros(len(c[0])) if c[1] is None else np.asarray(c[1], np.float64) for c in clouds]))
+        off = np.zeros(len(clouds) + 1, np.int64)
+        off[1:] = np.cumsum([len(c[0]) for c in clouds])
+        R = len(clouds)
+        hs = (C.c_void_p * R)()
+        status = (C.c_int32 * R)()
+        _check(_lib.kds_tree_build_batch(xyz.ctypes.data, _ptr(st), off.ctypes.data, R, L.KDS_MEM_HOST,
+                                         C.byref(self.params), stream, hs, status), "kds_tree_build_batch")
+        return [Tree(hs[i]) if status[i] == L.KDS_OK else None for i in range(R)]
+
 
 # ---------------------------------------------------------------------------- aligners
 class _AlignerBase:
@@ -311,6 +329,24 @@ class _AlignerBase:
         H = np.zeros(36)
         _check(_lib.kds_aligner_get_pose_hessian(self._h, H.ctypes.data), "kds_aligner_get_pose_hessian")
         return H.reshape(6, 6)
+
+    def set_profiling(self, on: bool = True) -> None:
+        _check(_lib.kds_aligner_set_profiling(self._h, 1 if on else 0), "kds_aligner_set_profiling")
+
+    def profile(self) -> tuple[float, int]:
+        """(mean linearization launch duration in ms, launches) of the last compute."""
+        m = C.c_double()
+        n = C.c_int32()
+        _check(_lib.kds_aligner_get_profile(self._h, C.byref(m), C.byref(n)), "kds_aligner_get_profile")
+        return m.value, n.value
+
+    def count_touched_nodes(self) -> int:
+        c = C.c_int64()
+        _check(_lib.kds_aligner_count_touched_nodes(self._h, C.byref(c)), "kds_aligner_count_touched_nodes")
+        return c.value
+
+    def set_stream(self, stream) -> None:
+        _check(_lib.kds_aligner_set_stream(self._h, stream), "kds_aligner_set_stream")
 
     def linearize_debug(self, caches36, v=None, fixed_v=None, kind=None, stats_mode=False):
         """One linearization at explicit float caches (Xm, Xf, Xmf): per-leaf matches and status."""

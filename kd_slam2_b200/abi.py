@@ -125,8 +125,11 @@ _I64 = C.c_int64
 SIGNATURES = {
     "kds_last_error": (C.c_char_p, []),
     "kds_init": (C.c_int, [_I32, _I32]),
+    "kds_launch_count": (_I64, []),
     "kds_tree_params_default": (None, [C.POINTER(TreeParams)]),
     "kds_tree_build": (C.c_int, [_P, _P, _I64, _I32, C.POINTER(TreeParams), _P, C.POINTER(_P)]),
+    "kds_tree_build_batch": (C.c_int, [_P, _P, _P, _I32, _I32, C.POINTER(TreeParams), _P, C.POINTER(_P),
+                                       C.POINTER(_I32)]),
     "kds_tree_import": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _I64, C.c_double, C.POINTER(_P)]),
     "kds_tree_get_info": (C.c_int, [_P, C.POINTER(TreeInfo)]),
     "kds_tree_export": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
@@ -160,6 +163,9 @@ SIGNATURES = {
     "kds_aligner_get_stats": (C.c_int, [_P, C.POINTER(Stats)]),
     "kds_aligner_get_stats_log": (C.c_int, [_P, C.POINTER(Stats), _I32, C.POINTER(_I32)]),
     "kds_aligner_linearize_debug": (C.c_int, [_P, _P, _P, _P, _I32, _I32, _P, _P, _P, _P, C.POINTER(Stats)]),
+    "kds_aligner_set_profiling": (C.c_int, [_P, _I32]),
+    "kds_aligner_get_profile": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(_I32)]),
+    "kds_aligner_count_touched_nodes": (C.c_int, [_P, C.POINTER(_I64)]),
     "kds_aligner_free": (None, [_P]),
     "kds_batch_create": (C.c_int, [C.POINTER(_P)]),
     "kds_batch_run": (C.c_int, [_P, C.POINTER(Job), _I32, _I32, _P]),

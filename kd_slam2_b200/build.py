@@ -25,6 +25,7 @@ NVCC_COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "
 
 UNITS = [
     ("kds_tree.cu", ["-fmad=false"]),
+    ("kds_build.cu", ["-fmad=false"]),
     ("kds_align.cu", []),
     ("kds_api.cu", []),
 ]

@@ -390,51 +390,6 @@ __device__ void dpose_d(const double* ZXi, const double* Xm, double* e, double J
     }
 }
 
-// symmetric LDL^T with diagonal pivoting, n <= 12, in place on A (row-major)
-__device__ bool ldlt_solve_d(int n, double* A, const double* rhs, double* x) {
-  int perm[12];
-  double L[12][12], Dg[12], y[12];
-  for (int i = 0; i < n; ++i) {
-    perm[i] = i;
-    for (int j = 0; j < n; ++j) L[i][j] = (i == j) ? 1.0 : 0.0;
-  }
-  for (int k = 0; k < n; ++k) {
-    int p = k;
-    double best = fabs(A[k * n + k]);
-    for (int i = k + 1; i < n; ++i)
-      if (fabs(A[i * n + i]) > best) { best = fabs(A[i * n + i]); p = i; }
-    if (p != k) {
-      for (int j = 0; j < n; ++j) { double tmp = A[k * n + j]; A[k * n + j] = A[p * n + j]; A[p * n + j] = tmp; }
-      for (int i = 0; i < n; ++i) { double tmp = A[i * n + k]; A[i * n + k] = A[i * n + p]; A[i * n + p] = tmp; }
-      for (int j = 0; j < k; ++j) { double tmp = L[k][j]; L[k][j] = L[p][j]; L[p][j] = tmp; }
-      int tp = perm[k]; perm[k] = perm[p]; perm[p] = tp;
-    }
-    double d = A[k * n + k];
-    Dg[k] = d;
-    if (d == 0.0) return false;
-    for (int i = k + 1; i < n; ++i) L[i][k] = A[i * n + k] / d;
-    for (int i = k + 1; i < n; ++i)
-      for (int j = k + 1; j <= i; ++j) {
-        A[i * n + j] = A[i * n + j] - L[i][k] * d * L[j][k];
-        A[j * n + i] = A[i * n + j];
-      }
-  }
-  for (int i = 0; i < n; ++i) y[i] = rhs[perm[i]];
-  for (int i = 0; i < n; ++i) {
-    double acc = y[i];
-    for (int j = 0; j < i; ++j) acc -= L[i][j] * y[j];
-    y[i] = acc;
-  }
-  for (int i = 0; i < n; ++i) y[i] /= Dg[i];
-  for (int i = n - 1; i >= 0; --i) {
-    double acc = y[i];
-    for (int j = i + 1; j < n; ++j) acc -= L[j][i] * y[j];
-    y[i] = acc;
-  }
-  for (int i = 0; i < n; ++i) x[perm[i]] = y[i];
-  return true;
-}
-
 __device__ void refresh_caches(const JobState& S, LinDev* lins, int lb, int lc) {
   for (int l = lb; l < lb + lc; ++l) {
     LinDev& L = lins[l];
@@ -453,17 +408,81 @@ __device__ void refresh_caches(const JobState& S, LinDev* lins, int lb, int lc) 
   }
 }
 
-__device__ __noinline__ void finalize(const JobIn& Jn, JobState& S, JobOut& O, kds_stats* log, LinDev* lins, const double* red) {
+// Pose prior (posePriorBuildQuadraticForm, kd/icp/tree_aligner_base_.h:139-152): adds
+// J^T Omega J and J^T Omega e to the pose block.  Single thread, used by the localizer.
+__device__ __noinline__ void add_pose_prior(const JobIn& Jn, const double* X, double* H, double* b, int D) {
+  double e6[6], Jp[6][6];
+  dpose_d(Jn.prior_ZXi, X, e6, Jp);
+  const double* Om = Jn.prior_info;
+  double OJ[6][6], Oe[6];
+  for (int i = 0; i < 6; ++i) {
+    for (int j = 0; j < 6; ++j) {
+      double a = 0;
+      for (int k = 0; k < 6; ++k) a += Om[i * 6 + k] * Jp[k][j];
+      OJ[i][j] = a;
+    }
+    double a = 0;
+    for (int k = 0; k < 6; ++k) a += Om[i * 6 + k] * e6[k];
+    Oe[i] = a;
+  }
+  for (int i = 0; i < 6; ++i) {
+    for (int j = 0; j < 6; ++j) {
+      double a = 0;
+      for (int k = 0; k < 6; ++k) a += Jp[k][i] * OJ[k][j];
+      H[i * D + j] += a;
+    }
+    double a = 0;
+    for (int k = 0; k < 6; ++k) a += Jp[k][i] * Oe[k];
+    b[i] += a;
+  }
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// The last block of a job: FP64 sum of the job's partials in tile order, then warp 0
+// runs ICP_::oneRound / CTICP_::oneRound (kd/icp/icp_impl_.h:72-89,
+// kd/cticp/cticp_impl_.h:67-91) with the D x D system in shared memory: Cholesky of
+// H + damping (SPD), warp-parallel trailing updates and triangular solves.
+__device__ __noinline__ void job_tail(const JobIn& Jn, JobState& S, JobOut& O, kds_stats* log, LinDev* lins,
+                                      const double* partials, double* red, int M) {
+  for (int k = threadIdx.x; k < kPStride; k += blockDim.x) {
+    if (k >= M && k < kPStats) { red[k] = 0.0; continue; }
+    double acc = 0.0;
+    for (int t = Jn.tile_begin; t < Jn.tile_begin + Jn.tile_count; ++t) acc += __ldcg(partials + (size_t)t * kPStride + k);
+    red[k] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
   const int kind = Jn.kind;
   const int Dk = kind == 0 ? 6 : (kind == 1 ? 12 : 18);
   const int D = kind == 0 ? 6 : 12;
-  // unpack the upper triangle of the Dk x Dk system
-  double Hf[18 * 18], bf[18];
-  {
-    int k = 0;
-    for (int a = 0; a < Dk; ++a)
-      for (int c = a; c < Dk; ++c) { Hf[a * Dk + c] = red[k]; Hf[c * Dk + a] = red[k]; ++k; }
-    for (int a = 0; a < Dk; ++a) bf[a] = red[k++];
+  double* sH = red + kPStride;  // D*D
+  double* sA = sH + 144;        // D*D
+  double* sb = sA + 144;        // D
+  double* sy = sb + 12;         // D
+  double* sx = sy + 12;         // D
+  // unpack the packed upper triangle
+  for (int k = lane; k < M; k += 32) {
+    int r, c;
+    entry_rc(Dk, k, r, c);
+    double v = red[k];
+    if (c == Dk) {
+      if (r < D) sb[r] = v;
+      else O.b_vel_B[r - 12] = v;
+    } else if (c < D) {
+      sH[r * D + c] = v;
+      sH[c * D + r] = v;
+    } else {  // dual blocks, c >= 12
+      if (r < 6) O.H_cross_pose_vel_B[r * 6 + (c - 12)] = v;
+      else if (r < 12) O.H_cross_vel_AB[(r - 6) * 6 + (c - 12)] = v;
+      else { O.H_vel_B[(r - 12) * 6 + (c - 12)] = v; O.H_vel_B[(c - 12) * 6 + (r - 12)] = v; }
+    }
   }
   kds_stats st;
   st.num_inliers = (int32_t)red[kPStats + 0];
@@ -475,76 +494,75 @@ __device__ __noinline__ void finalize(const JobIn& Jn, JobState& S, JobOut& O, k
   st.chi2_kernelized = (float)red[kPStats + 6];
   st.pert_pose_norm = 0.f;
   st.pert_vel_norm = 0.f;
-  double H[144], b[12];
-  for (int a = 0; a < D; ++a) {
-    for (int c = 0; c < D; ++c) H[a * D + c] = Hf[a * Dk + c];
-    b[a] = bf[a];
-  }
-  if (kind == 2) {
-    for (int a = 0; a < 6; ++a) {
-      for (int c = 0; c < 6; ++c) {
-        O.H_vel_B[a * 6 + c] = Hf[(12 + a) * Dk + 12 + c];
-        O.H_cross_pose_vel_B[a * 6 + c] = Hf[a * Dk + 12 + c];
-        O.H_cross_vel_AB[a * 6 + c] = Hf[(6 + a) * Dk + 12 + c];
-      }
-      O.b_vel_B[a] = bf[12 + a];
-    }
-  }
   const int it = S.iter;
+  __syncwarp();
   if (Jn.mode != KDS_JOB_COMPUTE) {
-    for (int i = 0; i < D * D; ++i) O.H[i] = H[i];
-    for (int i = 0; i < D; ++i) O.b[i] = b[i];
-    O.stats = st;
-    O.result = 0;
-    O.iterations = 1;
-    S.done = 1;
+    for (int i = lane; i < D * D; i += 32) O.H[i] = sH[i];
+    if (lane < D) O.b[lane] = sb[lane];
+    if (lane == 0) {
+      O.stats = st;
+      O.result = 0;
+      O.iterations = 1;
+      S.done = 1;
+      S.arrive = 0u;
+    }
     return;
   }
-  if (Jn.prior_enabled) {
-    double e6[6], Jp[6][6];
-    dpose_d(Jn.prior_ZXi, S.X, e6, Jp);
-    const double* Om = Jn.prior_info;
-    double OJ[6][6], Oe[6];
-    for (int i = 0; i < 6; ++i) {
-      for (int j = 0; j < 6; ++j) {
-        double a = 0;
-        for (int k = 0; k < 6; ++k) a += Om[i * 6 + k] * Jp[k][j];
-        OJ[i][j] = a;
-      }
-      double a = 0;
-      for (int k = 0; k < 6; ++k) a += Om[i * 6 + k] * e6[k];
-      Oe[i] = a;
-    }
-    for (int i = 0; i < 6; ++i) {
-      for (int j = 0; j < 6; ++j) {
-        double a = 0;
-        for (int k = 0; k < 6; ++k) a += Jp[k][i] * OJ[k][j];
-        H[i * D + j] += a;
-      }
-      double a = 0;
-      for (int k = 0; k < 6; ++k) a += Jp[k][i] * Oe[k];
-      b[i] += a;
-    }
+  if (Jn.prior_enabled && lane == 0) add_pose_prior(Jn, S.X, sH, sb, D);
+  __syncwarp();
+  for (int i = lane; i < D * D; i += 32) {
+    O.H[i] = sH[i];
+    sA[i] = sH[i];
   }
-  for (int i = 0; i < D * D; ++i) O.H[i] = H[i];
-  for (int i = 0; i < D; ++i) O.b[i] = b[i];
-  O.iterations = it + 1;
+  if (lane < D) {
+    O.b[lane] = sb[lane];
+    sA[lane * D + lane] += (lane < 6) ? (double)Jn.P.damping : (double)Jn.P.velocity_damping;
+  }
   if (st.num_inliers + st.num_outliers < Jn.P.min_good_measurements) {
-    if (log && it < kMaxLog) log[it] = st;
-    O.stats = st;
-    S.done = 1;
-    S.result = -it;
-    O.result = S.result;
+    if (lane == 0) {
+      if (log && it < kMaxLog) log[it] = st;
+      O.stats = st;
+      O.iterations = it + 1;
+      S.done = 1;
+      S.result = -it;
+      O.result = S.result;
+      S.arrive = 0u;
+    }
     return;
   }
-  double A[144], rhs[12], dx[12];
-  for (int i = 0; i < D * D; ++i) A[i] = H[i];
-  for (int i = 0; i < D; ++i) {
-    A[i * D + i] += (i < 6) ? (double)Jn.P.damping : (double)Jn.P.velocity_damping;
-    rhs[i] = -b[i];
+  __syncwarp();
+  // Cholesky, lower triangle of sA
+  bool ok = true;
+  for (int k = 0; k < D; ++k) {
+    double d = sA[k * D + k];
+    ok = ok && (d > 0.0);
+    double lkk = sqrt(fmax(d, 1e-300));
+    __syncwarp();
+    if (lane > k && lane < D) sA[lane * D + k] /= lkk;
+    if (lane == k) sA[k * D + k] = lkk;
+    __syncwarp();
+    for (int i = k + 1; i < D; ++i) {
+      int j = k + 1 + lane;
+      if (j <= i) sA[i * D + j] -= sA[i * D + k] * sA[j * D + k];
+    }
+    __syncwarp();
   }
-  if (!ldlt_solve_d(D, A, rhs, dx))
-    for (int i = 0; i < D; ++i) dx[i] = 0.0;
+  // L y = -b, then L^T x = y
+  for (int i = 0; i < D; ++i) {
+    double part = (lane < i) ? sA[i * D + lane] * sy[lane] : 0.0;
+    double sum = warp_sum_d(part);
+    if (lane == 0) sy[i] = (-sb[i] - sum) / sA[i * D + i];
+    __syncwarp();
+  }
+  for (int i = D - 1; i >= 0; --i) {
+    double part = (lane > i && lane < D) ? sA[lane * D + i] * sx[lane] : 0.0;
+    double sum = warp_sum_d(part);
+    if (lane == 0) sx[i] = (sy[i] - sum) / sA[i * D + i];
+    __syncwarp();
+  }
+  if (lane != 0) return;
+  double dx[12];
+  for (int i = 0; i < D; ++i) dx[i] = ok ? sx[i] : 0.0;
   double pp = 0.0, pv = 0.0;
   for (int i = 0; i < 6; ++i) pp += dx[i] * dx[i];
   st.pert_pose_norm = (float)sqrt(pp);
@@ -555,6 +573,7 @@ __device__ __noinline__ void finalize(const JobIn& Jn, JobState& S, JobOut& O, k
   for (int i = 0; i < D; ++i) O.dx[i] = dx[i];
   if (log && it < kMaxLog) log[it] = st;
   O.stats = st;
+  O.iterations = it + 1;
   if (!Jn.stats_mode) {
     double dX[12], Xn[12];
     expmap_d(dx, dX);
@@ -589,23 +608,7 @@ __device__ __noinline__ void finalize(const JobIn& Jn, JobState& S, JobOut& O, k
   for (int i = 0; i < 12; ++i) O.X[i] = S.X[i];
   for (int i = 0; i < 6; ++i) O.v[i] = S.v[i];
   if (!S.done) refresh_caches(S, lins, Jn.lin_begin, Jn.lin_count);
-}
-
-// ---------------------------------------------------------------------------
-// The last block of a job: FP64 sum of the job's partials in tile order, then finalize.
-__device__ __noinline__ void job_tail(const JobIn& Jn, JobState& S, JobOut& O, kds_stats* log, LinDev* lins,
-                                      const double* partials, double* red, int M) {
-  for (int k = threadIdx.x; k < kPStride; k += blockDim.x) {
-    if (k >= M && k < kPStats) { red[k] = 0.0; continue; }
-    double acc = 0.0;
-    for (int t = Jn.tile_begin; t < Jn.tile_begin + Jn.tile_count; ++t) acc += __ldcg(partials + (size_t)t * kPStride + k);
-    red[k] = acc;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    finalize(Jn, S, O, log, lins, red);
-    S.arrive = 0u;
-  }
+  S.arrive = 0u;
 }
 
 // One Gauss-Newton iteration over the tiles [tile0, tile0 + gridDim.x) of one kind.
@@ -687,6 +690,63 @@ __global__ void k_init_jobs(const JobIn* jobs, JobState* states, JobOut* outs, L
 }
 
 // ---------------------------------------------------------------------------
+// Traffic model helper: marks every fixed node that the greedy descents visit.
+template <int KIND>
+__global__ void k_touch(const JobIn* jobs, const LinDev* lins, uint32_t* bitmap) {
+  const JobIn& Jn = jobs[0];
+  const LinDev& L = lins[Jn.lin_begin];
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Jn.m_num_leaves || L.f_num_nodes <= 0) return;
+  const CacheF& C = L.cache;
+  float4 md = Jn.m_md[i], nr = Jn.m_nrm[i];
+  F3 m = f3(md.x, md.y, md.z), n = f3(nr.x, nr.y, nr.z);
+  F3 mw = m, nw = n;
+  if (KIND != 0) warp_x(C.v, md.w, m, n, mw, nw);
+  F3 q = apply_iso_x(C.Xmf, mw);
+  int idx = 0;
+  while (idx >= 0) {
+    atomicOr(&bitmap[idx >> 5], 1u << (idx & 31));
+    DNode nd = load_node(L.fnodes + idx);
+    int l = node_left(nd), r = node_right(nd);
+    if (l < 0 && r < 0) break;
+    idx = dot3x(node_dir(nd), sub3x(q, node_mean(nd))) > 0.0f ? l : r;
+  }
+}
+__global__ void k_popc(const uint32_t* bitmap, int64_t words, unsigned long long* count) {
+  unsigned long long c = 0;
+  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < words; w += (int64_t)gridDim.x * blockDim.x)
+    c += __popc(bitmap[w]);
+  atomicAdd(count, c);
+}
+
+int count_touched(Runner& R, int kind, int64_t fixed_nodes, int64_t* out, cudaStream_t s) {
+  *out = 0;
+  if (R.num_jobs < 1 || fixed_nodes <= 0) return KDS_OK;
+  k_init_jobs<<<1, 128, 0, s>>>(R.d_jobs, R.d_states, R.d_outs, R.d_lins, 1); ::kds::count_launch();
+  int64_t words = (fixed_nodes + 31) / 32;
+  uint32_t* bm = nullptr;
+  unsigned long long* cnt = nullptr;
+  KDS_CK(cudaMalloc(&bm, words * 4 + 64));
+  cnt = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(bm) + ((words * 4 + 7) & ~7ll));
+  cudaMemsetAsync(bm, 0, words * 4 + 64, s);
+  int nl = R.h_jobs[0].m_num_leaves;
+  int g = (nl + 255) / 256;
+  if (g > 0) {
+    if (kind == 0) k_touch<0><<<g, 256, 0, s>>>(R.d_jobs, R.d_lins, bm);
+    else k_touch<1><<<g, 256, 0, s>>>(R.d_jobs, R.d_lins, bm);
+    ::kds::count_launch();
+  }
+  k_popc<<<64, 256, 0, s>>>(bm, words, cnt); ::kds::count_launch();
+  unsigned long long h = 0;
+  cudaMemcpyAsync(&h, cnt, 8, cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  cudaFree(bm);
+  if (e != cudaSuccess) return cuda_status(e, "count_touched", __FILE__, __LINE__);
+  *out = (int64_t)h;
+  return KDS_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Host runner
 int Runner::reserve(int nj, int nl, int nt) {
   if (nj <= cap_jobs && nl <= cap_lins && nt <= cap_tiles) return KDS_OK;
@@ -723,6 +783,8 @@ int Runner::reserve(int nj, int nl, int nt) {
 
 void Runner::release() {
   drop_graph();
+  for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
+  prof_ev.clear();
   if (block) cudaFree(block);
   block = nullptr;
   cap_jobs = cap_lins = cap_tiles = 0;
@@ -781,20 +843,58 @@ int Runner::max_launches() const {
   return m;
 }
 
+int Runner::ensure_events(int n) {
+  while ((int)prof_ev.size() < n) {
+    cudaEvent_t e;
+    KDS_CK(cudaEventCreate(&e));
+    prof_ev.push_back(e);
+  }
+  return KDS_OK;
+}
+
+double Runner::profile_mean_ms(int* launches) const {
+  double sum = 0.0;
+  int n = 0;
+  for (int i = 0; i < prof_launches; ++i) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, prof_ev[2 * i], prof_ev[2 * i + 1]) == cudaSuccess) {
+      sum += ms;
+      ++n;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  if (launches) *launches = n;
+  return n ? sum / n : 0.0;
+}
+
 int Runner::enqueue(cudaStream_t s, int32_t* dbg_match, int32_t* dbg_status) {
   if (num_jobs == 0) return KDS_OK;
-  k_init_jobs<<<(num_jobs + 127) / 128, 128, 0, s>>>(d_jobs, d_states, d_outs, d_lins, num_jobs);
+  k_init_jobs<<<(num_jobs + 127) / 128, 128, 0, s>>>(d_jobs, d_states, d_outs, d_lins, num_jobs); ::kds::count_launch();
   int L = max_launches();
+  int nk = (kind_count[0] ? 1 : 0) + (kind_count[1] ? 1 : 0) + (kind_count[2] ? 1 : 0);
+  prof_launches = profiling ? L * nk : 0;
+  if (profiling) {
+    int rc = ensure_events(2 * prof_launches);
+    if (rc) return rc;
+  }
+  int ev = 0;
   for (int i = 0; i < L; ++i) {
-    if (kind_count[0])
-      k_linearize<0><<<kind_count[0], kBlock, 0, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
-                                                      kind_begin[0], d_partials, dbg_match, dbg_status);
-    if (kind_count[1])
-      k_linearize<1><<<kind_count[1], kBlock, 0, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
-                                                      kind_begin[1], d_partials, dbg_match, dbg_status);
-    if (kind_count[2])
-      k_linearize<2><<<kind_count[2], kBlock, 0, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
-                                                      kind_begin[2], d_partials, dbg_match, dbg_status);
+    for (int kind = 0; kind < 3; ++kind) {
+      if (!kind_count[kind]) continue;
+      if (profiling) KDS_CK(cudaEventRecordWithFlags(prof_ev[ev++], s, cudaEventRecordExternal));
+      if (kind == 0)
+        k_linearize<0><<<kind_count[0], kBlock, 0, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
+                                                        kind_begin[0], d_partials, dbg_match, dbg_status);
+      else if (kind == 1)
+        k_linearize<1><<<kind_count[1], kBlock, 0, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
+                                                        kind_begin[1], d_partials, dbg_match, dbg_status);
+      else
+        k_linearize<2><<<kind_count[2], kBlock, 0, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
+                                                        kind_begin[2], d_partials, dbg_match, dbg_status);
+      ::kds::count_launch();
+      if (profiling) KDS_CK(cudaEventRecordWithFlags(prof_ev[ev++], s, cudaEventRecordExternal));
+    }
   }
   KDS_CK(cudaGetLastError());
   return KDS_OK;
@@ -809,6 +909,7 @@ int Runner::run(cudaStream_t s, bool use_graph, int32_t* dbg_match, int32_t* dbg
   key.push_back(num_tiles);
   key.push_back(max_launches());
   for (int k = 0; k < 3; ++k) { key.push_back(kind_begin[k]); key.push_back(kind_count[k]); }
+  key.push_back(profiling ? 1 : 0);
   if (key != graph_key) {
     drop_graph();
     cudaStream_t cs;

@@ -112,6 +112,12 @@ struct Runner {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   std::vector<int64_t> graph_key;
+  // optional event pair per linearization launch (measurement only)
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_ev;
+  int prof_launches = 0;
+  int ensure_events(int n);
+  double profile_mean_ms(int* launches) const;
 
   int reserve(int nj, int nl, int nt);
   void release();
@@ -123,5 +129,7 @@ struct Runner {
   int fetch(cudaStream_t s, std::vector<JobOut>& outs, std::vector<kds_stats>* logs);
   ~Runner() { release(); }
 };
+
+int count_touched(Runner& R, int kind, int64_t fixed_nodes, int64_t* out, cudaStream_t s);
 
 }  // namespace kds

@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -31,6 +32,9 @@ int cuda_status(cudaError_t e, const char* what, const char* file, int line) {
   return KDS_ERR_CUDA;
 }
 
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 static std::once_flag g_once;
 static int g_init_status = KDS_OK;
 
@@ -42,7 +46,16 @@ int ensure_init() {
       cudaGetLastError();
       set_error("no CUDA device available");
       g_init_status = KDS_ERR_NO_DEVICE;
+      return;
     }
+    // keep memory freed with cudaFreeAsync in the device's pool for reuse
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
   });
   if (g_init_status != KDS_OK) set_error("no CUDA device available");
   return g_init_status;
@@ -95,6 +108,8 @@ extern "C" {
 
 const char* kds_last_error(void) { return g_last_error.c_str(); }
 
+int64_t kds_launch_count(void) { return g_launches.load(); }
+
 int kds_init(int32_t device, int32_t blocking_sync) {
   int n = 0;
   cudaError_t e = cudaGetDeviceCount(&n);
@@ -139,6 +154,19 @@ int kds_tree_build(const float* xyz, const double* stamps, int64_t n, int32_t me
   kds_tree_params def;
   if (!p) { kds_tree_params_default(&def); p = &def; }
   return tree_build(xyz, stamps, n, mem, p, as_stream(stream), out);
+}
+
+int kds_tree_build_batch(const float* xyz, const double* stamps, const int64_t* offsets, int32_t num_trees,
+                         int32_t mem, const kds_tree_params* p, void* stream, kds_tree** out, int32_t* status) {
+  if (!out || !status || !offsets || num_trees <= 0 || (mem != KDS_MEM_HOST && mem != KDS_MEM_DEVICE)) {
+    set_error("kds_tree_build_batch: bad arguments");
+    return KDS_ERR_INVALID_ARG;
+  }
+  for (int r = 0; r < num_trees; ++r) out[r] = nullptr;
+  KDS_INIT();
+  kds_tree_params def;
+  if (!p) { kds_tree_params_default(&def); p = &def; }
+  return tree_build_forest(xyz, stamps, offsets, num_trees, mem, p, as_stream(stream), out, status);
 }
 
 int kds_tree_import(const float* mean, const float* dir, const double* dts_mean, const double* dts_cov,
@@ -539,6 +567,36 @@ int kds_aligner_linearize_debug(kds_aligner* a, const float caches[36], const fl
   memcpy(a->v, vs, sizeof(vs));
   memcpy(a->fv, fvs, sizeof(fvs));
   return rc;
+}
+
+int kds_aligner_set_profiling(kds_aligner* a, int32_t on) {
+  CHECK_A(a);
+  a->runner.profiling = on != 0;
+  return KDS_OK;
+}
+
+int kds_aligner_get_profile(const kds_aligner* a, double* mean_ms, int32_t* launches) {
+  CHECK_A(a);
+  int n = 0;
+  double m = a->runner.profile_mean_ms(&n);
+  if (mean_ms) *mean_ms = m;
+  if (launches) *launches = n;
+  return KDS_OK;
+}
+
+int kds_aligner_count_touched_nodes(kds_aligner* a, int64_t* count) {
+  CHECK_A(a);
+  if (!count) return KDS_ERR_INVALID_ARG;
+  std::vector<JobIn> jobs(1);
+  std::vector<LinDev> lins;
+  int kind = a->type == KDS_ICP ? 0 : 1;
+  int rc = make_job(a, kind, KDS_JOB_LINEARIZE, 0, 0, jobs[0], lins);
+  if (rc) return rc;
+  cudaStream_t s = a->stream ? a->stream : cudaStreamPerThread;
+  rc = a->runner.setup(jobs, lins, s);
+  if (rc) return rc;
+  const kds_tree* f = a->forest.empty() ? a->fixed : a->forest[0].tree;
+  return count_touched(a->runner, kind, f->d.num_nodes, count, s);
 }
 
 void kds_aligner_free(kds_aligner* a) { delete a; }

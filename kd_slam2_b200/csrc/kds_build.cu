@@ -1,0 +1,1171 @@
+// GPU surfel KD-tree build for one or many clouds at once (a forest).  Compiled with
+// -fmad=false: every double/float expression rounds each multiply and add separately,
+// so the result is bit-identical to the CPU oracle's canonical build.
+//
+// Replaces TreeGenerator_::makeTree (kd/tree/tree_generator_impl_.h:7-19), which the
+// reference runs on the CPU only.  The tree is built level by level for all trees of
+// the batch together:
+//   * per-node moments [xx,xy,xz,yy,yz,zz,x,y,z,dt,dt^2] are exact, order-free 128-bit
+//     fixed-point sums: each product of two floats (or double stamp term) is decomposed
+//     into sign/mantissa/exponent and its floor(v * 2^64) is formed with integer shifts,
+//     so warps, blocks and atomics may add them in any order;
+//   * FP64 covariance, cyclic Jacobi eigensolver, FlatLeafPolicy_ decision
+//     (kd/tree/flat_leaf_policy_.h:52-108) in FP64;
+//   * stable partition by Node_::whichSide in float (kd/tree/node_.h:53-56);
+//   * children numbered by a scan over the level's split flags: nodes of one level
+//     are grouped by tree, so each tree's nodes in global order are its BFS order
+//     (kd/tree/tree_cpu_impl_.h:136-158), kept by prune (kd/tree/tree_cpu_.h:172-207).
+// Nodes with <= kBig points are processed by one warp each; larger ones by blocks over
+// kChunk-point chunks with 128-bit atomics.  The level bounds live in device memory;
+// the host checks for completion only every kLevelsPerSync levels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "kds_internal.cuh"
+
+namespace kds {
+
+namespace {
+
+constexpr int kBig = 1024;
+constexpr int kChunk = 1024;
+constexpr int kThreads = 256;
+constexpr int kGridBlocks = 148 * 4;
+constexpr int kLevelBlocks = 64;
+constexpr int kLevelsPerSync = 4;
+constexpr int kMaxDepth = 64;
+
+// ---------------------------------------------------------------------------
+// 128-bit two's complement fixed point (units of 2^-64)
+struct U128 {
+  unsigned long long lo, hi;
+};
+__host__ __device__ __forceinline__ U128 u128_zero() { U128 r; r.lo = 0ull; r.hi = 0ull; return r; }
+__host__ __device__ __forceinline__ U128 u128_add(U128 a, U128 b) {
+  U128 r;
+  r.lo = a.lo + b.lo;
+  r.hi = a.hi + b.hi + (r.lo < a.lo ? 1ull : 0ull);
+  return r;
+}
+__device__ __forceinline__ U128 shfl_xor_u128(U128 v, int m) {
+  U128 r;
+  r.lo = __shfl_xor_sync(0xffffffffu, v.lo, m);
+  r.hi = __shfl_xor_sync(0xffffffffu, v.hi, m);
+  return r;
+}
+__device__ __forceinline__ void atomic_add_u128(U128* dst, U128 v) {
+  unsigned long long old = atomicAdd(&dst->lo, v.lo);
+  unsigned long long carry = (old + v.lo < old) ? 1ull : 0ull;
+  atomicAdd(&dst->hi, v.hi + carry);
+}
+__host__ __device__ __forceinline__ double fx_to_d(U128 q) {
+  long long hi = (long long)q.hi;
+  return ((double)hi * 0x1p64 + (double)q.lo) * 0x1p-64;
+}
+
+// floor(v * 2^64) for v = (-1)^sign * mant * 2^exp2 (exact integer arithmetic)
+__device__ __forceinline__ U128 fx_parts(unsigned sign, unsigned long long mant, int exp2) {
+  U128 mag = u128_zero();
+  bool rem = false;
+  if (mant == 0ull) return mag;
+  int sh = exp2 + 64;
+  if (sh >= 64) {
+    mag.hi = mant << (sh - 64);
+  } else if (sh > 0) {
+    mag.lo = mant << sh;
+    mag.hi = mant >> (64 - sh);
+  } else if (sh == 0) {
+    mag.lo = mant;
+  } else {
+    int r = -sh;
+    if (r >= 64) {
+      rem = true;
+    } else {
+      mag.lo = mant >> r;
+      rem = (mant & ((1ull << r) - 1ull)) != 0ull;
+    }
+  }
+  if (!sign) return mag;
+  U128 neg;  // -mag - rem: ~mag when rem, else ~mag + 1
+  neg.lo = ~mag.lo;
+  neg.hi = ~mag.hi;
+  if (!rem) {
+    neg.lo += 1ull;
+    if (neg.lo == 0ull) neg.hi += 1ull;
+  }
+  return neg;
+}
+__device__ __forceinline__ void f_parts(float f, unsigned& s, unsigned& m, int& e) {
+  unsigned b = __float_as_uint(f);
+  s = b >> 31;
+  unsigned E = (b >> 23) & 0xffu;
+  m = b & 0x7fffffu;
+  if (E == 0u) {
+    e = -149;
+  } else {
+    m |= 0x800000u;
+    e = (int)E - 150;
+  }
+}
+__device__ __forceinline__ U128 fx_f(float a) {
+  unsigned s, m;
+  int e;
+  f_parts(a, s, m, e);
+  return fx_parts(s, m, e);
+}
+__device__ __forceinline__ U128 fx_ff(float a, float b) {
+  unsigned sa, ma, sb, mb;
+  int ea, eb;
+  f_parts(a, sa, ma, ea);
+  f_parts(b, sb, mb, eb);
+  return fx_parts(sa ^ sb, (unsigned long long)ma * (unsigned long long)mb, ea + eb);
+}
+__device__ __forceinline__ U128 fx_d(double d) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(d);
+  unsigned s = (unsigned)(b >> 63);
+  int E = (int)((b >> 52) & 0x7ffull);
+  unsigned long long m = b & ((1ull << 52) - 1ull);
+  int e;
+  if (E == 0) {
+    e = -1074;
+  } else {
+    m |= 1ull << 52;
+    e = E - 1075;
+  }
+  return fx_parts(s, m, e);
+}
+
+struct Moments {
+  U128 s[11];
+};
+
+__device__ __forceinline__ void moments_add_point(Moments& M, float4 p, double st, double ts0) {
+  M.s[0] = u128_add(M.s[0], fx_ff(p.x, p.x));
+  M.s[1] = u128_add(M.s[1], fx_ff(p.x, p.y));
+  M.s[2] = u128_add(M.s[2], fx_ff(p.x, p.z));
+  M.s[3] = u128_add(M.s[3], fx_ff(p.y, p.y));
+  M.s[4] = u128_add(M.s[4], fx_ff(p.y, p.z));
+  M.s[5] = u128_add(M.s[5], fx_ff(p.z, p.z));
+  M.s[6] = u128_add(M.s[6], fx_f(p.x));
+  M.s[7] = u128_add(M.s[7], fx_f(p.y));
+  M.s[8] = u128_add(M.s[8], fx_f(p.z));
+  double dt = st - ts0;
+  M.s[9] = u128_add(M.s[9], fx_d(dt));
+  M.s[10] = u128_add(M.s[10], fx_d(dt * dt));
+}
+
+// ---------------------------------------------------------------------------
+struct BNode {
+  int32_t start, end;
+  int32_t level;
+  int32_t tree;
+  int32_t split;      // 1: inner node
+  int32_t mid;
+  int32_t left, right;
+  int32_t has_parent;
+  int32_t par_has;    // propagated normal received from the parent
+  int32_t has_prop;   // propagated normal handed to the children
+  int32_t pad_;
+  float mean[3], dir[3];
+  double dts_mean, dts_cov;
+  double prop[3];
+  double par_prop[3];
+};
+
+struct BuildParams {
+  int32_t propagate_normal;
+  int32_t leaf_min_points;
+  int32_t leaf_max_points;
+  float leaf_density;
+  float leaf_min_normal_incidence;
+  float leaf_normal_eigenratio;
+  float prune_incidence;
+  int32_t max_level;
+};
+
+struct LevelState {
+  int32_t lb, le;        // node range of the current level
+  int32_t cur;           // point buffer holding the current level
+  int32_t depth;         // number of levels processed
+  int32_t max_size;      // largest node of the current level
+  int32_t max_next;      // largest node of the next level (being built)
+  int32_t error;         // 1: node capacity, 2: input out of range
+  int32_t num_chunks, num_big;
+  int32_t pad_;
+};
+
+__device__ __forceinline__ double ddot3(const double* a, const double* b) {
+  double p0 = a[0] * b[0], p1 = a[1] * b[1], p2 = a[2] * b[2];
+  return p0 + (p1 + p2);
+}
+
+// Cyclic Jacobi eigensolver for a symmetric 3x3 (Golub & Van Loan, sec. 8.5), fixed
+// 8 sweeps; eigenvalues ascending, eigenvectors as columns of V.
+__device__ void jacobi3(const double Ain[3][3], double ev[3], double V[3][3]) {
+  double a[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) { a[i][j] = Ain[i][j]; V[i][j] = (i == j) ? 1.0 : 0.0; }
+  for (int sweep = 0; sweep < 8; ++sweep) {
+    for (int pq = 0; pq < 3; ++pq) {
+      int p = (pq == 2) ? 1 : 0;
+      int q = (pq == 0) ? 1 : 2;
+      int r = 3 - p - q;
+      double apq = a[p][q];
+      if (apq == 0.0) continue;
+      double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
+      double t = 1.0 / (fabs(theta) + sqrt(theta * theta + 1.0));
+      if (theta < 0.0) t = -t;
+      double c = 1.0 / sqrt(t * t + 1.0);
+      double s = t * c;
+      double arp = a[r][p], arq = a[r][q];
+      a[p][p] = a[p][p] - t * apq;
+      a[q][q] = a[q][q] + t * apq;
+      a[p][q] = 0.0;
+      a[q][p] = 0.0;
+      double nrp = c * arp - s * arq;
+      double nrq = s * arp + c * arq;
+      a[r][p] = nrp; a[p][r] = nrp;
+      a[r][q] = nrq; a[q][r] = nrq;
+      for (int k = 0; k < 3; ++k) {
+        double vkp = V[k][p], vkq = V[k][q];
+        V[k][p] = c * vkp - s * vkq;
+        V[k][q] = s * vkp + c * vkq;
+      }
+    }
+  }
+  double d[3] = {a[0][0], a[1][1], a[2][2]};
+  int idx[3] = {0, 1, 2};
+  for (int i = 1; i < 3; ++i) {
+    int k = idx[i];
+    int j = i - 1;
+    while (j >= 0 && d[k] < d[idx[j]]) { idx[j + 1] = idx[j]; --j; }
+    idx[j + 1] = k;
+  }
+  double Vs[3][3];
+  for (int c2 = 0; c2 < 3; ++c2) {
+    ev[c2] = d[idx[c2]];
+    for (int r2 = 0; r2 < 3; ++r2) Vs[r2][c2] = V[r2][idx[c2]];
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) V[i][j] = Vs[i][j];
+}
+
+// FlatLeafPolicy_::fillMetadata over CountLeafPolicy_ and LabelPolicyBase_
+// (kd/tree/flat_leaf_policy_.h:52-108, count_leaf_policy_.h:27-43,
+// label_policy_base_impl_.h:12-97) on FP64 statistics.
+__device__ void decide(const Moments& M, int64_t n, BNode& nd, const BuildParams& P) {
+  for (int i = 0; i < 3; ++i) { nd.mean[i] = 0.f; nd.dir[i] = 0.f; }
+  nd.dts_mean = 0.0;
+  nd.dts_cov = 0.0;
+  double mean_d[3] = {0, 0, 0};
+  double e0[3] = {0, 0, 0}, e2[3] = {0, 0, 0};
+  double lam[3] = {0, 0, 0};
+  bool is_bad = true;
+  if (n > 0) {
+    double dn = (double)n;
+    double Sd[11];
+    for (int k = 0; k < 11; ++k) Sd[k] = fx_to_d(M.s[k]);
+    nd.dts_mean = Sd[9] / dn;
+    nd.dts_cov = Sd[10] / dn - nd.dts_mean * nd.dts_mean;
+    for (int i = 0; i < 3; ++i) mean_d[i] = Sd[6 + i] / dn;
+    for (int i = 0; i < 3; ++i) nd.mean[i] = (float)mean_d[i];
+    if (n >= 3) {
+      double C[3][3];
+      C[0][0] = Sd[0] / dn - mean_d[0] * mean_d[0];
+      C[0][1] = Sd[1] / dn - mean_d[0] * mean_d[1];
+      C[0][2] = Sd[2] / dn - mean_d[0] * mean_d[2];
+      C[1][1] = Sd[3] / dn - mean_d[1] * mean_d[1];
+      C[1][2] = Sd[4] / dn - mean_d[1] * mean_d[2];
+      C[2][2] = Sd[5] / dn - mean_d[2] * mean_d[2];
+      C[1][0] = C[0][1];
+      C[2][0] = C[0][2];
+      C[2][1] = C[1][2];
+      double V[3][3];
+      jacobi3(C, lam, V);
+      for (int i = 0; i < 3; ++i) { e0[i] = V[i][0]; e2[i] = V[i][2]; }
+      if (ddot3(mean_d, e0) > 0.0) for (int i = 0; i < 3; ++i) e0[i] = -e0[i];
+      if (ddot3(mean_d, e2) > 0.0) for (int i = 0; i < 3; ++i) e2[i] = -e2[i];
+      is_bad = false;
+    }
+  }
+  bool is_node = false, is_leaf = false;
+  if (is_bad) {
+    is_leaf = true;
+  } else if ((float)n > (float)P.leaf_max_points) {
+    is_node = true;
+    for (int i = 0; i < 3; ++i) nd.dir[i] = (float)e2[i];
+  } else {
+    is_leaf = true;
+    for (int i = 0; i < 3; ++i) nd.dir[i] = (float)e0[i];
+  }
+  bool has_prop = false;
+  double prop[3] = {0, 0, 0};
+  if (nd.has_parent && P.propagate_normal) {
+    has_prop = nd.par_has != 0;
+    for (int i = 0; i < 3; ++i) prop[i] = nd.par_prop[i];
+  }
+  bool is_flat = false;
+  bool do_prop = false;
+  if (is_bad || (float)n < (float)P.leaf_min_points) {
+    do_prop = true;
+  } else {
+    double eigenratio = lam[0] / lam[2];
+    is_flat = eigenratio < (double)P.leaf_normal_eigenratio &&
+              fabs(ddot3(mean_d, e0)) > (double)P.leaf_min_normal_incidence;
+    if (is_flat) {
+      has_prop = true;
+      for (int i = 0; i < 3; ++i) prop[i] = e0[i];
+    }
+    if (!is_node) {
+      double volume = lam[1] * lam[2];
+      double density = (double)n / volume;
+      if (density < (double)P.leaf_density) {
+        is_leaf = false;
+        is_node = true;
+        for (int i = 0; i < 3; ++i) nd.dir[i] = (float)e2[i];
+      } else if (is_leaf && is_flat) {
+        for (int i = 0; i < 3; ++i) nd.dir[i] = (float)e0[i];
+      } else {
+        do_prop = true;
+      }
+    }
+  }
+  if (do_prop) {
+    is_leaf = true;
+    if (has_prop) {
+      double d[3] = {prop[0], prop[1], prop[2]};
+      if (ddot3(mean_d, d) > 0.0) for (int i = 0; i < 3; ++i) d[i] = -d[i];
+      for (int i = 0; i < 3; ++i) nd.dir[i] = (float)d[i];
+    }
+  }
+  if (is_node && nd.level >= P.max_level - 1) {
+    is_node = false;
+    if (is_flat) {
+      for (int i = 0; i < 3; ++i) nd.dir[i] = (float)e0[i];
+    } else if (has_prop) {
+      double d[3] = {prop[0], prop[1], prop[2]};
+      if (ddot3(mean_d, d) > 0.0) for (int i = 0; i < 3; ++i) d[i] = -d[i];
+      for (int i = 0; i < 3; ++i) nd.dir[i] = (float)d[i];
+    } else {
+      for (int i = 0; i < 3; ++i) nd.dir[i] = (float)e0[i];
+    }
+  }
+  nd.split = is_node ? 1 : 0;
+  nd.has_prop = has_prop ? 1 : 0;
+  for (int i = 0; i < 3; ++i) nd.prop[i] = prop[i];
+}
+
+__device__ __forceinline__ bool which_side_f(const float* mean, const float* dir, float4 q) {
+  F3 d = sub3x(f3(q.x, q.y, q.z), f3(mean[0], mean[1], mean[2]));
+  return dot3x(f3(dir[0], dir[1], dir[2]), d) > 0.0f;
+}
+
+// block-wide exclusive scan of one int per thread; *total = block sum
+__device__ __forceinline__ int block_scan(int v, int* sm, int* total) {
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+  for (int off = 1; off < 32; off <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) sm[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int nw = blockDim.x >> 5;
+    int y = (lane < nw) ? sm[lane] : 0;
+    for (int off = 1; off < 32; off <<= 1) {
+      int z = __shfl_up_sync(0xffffffffu, y, off);
+      if (lane >= off) y += z;
+    }
+    if (lane < nw) sm[lane] = y;
+  }
+  __syncthreads();
+  int wprefix = (w > 0) ? sm[w - 1] : 0;
+  *total = sm[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return wprefix + x - v;
+}
+
+// ---------------------------------------------------------------------------
+// Kernels
+
+__global__ void k_ingest(const float* xyz, const double* st, int64_t n, float4* pts, double* sts, int32_t* ids,
+                         LevelState* ls) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+    double s = st ? st[i] : 0.0;
+    bool ok = fabsf(x) < 32768.f && fabsf(y) < 32768.f && fabsf(z) < 32768.f && isfinite(s);
+    if (!ok) ls->error = 2;
+    pts[i] = make_float4(x, y, z, 0.f);
+    sts[i] = s;
+    ids[i] = (int32_t)i;
+  }
+}
+
+// One block per tree: ts_start = min stamp (label_policy_base_impl_.h:28-35); dt range check.
+__global__ void k_tree_prep(const double* sts, const int64_t* off, int R, double* ts0, LevelState* ls) {
+  __shared__ double sm[kThreads];
+  int r = blockIdx.x;
+  if (r >= R) return;
+  int64_t b = off[r], e = off[r + 1];
+  double m = 1.0e308;
+  for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) m = fmin(m, sts[i]);
+  sm[threadIdx.x] = m;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sm[threadIdx.x] = fmin(sm[threadIdx.x], sm[threadIdx.x + s]);
+    __syncthreads();
+  }
+  double t0 = (e > b) ? sm[0] : 0.0;
+  if (threadIdx.x == 0) ts0[r] = t0;
+  for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x)
+    if (!(sts[i] - t0 < 65536.0)) ls->error = 2;
+}
+
+__global__ void k_init_roots(BNode* nodes, const int64_t* off, int R, LevelState* ls, int32_t* level_begin) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < R) {
+    BNode nd;
+    memset(&nd, 0, sizeof(nd));
+    nd.start = (int32_t)off[r];
+    nd.end = (int32_t)off[r + 1];
+    nd.tree = r;
+    nd.left = nd.right = -1;
+    nodes[r] = nd;
+    atomicMax(&ls->max_size, nd.end - nd.start);
+  }
+  if (r == 0) {
+    ls->lb = 0;
+    ls->le = R;
+    ls->cur = 0;
+    ls->depth = 0;
+    ls->max_next = 0;
+    level_begin[0] = 0;
+  }
+}
+
+struct PointBufs {
+  float4* p[2];
+  double* s[2];
+  int32_t* id[2];
+  int32_t* perm;  // final point order (global indices)
+};
+
+// Warp per small node: moments, decision, stable partition (or leaf placement).
+__global__ void __launch_bounds__(kThreads) k_small(BNode* nodes, const LevelState* ls, PointBufs B,
+                                                    const double* ts0, BuildParams P) {
+  const int lb = ls->lb, le = ls->le, cur = ls->cur;
+  if (lb >= le) return;
+  const float4* pin = B.p[cur];
+  const double* sin_ = B.s[cur];
+  const int32_t* iin = B.id[cur];
+  float4* pout = B.p[cur ^ 1];
+  double* sout = B.s[cur ^ 1];
+  int32_t* iout = B.id[cur ^ 1];
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int ni = lb + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); ni < le; ni += nwarps) {
+    BNode nd = nodes[ni];
+    int s = nd.start, e = nd.end;
+    int n = e - s;
+    if (n > kBig) continue;
+    double t0 = ts0[nd.tree];
+    Moments M;
+    for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
+    for (int i = s + lane; i < e; i += 32) moments_add_point(M, pin[i], sin_[i], t0);
+    for (int off = 16; off > 0; off >>= 1)
+      for (int k = 0; k < 11; ++k) M.s[k] = u128_add(M.s[k], shfl_xor_u128(M.s[k], off));
+    decide(M, n, nd, P);
+    if (nd.split) {
+      int nl = 0;
+      for (int base = s; base < e; base += 32) {
+        int i = base + lane;
+        bool left = false;
+        if (i < e) left = which_side_f(nd.mean, nd.dir, pin[i]);
+        nl += __popc(__ballot_sync(0xffffffffu, left));
+      }
+      int cl = 0, cr = 0;
+      unsigned lt = (1u << lane) - 1u;
+      for (int base = s; base < e; base += 32) {
+        int i = base + lane;
+        bool valid = i < e;
+        bool left = false;
+        float4 p;
+        if (valid) { p = pin[i]; left = which_side_f(nd.mean, nd.dir, p); }
+        unsigned bl = __ballot_sync(0xffffffffu, valid && left);
+        unsigned br = __ballot_sync(0xffffffffu, valid && !left);
+        if (valid) {
+          int dst = left ? (s + cl + __popc(bl & lt)) : (s + nl + cr + __popc(br & lt));
+          pout[dst] = p;
+          sout[dst] = sin_[i];
+          iout[dst] = iin[i];
+        }
+        cl += __popc(bl);
+        cr += __popc(br);
+      }
+      nd.mid = s + nl;
+    } else {
+      for (int i = s + lane; i < e; i += 32) B.perm[i] = iin[i];
+      nd.mid = e;
+    }
+    if (lane == 0) nodes[ni] = nd;
+  }
+}
+
+// ---- large nodes ------------------------------------------------------------------
+struct Chunk {
+  int32_t node;
+  int32_t begin;
+  int32_t end;
+  int32_t big;  // ordinal among the level's large nodes
+};
+
+// One block: lists the level's large nodes and their chunks (block scans with carry).
+__global__ void k_big_plan(const BNode* nodes, LevelState* ls, Chunk* chunks, int32_t chunk_cap, int32_t* big_list,
+                           int32_t* node_chunk0, U128* acc) {
+  __shared__ int sm[32];
+  const int lb = ls->lb, le = ls->le;
+  int carry_c = 0, carry_b = 0;
+  for (int base = lb; base < le; base += blockDim.x) {
+    int i = base + threadIdx.x;
+    int n = 0;
+    if (i < le) n = nodes[i].end - nodes[i].start;
+    bool big = n > kBig;
+    int nc = big ? (n + kChunk - 1) / kChunk : 0;
+    int tc, tb;
+    int oc = block_scan(nc, sm, &tc) + carry_c;
+    int ob = block_scan(big ? 1 : 0, sm, &tb) + carry_b;
+    if (big) {
+      big_list[ob] = i;
+      node_chunk0[ob] = oc;
+      int s = nodes[i].start, e = nodes[i].end;
+      for (int k = 0; k < nc; ++k) {
+        int c = oc + k;
+        if (c < chunk_cap) {
+          chunks[c].node = i;
+          chunks[c].begin = s + k * kChunk;
+          chunks[c].end = min(s + (k + 1) * kChunk, e);
+          chunks[c].big = ob;
+        }
+      }
+      for (int k = 0; k < 11; ++k) acc[(size_t)ob * 11 + k] = u128_zero();
+    }
+    carry_c += tc;
+    carry_b += tb;
+  }
+  if (threadIdx.x == 0) {
+    ls->num_chunks = min(carry_c, chunk_cap);
+    ls->num_big = carry_b;
+    if (carry_c > chunk_cap) ls->error = 1;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_big_moments(const Chunk* chunks, const LevelState* ls,
+                                                          const PointBufs B, const double* ts0, const BNode* nodes,
+                                                          U128* acc) {
+  __shared__ U128 sm[kThreads / 32][11];
+  const int nc = ls->num_chunks, cur = ls->cur;
+  const float4* pts = B.p[cur];
+  const double* st = B.s[cur];
+  for (int ci = blockIdx.x; ci < nc; ci += gridDim.x) {
+    Chunk c = chunks[ci];
+    double t0 = ts0[nodes[c.node].tree];
+    Moments M;
+    for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
+    for (int i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) moments_add_point(M, pts[i], st[i], t0);
+    for (int off = 16; off > 0; off >>= 1)
+      for (int k = 0; k < 11; ++k) M.s[k] = u128_add(M.s[k], shfl_xor_u128(M.s[k], off));
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+      for (int k = 0; k < 11; ++k) sm[w][k] = M.s[k];
+    __syncthreads();
+    if (threadIdx.x < 11) {
+      U128 t = u128_zero();
+      for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) t = u128_add(t, sm[ww][threadIdx.x]);
+      atomic_add_u128(&acc[(size_t)c.big * 11 + threadIdx.x], t);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_big_decide(BNode* nodes, const LevelState* ls, const int32_t* big_list, const U128* acc,
+                             BuildParams P) {
+  const int nb = ls->num_big;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += gridDim.x * blockDim.x) {
+    int i = big_list[t];
+    BNode nd = nodes[i];
+    Moments M;
+    for (int k = 0; k < 11; ++k) M.s[k] = acc[(size_t)t * 11 + k];
+    decide(M, nd.end - nd.start, nd, P);
+    nodes[i] = nd;
+  }
+}
+
+__global__ void k_big_count(const Chunk* chunks, const LevelState* ls, const BNode* nodes, const PointBufs B,
+                            int32_t* chunk_nl) {
+  __shared__ int cnt;
+  const int nc = ls->num_chunks;
+  const float4* pts = B.p[ls->cur];
+  for (int ci = blockIdx.x; ci < nc; ci += gridDim.x) {
+    Chunk c = chunks[ci];
+    const BNode& nd = nodes[c.node];
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    int local = 0;
+    if (nd.split)
+      for (int i = c.begin + threadIdx.x; i < c.end; i += blockDim.x)
+        local += which_side_f(nd.mean, nd.dir, pts[i]) ? 1 : 0;
+    atomicAdd(&cnt, local);
+    __syncthreads();
+    if (threadIdx.x == 0) chunk_nl[ci] = cnt;
+    __syncthreads();
+  }
+}
+
+__global__ void k_big_offsets(BNode* nodes, const LevelState* ls, const int32_t* big_list,
+                              const int32_t* node_chunk0, const int32_t* chunk_nl, int32_t* chunk_loff) {
+  const int nb = ls->num_big, nc = ls->num_chunks;
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    int i = big_list[b];
+    int c0 = node_chunk0[b];
+    int c1 = (b + 1 < nb) ? node_chunk0[b + 1] : nc;
+    int acc = 0;
+    for (int c = c0; c < c1; ++c) { chunk_loff[c] = acc; acc += chunk_nl[c]; }
+    BNode& nd = nodes[i];
+    nd.mid = nd.split ? nd.start + acc : nd.end;
+  }
+}
+
+// stable scatter of one chunk: each thread owns a contiguous run of points
+__global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, const LevelState* ls,
+                                                          const BNode* nodes, PointBufs B,
+                                                          const int32_t* chunk_loff) {
+  __shared__ int sc[kThreads];
+  const int nc = ls->num_chunks, cur = ls->cur;
+  const float4* pin = B.p[cur];
+  const double* sin_ = B.s[cur];
+  const int32_t* iin = B.id[cur];
+  float4* pout = B.p[cur ^ 1];
+  double* sout = B.s[cur ^ 1];
+  int32_t* iout = B.id[cur ^ 1];
+  for (int ci = blockIdx.x; ci < nc; ci += gridDim.x) {
+    Chunk c = chunks[ci];
+    const BNode& nd = nodes[c.node];
+    int len = c.end - c.begin;
+    if (!nd.split) {
+      for (int i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) B.perm[i] = iin[i];
+      continue;  // uniform per block
+    }
+    int per = (len + blockDim.x - 1) / blockDim.x;
+    int b0 = c.begin + threadIdx.x * per;
+    int b1 = min(b0 + per, c.end);
+    int mine = 0;
+    for (int i = b0; i < b1; ++i) mine += which_side_f(nd.mean, nd.dir, pin[i]) ? 1 : 0;
+    __syncthreads();
+    sc[threadIdx.x] = mine;
+    __syncthreads();
+    for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+      int v = (threadIdx.x >= (unsigned)off) ? sc[threadIdx.x - off] : 0;
+      __syncthreads();
+      sc[threadIdx.x] += v;
+      __syncthreads();
+    }
+    int lbefore = sc[threadIdx.x] - mine;
+    int loff = chunk_loff[ci] + lbefore;
+    int pbefore = (c.begin - nd.start) + (b0 - c.begin);
+    int roff = pbefore - loff;
+    int nl_total = nd.mid - nd.start;
+    for (int i = b0; i < b1; ++i) {
+      float4 p = pin[i];
+      int dst;
+      if (which_side_f(nd.mean, nd.dir, p)) dst = nd.start + loff++;
+      else dst = nd.start + nl_total + roff++;
+      pout[dst] = p;
+      sout[dst] = sin_[i];
+      iout[dst] = iin[i];
+    }
+  }
+}
+
+// ---- children ------------------------------------------------------------------------
+__device__ __forceinline__ void level_range(const LevelState* ls, int& b, int& e) {
+  const int lb = ls->lb, le = ls->le;
+  const int nl = le - lb;
+  const int per = (nl + gridDim.x - 1) / gridDim.x;
+  b = lb + blockIdx.x * per;
+  e = min(b + per, le);
+}
+
+__global__ void k_level_sums(const BNode* nodes, const LevelState* ls, int32_t* bsum) {
+  __shared__ int sm[32];
+  int b, e;
+  level_range(ls, b, e);
+  int v = 0;
+  for (int i = b + threadIdx.x; i < e; i += blockDim.x) v += nodes[i].split ? 1 : 0;
+  int total;
+  block_scan(v, sm, &total);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void k_level_children(BNode* nodes, LevelState* ls, const int32_t* bsum, int32_t cap) {
+  __shared__ int sm[32];
+  int b, e;
+  level_range(ls, b, e);
+  const int le = ls->le;
+  int pre = 0;
+  for (int k = 0; k < (int)blockIdx.x; ++k) pre += bsum[k];
+  int carry = 0;
+  for (int base = b; base < e; base += blockDim.x) {
+    int i = base + threadIdx.x;
+    bool sp = (i < e) && nodes[i].split;
+    int tot;
+    int r = block_scan(sp ? 1 : 0, sm, &tot) + carry + pre;
+    carry += tot;
+    if (i < e) {
+      BNode& nd = nodes[i];
+      if (!sp) {
+        nd.left = -1;
+        nd.right = -1;
+      } else {
+        int li = le + 2 * r;
+        if (li + 1 >= cap) {
+          ls->error = 1;
+          nd.split = 0;
+          nd.left = nd.right = -1;
+        } else {
+          nd.left = li;
+          nd.right = li + 1;
+          for (int k = 0; k < 2; ++k) {
+            BNode c;
+            memset(&c, 0, sizeof(c));
+            c.start = k == 0 ? nd.start : nd.mid;
+            c.end = k == 0 ? nd.mid : nd.end;
+            c.level = nd.level + 1;
+            c.tree = nd.tree;
+            c.left = c.right = -1;
+            c.has_parent = 1;
+            c.par_has = nd.has_prop;
+            for (int j = 0; j < 3; ++j) c.par_prop[j] = nd.prop[j];
+            nodes[li + k] = c;
+            atomicMax(&ls->max_next, c.end - c.start);
+          }
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_level_advance(LevelState* ls, const int32_t* bsum, int nblocks, int32_t* level_begin) {
+  if (ls->lb >= ls->le) return;
+  int total = 0;
+  for (int k = 0; k < nblocks; ++k) total += bsum[k];
+  ls->lb = ls->le;
+  ls->le = ls->le + 2 * total;
+  ls->cur ^= 1;
+  ls->depth += 1;
+  if (ls->depth < kMaxDepth + 1) level_begin[ls->depth] = ls->lb;
+  ls->max_size = ls->max_next;
+  ls->max_next = 0;
+}
+
+// ---- prune and per-tree compaction -----------------------------------------------------
+__global__ void k_alive(const BNode* nodes, int32_t lb, int32_t le, int32_t* alive, float incidence) {
+  int i = lb + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= le) return;
+  const BNode& nd = nodes[i];
+  int a;
+  if (nd.left < 0 && nd.right < 0) {
+    // IsGoodLeafPredicate_ in float (kd/tree/tree_predicates_.h:18-29)
+    F3 d = f3(nd.dir[0], nd.dir[1], nd.dir[2]);
+    F3 m = f3(nd.mean[0], nd.mean[1], nd.mean[2]);
+    bool ok = dot3x(d, d) > 0.0f && fabsf(dot3x(m, d)) > incidence;
+    a = ok ? 1 : 0;
+  } else {
+    a = ((nd.left >= 0 && alive[nd.left]) || (nd.right >= 0 && alive[nd.right])) ? 1 : 0;
+  }
+  alive[i] = a;
+}
+
+// group = (level, tree); nodes of one group are contiguous in global order
+__global__ void k_group_counts(const BNode* nodes, int32_t total, const int32_t* alive, int R, int32_t* cnt,
+                               int32_t* lcnt, int32_t* ucnt, int32_t* leaf_flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const BNode& nd = nodes[i];
+    int g = nd.level * R + nd.tree;
+    atomicAdd(&ucnt[nd.tree], 1);
+    int lf = 0;
+    if (alive[i]) {
+      atomicAdd(&cnt[g], 1);
+      if (nd.left < 0 && nd.right < 0) {
+        atomicAdd(&lcnt[g], 1);
+        lf = 1;
+      }
+    }
+    leaf_flag[i] = lf;
+  }
+}
+
+// exclusive prefix over groups in (level, tree) order, and per-tree level offsets
+__global__ void k_group_tables(int depth, int R, const int32_t* cnt, const int32_t* lcnt, int32_t* gp, int32_t* lgp,
+                               int32_t* to, int32_t* lto, int32_t* tot_nodes, int32_t* tot_leaves) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int a = 0, la = 0;
+  for (int l = 0; l < depth; ++l)
+    for (int t = 0; t < R; ++t) {
+      int g = l * R + t;
+      gp[g] = a;
+      lgp[g] = la;
+      a += cnt[g];
+      la += lcnt[g];
+    }
+  for (int t = 0; t < R; ++t) {
+    int s = 0, ls = 0;
+    for (int l = 0; l < depth; ++l) {
+      int g = l * R + t;
+      to[g] = s;
+      lto[g] = ls;
+      s += cnt[g];
+      ls += lcnt[g];
+    }
+    tot_nodes[t] = s;
+    tot_leaves[t] = ls;
+  }
+}
+
+__global__ void k_compact_forest(const BNode* nodes, int32_t total, const int32_t* alive, const int32_t* rank,
+                                 const int32_t* leaf_flag, const int32_t* lrank, int R, const int32_t* gp,
+                                 const int32_t* lgp, const int32_t* to, const int32_t* lto, TreeDev* trees) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    if (!alive[i]) continue;
+    const BNode& nd = nodes[i];
+    TreeDev& T = trees[nd.tree];
+    if (T.nodes == nullptr) continue;  // rejected tree
+    int g = nd.level * R + nd.tree;
+    int o = to[g] + (rank[i] - gp[g]);
+    int gc = (nd.level + 1) * R + nd.tree;
+    int l = (nd.left >= 0 && alive[nd.left]) ? to[gc] + (rank[nd.left] - gp[gc]) : -1;
+    int r = (nd.right >= 0 && alive[nd.right]) ? to[gc] + (rank[nd.right] - gp[gc]) : -1;
+    DNode d;
+    d.a = make_float4(nd.mean[0], nd.mean[1], nd.mean[2], nd.dir[0]);
+    d.b = make_float4(nd.dir[1], nd.dir[2], __int_as_float(l), __int_as_float(r));
+    T.nodes[o] = d;
+    T.dts_f[o] = (float)nd.dts_mean;
+    T.dts_mean[o] = nd.dts_mean;
+    T.dts_cov[o] = nd.dts_cov;
+    int64_t base = nd.start;  // ranges are global; made tree-relative below
+    T.range[2 * o] = base;
+    T.range[2 * o + 1] = nd.end;
+    T.level[o] = nd.level;
+    if (leaf_flag[i]) T.leaf_idx[lto[g] + (lrank[i] - lgp[g])] = o;
+  }
+}
+
+// tree-relative point ranges and point order; blockIdx.y = tree
+__global__ void k_finish_trees(TreeDev* trees, const int64_t* off, const int32_t* perm_final) {
+  const int r = blockIdx.y;
+  TreeDev& T = trees[r];
+  if (T.nodes == nullptr) return;
+  const int64_t o0 = off[r];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < T.num_nodes;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    T.range[2 * i] -= o0;
+    T.range[2 * i + 1] -= o0;
+  }
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < T.num_points;
+       i += (int64_t)gridDim.x * blockDim.x)
+    T.perm[i] = perm_final[o0 + i] - (int32_t)o0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < T.num_leaves;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int o = T.leaf_idx[i];
+    DNode d = T.nodes[o];
+    T.leaf_md[i] = make_float4(d.a.x, d.a.y, d.a.z, T.dts_f[o]);
+    T.leaf_nrm[i] = make_float4(d.a.w, d.b.x, d.b.y, 0.f);
+  }
+}
+
+inline int nblk(int64_t n, int t) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + t - 1) / t, 1 << 20)); }
+
+template <class T> T* carve(char*& p, size_t count) {
+  size_t bytes = (count * sizeof(T) + 255) & ~(size_t)255;
+  T* r = reinterpret_cast<T*>(p);
+  p += bytes;
+  return r;
+}
+template <class T> size_t carve_size(size_t count) { return (count * sizeof(T) + 255) & ~(size_t)255; }
+
+struct BuildWs {
+  void* block = nullptr;
+  PointBufs B;
+  BNode* nodes;
+  int32_t *alive, *rank, *leaf_flag, *lrank, *tile_sums;
+  Chunk* chunks;
+  int32_t *chunk_nl, *chunk_loff, *big_list, *node_chunk0;
+  U128* acc;
+  double* ts0;
+  int64_t* off;
+  LevelState* ls;
+  int32_t* level_begin;
+  int32_t* bsum;
+  int32_t *cnt, *lcnt, *ucnt, *gp, *lgp, *to, *lto, *tot_nodes, *tot_leaves, *scan_tot;
+  TreeDev* trees;
+  int64_t cap_nodes;
+  int32_t chunk_cap;
+};
+
+int ws_alloc(BuildWs& w, int64_t n, int R, cudaStream_t s) {
+  w.cap_nodes = 2 * n + 4096 + 4 * (int64_t)R;
+  w.chunk_cap = (int32_t)(n / kChunk + n / kBig + 16);
+  const int64_t cn = w.cap_nodes;
+  const int64_t ntiles = cn / 4096 + 2;
+  const int64_t G = (int64_t)(kMaxDepth + 2) * R;
+  size_t bytes = 2 * carve_size<float4>(n) + 2 * carve_size<double>(n) + 3 * carve_size<int32_t>(n) +
+                 carve_size<BNode>(cn) + 4 * carve_size<int32_t>(cn) + carve_size<int32_t>(ntiles) +
+                 carve_size<Chunk>(w.chunk_cap) + 4 * carve_size<int32_t>(w.chunk_cap) +
+                 carve_size<U128>((size_t)11 * (n / kBig + 2)) + carve_size<double>(R) +
+                 carve_size<int64_t>(R + 1) + carve_size<LevelState>(1) + carve_size<int32_t>(kMaxDepth + 2) +
+                 carve_size<int32_t>(kLevelBlocks) + 7 * carve_size<int32_t>(G) + 3 * carve_size<int32_t>(R) +
+                 carve_size<int32_t>(8) + carve_size<TreeDev>(R) + 256;
+  cudaError_t e = cudaMallocAsync(&w.block, bytes, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    w.block = nullptr;
+    set_error("cudaMallocAsync of %zu bytes for the tree build workspace failed: %s", bytes, cudaGetErrorString(e));
+    return KDS_ERR_OOM;
+  }
+  char* p = (char*)w.block;
+  w.B.p[0] = carve<float4>(p, n);
+  w.B.p[1] = carve<float4>(p, n);
+  w.B.s[0] = carve<double>(p, n);
+  w.B.s[1] = carve<double>(p, n);
+  w.B.id[0] = carve<int32_t>(p, n);
+  w.B.id[1] = carve<int32_t>(p, n);
+  w.B.perm = carve<int32_t>(p, n);
+  w.nodes = carve<BNode>(p, cn);
+  w.alive = carve<int32_t>(p, cn);
+  w.rank = carve<int32_t>(p, cn);
+  w.leaf_flag = carve<int32_t>(p, cn);
+  w.lrank = carve<int32_t>(p, cn);
+  w.tile_sums = carve<int32_t>(p, ntiles);
+  w.chunks = carve<Chunk>(p, w.chunk_cap);
+  w.chunk_nl = carve<int32_t>(p, w.chunk_cap);
+  w.chunk_loff = carve<int32_t>(p, w.chunk_cap);
+  w.big_list = carve<int32_t>(p, w.chunk_cap);
+  w.node_chunk0 = carve<int32_t>(p, w.chunk_cap);
+  w.acc = carve<U128>(p, (size_t)11 * (n / kBig + 2));
+  w.ts0 = carve<double>(p, R);
+  w.off = carve<int64_t>(p, R + 1);
+  w.ls = carve<LevelState>(p, 1);
+  w.level_begin = carve<int32_t>(p, kMaxDepth + 2);
+  w.bsum = carve<int32_t>(p, kLevelBlocks);
+  w.cnt = carve<int32_t>(p, G);
+  w.lcnt = carve<int32_t>(p, G);
+  w.gp = carve<int32_t>(p, G);
+  w.lgp = carve<int32_t>(p, G);
+  w.to = carve<int32_t>(p, G);
+  w.lto = carve<int32_t>(p, G);
+  w.ucnt = carve<int32_t>(p, G);
+  w.tot_nodes = carve<int32_t>(p, R);
+  w.tot_leaves = carve<int32_t>(p, R);
+  w.scan_tot = carve<int32_t>(p, R);
+  w.trees = carve<TreeDev>(p, R);
+  return KDS_OK;
+}
+
+}  // namespace
+
+// Builds R trees from R clouds stored back to back (offsets[R+1] on the host).
+// out[r] = NULL and status[r] = KDS_ERR_TREE_REJECTED where makeTree returns nullptr.
+int tree_build_forest(const float* xyz, const double* stamps, const int64_t* offsets, int32_t R, int32_t mem,
+                      const kds_tree_params* prm, cudaStream_t s, kds_tree** out, int32_t* status) {
+  for (int r = 0; r < R; ++r) { out[r] = nullptr; status[r] = KDS_ERR_TREE_REJECTED; }
+  if (R <= 0) { set_error("kds_tree_build: no clouds"); return KDS_ERR_INVALID_ARG; }
+  const int64_t N = offsets[R] - offsets[0];
+  if (offsets[0] != 0 || N < 0 || N > ((int64_t)1 << 30)) {
+    set_error("kds_tree_build: bad point count / offsets");
+    return KDS_ERR_INVALID_ARG;
+  }
+  std::vector<int64_t> off(offsets, offsets + R + 1);
+  int32_t max_size = 0;
+  for (int r = 0; r < R; ++r) {
+    if (off[r + 1] < off[r]) { set_error("kds_tree_build: offsets must be non-decreasing"); return KDS_ERR_INVALID_ARG; }
+    max_size = std::max<int32_t>(max_size, (int32_t)(off[r + 1] - off[r]));
+  }
+  BuildParams P;
+  P.propagate_normal = prm->propagate_normal;
+  P.leaf_min_points = prm->leaf_min_points;
+  P.leaf_max_points = prm->leaf_max_points;
+  P.leaf_density = prm->leaf_density;
+  P.leaf_min_normal_incidence = prm->leaf_min_normal_incidence;
+  P.leaf_normal_eigenratio = prm->leaf_normal_eigenratio;
+  P.prune_incidence = prm->prune_min_normal_incidence;
+  P.max_level = prm->max_level > 0 ? std::min(prm->max_level, kMaxDepth) : 48;
+  if (N == 0) return KDS_OK;  // every cloud rejected (fewer points than leaf_min_points)
+
+  BuildWs w;
+  int rc = ws_alloc(w, std::max<int64_t>(N, 1), R, s);
+  if (rc) return rc;
+  struct Guard {
+    BuildWs* w;
+    cudaStream_t s;
+    void* h_xyz = nullptr;
+    void* h_st = nullptr;
+    ~Guard() {
+      if (w->block) cudaFreeAsync(w->block, s);
+      if (h_xyz) cudaFreeAsync(h_xyz, s);
+      if (h_st) cudaFreeAsync(h_st, s);
+    }
+  } guard{&w, s};
+  const float* d_xyz = xyz;
+  const double* d_st = stamps;
+  if (mem == KDS_MEM_HOST) {
+    KDS_CK(cudaMallocAsync(&guard.h_xyz, sizeof(float) * 3 * N, s));
+    KDS_CK(cudaMemcpyAsync(guard.h_xyz, xyz, sizeof(float) * 3 * N, cudaMemcpyHostToDevice, s));
+    d_xyz = (const float*)guard.h_xyz;
+    if (stamps) {
+      KDS_CK(cudaMallocAsync(&guard.h_st, sizeof(double) * N, s));
+      KDS_CK(cudaMemcpyAsync(guard.h_st, stamps, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+      d_st = (const double*)guard.h_st;
+    }
+  }
+  KDS_CK(cudaMemsetAsync(w.ls, 0, sizeof(LevelState), s));
+  KDS_CK(cudaMemcpyAsync(w.off, off.data(), sizeof(int64_t) * (R + 1), cudaMemcpyHostToDevice, s));
+  k_ingest<<<nblk(N, kThreads), kThreads, 0, s>>>(d_xyz, d_st, N, w.B.p[0], w.B.s[0], w.B.id[0], w.ls);
+  count_launch();
+  k_tree_prep<<<R, kThreads, 0, s>>>(w.B.s[0], w.off, R, w.ts0, w.ls);
+  count_launch();
+  k_init_roots<<<(R + 127) / 128, 128, 0, s>>>(w.nodes, w.off, R, w.ls, w.level_begin);
+  count_launch();
+  KDS_CK(cudaGetLastError());
+
+  LevelState hls;
+  std::vector<int32_t> level_begin(kMaxDepth + 2, 0);
+  int32_t host_max = max_size;
+  const int cb = std::min<int>(w.chunk_cap, kGridBlocks * 2);
+  for (int round = 0; round < kMaxDepth; ++round) {
+    for (int k = 0; k < kLevelsPerSync; ++k) {
+      k_small<<<kGridBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.B, w.ts0, P);
+      count_launch();
+      if (host_max > kBig) {
+        k_big_plan<<<1, 1024, 0, s>>>(w.nodes, w.ls, w.chunks, w.chunk_cap, w.big_list, w.node_chunk0, w.acc);
+        k_big_moments<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.B, w.ts0, w.nodes, w.acc);
+        k_big_decide<<<64, 128, 0, s>>>(w.nodes, w.ls, w.big_list, w.acc, P);
+        k_big_count<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_nl);
+        k_big_offsets<<<64, 128, 0, s>>>(w.nodes, w.ls, w.big_list, w.node_chunk0, w.chunk_nl, w.chunk_loff);
+        k_big_scatter<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_loff);
+        for (int c = 0; c < 6; ++c) count_launch();
+      }
+      k_level_sums<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum);
+      k_level_children<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum, (int32_t)w.cap_nodes);
+      k_level_advance<<<1, 1, 0, s>>>(w.ls, w.bsum, kLevelBlocks, w.level_begin);
+      for (int c = 0; c < 3; ++c) count_launch();
+    }
+    KDS_CK(cudaGetLastError());
+    KDS_CK(cudaMemcpyAsync(&hls, w.ls, sizeof(LevelState), cudaMemcpyDeviceToHost, s));
+    KDS_CK(cudaStreamSynchronize(s));
+    if (hls.error == 2) { set_error("kds_tree_build: coordinate >= 32768 m, non-finite stamp or dt >= 65536 s"); return KDS_ERR_RANGE; }
+    if (hls.error == 1) { set_error("kds_tree_build: node capacity exceeded"); return KDS_ERR_CAPACITY; }
+    if (hls.lb >= hls.le) break;
+    host_max = hls.max_size;
+  }
+  if (hls.lb < hls.le) { set_error("kds_tree_build: depth limit"); return KDS_ERR_CAPACITY; }
+  const int depth = hls.depth;
+  const int32_t total = hls.le;
+  KDS_CK(cudaMemcpyAsync(level_begin.data(), w.level_begin, sizeof(int32_t) * (kMaxDepth + 2),
+                         cudaMemcpyDeviceToHost, s));
+  KDS_CK(cudaStreamSynchronize(s));
+  level_begin[depth] = total;
+  // prune: bottom-up per level
+  for (int l = depth - 1; l >= 0; --l) {
+    int32_t b = level_begin[l], e = level_begin[l + 1];
+    if (e > b) {
+      k_alive<<<nblk(e - b, kThreads), kThreads, 0, s>>>(w.nodes, b, e, w.alive, P.prune_incidence);
+      count_launch();
+    }
+  }
+  const int64_t G = (int64_t)(kMaxDepth + 2) * R;
+  KDS_CK(cudaMemsetAsync(w.cnt, 0, sizeof(int32_t) * G, s));
+  KDS_CK(cudaMemsetAsync(w.lcnt, 0, sizeof(int32_t) * G, s));
+  KDS_CK(cudaMemsetAsync(w.ucnt, 0, sizeof(int32_t) * G, s));
+  k_group_counts<<<nblk(total, kThreads), kThreads, 0, s>>>(w.nodes, total, w.alive, R, w.cnt, w.lcnt, w.ucnt,
+                                                            w.leaf_flag);
+  count_launch();
+  rc = scan_exclusive(w.alive, w.rank, total, w.tile_sums, w.scan_tot, s);
+  if (rc) return rc;
+  rc = scan_exclusive(w.leaf_flag, w.lrank, total, w.tile_sums, w.scan_tot, s);
+  if (rc) return rc;
+  k_group_tables<<<1, 1, 0, s>>>(depth, R, w.cnt, w.lcnt, w.gp, w.lgp, w.to, w.lto, w.tot_nodes, w.tot_leaves);
+  count_launch();
+  std::vector<int32_t> tn(R), tl(R), tu(R);
+  std::vector<double> ts0(R);
+  KDS_CK(cudaMemcpyAsync(tn.data(), w.tot_nodes, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, s));
+  KDS_CK(cudaMemcpyAsync(tl.data(), w.tot_leaves, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, s));
+  KDS_CK(cudaMemcpyAsync(tu.data(), w.ucnt, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, s));
+  KDS_CK(cudaMemcpyAsync(ts0.data(), w.ts0, sizeof(double) * R, cudaMemcpyDeviceToHost, s));
+  KDS_CK(cudaStreamSynchronize(s));
+  std::vector<TreeDev> td(R);
+  std::vector<kds_tree*> made(R, nullptr);
+  for (int r = 0; r < R; ++r) {
+    int64_t np = off[r + 1] - off[r];
+    if (np < prm->leaf_min_points || np == 0 || tl[r] < prm->tree_min_good_leaves) continue;
+    kds_tree* t = new kds_tree();
+    rc = tree_alloc(t->d, tn[r], tl[r], np, s);
+    if (rc) {
+      delete t;
+      for (int q = 0; q < r; ++q)
+        if (made[q]) { tree_release(made[q]->d); delete made[q]; }
+      return rc;
+    }
+    t->d.num_unpruned = tu[r];
+    t->d.ts_start = ts0[r];
+    t->d.depth = depth;
+    made[r] = t;
+    td[r] = t->d;
+  }
+  KDS_CK(cudaMemcpyAsync(w.trees, td.data(), sizeof(TreeDev) * R, cudaMemcpyHostToDevice, s));
+  k_compact_forest<<<nblk(total, kThreads), kThreads, 0, s>>>(w.nodes, total, w.alive, w.rank, w.leaf_flag, w.lrank,
+                                                              R, w.gp, w.lgp, w.to, w.lto, w.trees);
+  count_launch();
+  dim3 fg((unsigned)std::min<int64_t>(nblk(max_size, kThreads), 256), (unsigned)R);
+  k_finish_trees<<<fg, kThreads, 0, s>>>(w.trees, w.off, w.B.perm);
+  count_launch();
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    for (auto* t : made)
+      if (t) { tree_release(t->d); delete t; }
+    return cuda_status(e, "tree build", __FILE__, __LINE__);
+  }
+  for (int r = 0; r < R; ++r) {
+    out[r] = made[r];
+    status[r] = made[r] ? KDS_OK : KDS_ERR_TREE_REJECTED;
+  }
+  return KDS_OK;
+}
+
+int tree_build(const float* xyz, const double* stamps, int64_t n, int32_t mem, const kds_tree_params* prm,
+               cudaStream_t s, kds_tree** out) {
+  *out = nullptr;
+  if (n < 0 || n > ((int64_t)1 << 30)) {
+    set_error("kds_tree_build: bad point count %lld", (long long)n);
+    return KDS_ERR_INVALID_ARG;
+  }
+  if (n < prm->leaf_min_points || n == 0) {
+    set_error("kds_tree_build: %lld points < leaf_min_points", (long long)n);
+    return KDS_ERR_TREE_REJECTED;
+  }
+  int64_t off[2] = {0, n};
+  int32_t st = 0;
+  int rc = tree_build_forest(xyz, stamps, off, 1, mem, prm, s, out, &st);
+  if (rc) return rc;
+  if (st != KDS_OK) {
+    set_error("kds_tree_build: too few good leaves (tree_min_good_leaves %d)", prm->tree_min_good_leaves);
+    return KDS_ERR_TREE_REJECTED;
+  }
+  return KDS_OK;
+}
+
+}  // namespace kds

@@ -22,6 +22,9 @@ int cuda_status(cudaError_t e, const char* what, const char* file, int line);
     if (_e != cudaSuccess) return ::kds::cuda_status(_e, #call, __FILE__, __LINE__); \
   } while (0)
 
+// Number of kernels this library has launched (process-wide), for launch accounting.
+void count_launch();
+
 inline cudaStream_t as_stream(void* s) { return s ? (cudaStream_t)s : cudaStreamPerThread; }
 int ensure_init();
 
@@ -54,9 +57,10 @@ struct TreeDev {
   float4* leaf_nrm = nullptr;     // [num_leaves] normal.xyz, 0
   int32_t* perm = nullptr;        // [num_points] input index at each final position
   void* block = nullptr;          // single allocation backing the arrays above
+  cudaStream_t stream = nullptr;  // stream the block was allocated on (stream-ordered pool)
 };
 
-int tree_alloc(TreeDev& t, int64_t nodes, int64_t leaves, int64_t points);
+int tree_alloc(TreeDev& t, int64_t nodes, int64_t leaves, int64_t points, cudaStream_t s);
 void tree_release(TreeDev& t);
 
 // Gathers leaf_md / leaf_nrm from the node arrays (after build, import or morph).
@@ -202,7 +206,12 @@ __device__ __forceinline__ void warp_x(const float* v, float dt, F3 m, F3 n, F3&
 }  // namespace kds
 
 namespace kds {
-// Tree operations (kds_tree.cu)
+// Exclusive scan of n int32 (kds_tree.cu); tile_sums needs n / 4096 + 2 entries.
+int scan_exclusive(const int32_t* in, int32_t* out, int32_t n, int32_t* tile_sums, int32_t* total, cudaStream_t s);
+// Tree build (kds_build.cu)
+int tree_build_forest(const float* xyz, const double* stamps, const int64_t* offsets, int32_t R, int32_t mem,
+                      const kds_tree_params* prm, cudaStream_t s, kds_tree** out, int32_t* status);
+// Tree operations (kds_tree.cu / kds_build.cu)
 int tree_build(const float* xyz, const double* stamps, int64_t n, int32_t mem, const kds_tree_params* p,
                cudaStream_t s, kds_tree** out);
 int tree_import(const float* mean, const float* dir, const double* dts_mean, const double* dts_cov,

@@ -43,6 +43,26 @@ def test_tree_build_bit_exact(scene, seed, beams, params):
     assert_same_tree(O, G)
 
 
+def test_forest_build_equals_single_builds(scene):
+    """One batched pass over uneven clouds gives each tree bit-identical to its own build."""
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import synth
+    clouds = []
+    for i, beams in enumerate([16, 32, 16, 64]):
+        xyz, st = make_scan(scene, 2300 + i, beams=beams, elev=(-15.0, 15.0),
+                            vel=[5.0 * i, 0, 0, 0, 0, 0.1 * i])
+        clouds.append((xyz, st + 10.0 * i))
+    clouds.insert(2, (np.zeros((3, 3), np.float32), None))  # rejected: fewer than leaf_min_points
+    gen = kds.TreeGeneratorB2003D(leaf_max_points=16, propagate_normal=1)
+    trees = gen.make_trees(clouds)
+    assert trees[2] is None
+    for (xyz, st), T in zip(clouds, trees):
+        if len(xyz) < 5:
+            continue
+        O = orc.OTree.build(xyz, st, orc.tree_params(leaf_max_points=16, propagate_normal=1))
+        assert_same_tree(O, T)
+
+
 def test_tree_build_skewed_scan_with_stamps(scene):
     from kd_slam2_b200 import synth
     xyz, st = make_scan(scene, 2010, beams=32, vel=[10.0, 0, 0, 0, 0, np.deg2rad(30.0)])

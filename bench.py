@@ -302,8 +302,16 @@ def main():
             times += timed(True, 1)
             prof.append(aligner.profile())
     barrier()
+    st16 = np.zeros(16, np.uint64)
+    kds.lib().kds_phase_stamps(st16.ctypes.data)
     aligner.set_profiling(False)
     launches = kds.lib().kds_launch_count() - launches0
+    d = lambda a, b: int(st16[b]) - int(st16[a])
+    phases = {"first_block": {"stage_tree_top": d(0, 1), "leaves": d(1, 2), "publish": d(2, 3)},
+              "gn_block": {"sum_partials": d(8, 9), "stage_state": d(9, 10), "unpack": d(10, 11),
+                           "factorize": d(11, 12), "solve": d(12, 13), "update": d(13, 14),
+                           "write_back": d(14, 15)},
+              "unit": "SM cycles"}
     ms = float(np.mean(times))
     total_s = float(np.sum(times)) / 1e3
     if dist:
@@ -324,6 +332,27 @@ def main():
     e2e_value = world * args.steps / e2e_total
     h2d = int(wl["xyz"].nbytes + wl["st"].nbytes)
     d2h = 2 * 8 * (12 + 6) + 4 * 2 + 36  # pose, velocities, result codes and stats read back
+
+    # ---- phase breakdown (device-resident): tree build alone, alignment alone
+    def phase_times(n):
+        tb, ta = [], []
+        for _ in range(n):
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            t = gen.make_tree(d_xyz, d_st, device=True, stream=sh)
+            e1.record(stream)
+            aligner.set_moving(t)
+            aligner.set_x(wl["X0"])
+            aligner.set_velocities(wl["v0"])
+            aligner.compute()
+            e2.record(stream)
+            e2.synchronize()
+            tb.append(e0.elapsed_time(e1))
+            ta.append(e1.elapsed_time(e2))
+            t.free()
+        return float(np.median(tb)), float(np.median(ta))
+
+    build_ms, align_ms = phase_times(10)
 
     # ---- roofline of the dominant kernel (fused CT linearization, k_linearize<1>)
     lin_ms = float(np.mean([p[0] for p in prof if p[1] > 0])) if prof else None
@@ -356,6 +385,8 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "p50_ms": float(np.percentile(e2e_times, 50)), "p99_ms": float(np.percentile(e2e_times, 99))},
         "gpu_launches": int(launches),
+        "breakdown_ms": {"tree_build": build_ms, "align_15_iters": align_ms, "linearize_launch": lin_ms},
+        "linearize_phases": phases,
         "roofline": roofline,
         "clocks": clk.summary(),
         "accuracy": {"ret": int(ret), "t_err_vs_truth_m": et, "r_err_vs_truth_rad": er},

@@ -220,6 +220,11 @@ int kds_aligner_linearize_debug(kds_aligner* a, const float caches[36], const fl
 int kds_aligner_set_profiling(kds_aligner* a, int32_t on);
 int kds_aligner_get_profile(const kds_aligner* a, double* mean_ms, int32_t* launches);
 int kds_aligner_count_touched_nodes(kds_aligner* a, int64_t* count);
+/* SM-clock stamps of the last profiled linearization launch: [0..3] first block
+ * (entry, fixed-tree top staged, tile done, partial published), [8..15] the block that
+ * ran the Gauss-Newton step (entry, partials summed, state staged, factorization start,
+ * factorized, solved, pose updated, done).  Measurement hook only. */
+int kds_phase_stamps(uint64_t out[16]);
 void kds_aligner_free(kds_aligner* a);
 
 /* ------------------------------------------------------------------------------

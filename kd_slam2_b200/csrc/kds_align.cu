@@ -154,7 +154,8 @@ template <> struct KindDim<1> { static constexpr int D = 12; };
 template <> struct KindDim<2> { static constexpr int D = 18; };
 
 template <int KIND>
-__device__ __forceinline__ void leaf_term(const CacheF& C, const DNode* F, int fnn, const float* fdts, float4 md,
+__device__ __forceinline__ void leaf_term(const CacheF& C, const DNode* F, int fnn, const float* fdts,
+                                          const DNode* staged, int nstaged, float4 md,
                                           float4 nr, const ParamsF& P, bool stats_mode, int& status, int& match,
                                           float& e_out, float& gamma_out, float* J) {
   constexpr int D = KindDim<KIND>::D;
@@ -171,7 +172,7 @@ __device__ __forceinline__ void leaf_term(const CacheF& C, const DNode* F, int f
   int idx = fnn > 0 ? 0 : -1;
   DNode nd;
   while (idx >= 0) {
-    nd = load_node(F + idx);
+    nd = (idx < nstaged) ? staged[idx] : load_node(F + idx);
     int l = node_left(nd), r = node_right(nd);
     if (l < 0 && r < 0) break;
     bool side = dot3x(node_dir(nd), sub3x(q, node_mean(nd))) > 0.0f;
@@ -226,6 +227,7 @@ constexpr int kMaxFS = 21;  // factor row stride (D + 2, padded to odd)
 
 template <int KIND>
 __device__ __forceinline__ void tile_body(const JobIn& Jn, const LinDev& L, const CacheF& C, const TileDev& T,
+                                          const DNode* staged, int nstaged,
                                           double* wpart /* [kWarps][kPStride] */, float* fac /* [kWarps][32][kMaxFS] */,
                                           int32_t* dbg_match, int32_t* dbg_status) {
   constexpr int D = KindDim<KIND>::D;
@@ -240,7 +242,8 @@ __device__ __forceinline__ void tile_body(const JobIn& Jn, const LinDev& L, cons
   if (i < T.leaf_end) {
     float4 md = __ldg(Jn.m_md + i);
     float4 nr = __ldg(Jn.m_nrm + i);
-    leaf_term<KIND>(C, L.fnodes, L.f_num_nodes, L.fdts, md, nr, Jn.P, Jn.stats_mode != 0, status, match, e, gamma, J);
+    leaf_term<KIND>(C, L.fnodes, L.f_num_nodes, L.fdts, staged, nstaged, md, nr, Jn.P, Jn.stats_mode != 0, status,
+                    match, e, gamma, J);
     if (dbg_match) { dbg_match[i] = match; dbg_status[i] = status; }
   }
   bool contrib = status == ST_INLIER || status == ST_OUTLIER;
@@ -448,16 +451,93 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 // runs ICP_::oneRound / CTICP_::oneRound (kd/icp/icp_impl_.h:72-89,
 // kd/cticp/cticp_impl_.h:67-91) with the D x D system in shared memory: Cholesky of
 // H + damping (SPD), warp-parallel trailing updates and triangular solves.
-__device__ __noinline__ void job_tail(const JobIn& Jn, JobState& S, JobOut& O, kds_stats* log, LinDev* lins,
+__device__ void tail_warp(const JobIn& Jn, JobState& S, JobOut& O, kds_stats* log, LinDev* lins, double* red, int M);
+
+// Phase stamps (clock64) of the last launch, recorded only when profiling is on:
+// [0..3] block 0: entry, staged, tile done, partial published; [8..15] tail block:
+// entry, partials summed, state staged, solve start, factorized, solved, updated, done.
+__device__ int g_phase_on;
+__device__ unsigned long long g_phase[16];
+// Set by a kernel whose bounded wait on a TMA copy gave up; read and cleared by the host.
+__device__ int g_kernel_error;
+
+// Bounded wait for the phase with the given parity of an mbarrier to complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (int i = 0; i < (1 << 20); ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+constexpr int kTailJobOff = 560;    // doubles into the tail's shared scratch
+constexpr int kTailStateOff = 680;
+static_assert(kTailJobOff + sizeof(JobIn) / 8 + 1 <= kTailStateOff, "tail scratch layout");
+static_assert(kTailStateOff + sizeof(JobState) / 8 + 1 <= 4 * kPStride, "tail scratch layout");
+
+__device__ __noinline__ void job_tail(const JobIn& JnG, JobState& SG, JobOut& O, kds_stats* log, LinDev* lins,
                                       const double* partials, double* red, int M) {
+  const bool stamp = g_phase_on && threadIdx.x == 0;
+  if (stamp) g_phase[8] = clock64();
   for (int k = threadIdx.x; k < kPStride; k += blockDim.x) {
     if (k >= M && k < kPStats) { red[k] = 0.0; continue; }
     double acc = 0.0;
-    for (int t = Jn.tile_begin; t < Jn.tile_begin + Jn.tile_count; ++t) acc += __ldcg(partials + (size_t)t * kPStride + k);
+    const double* src = partials + (size_t)JnG.tile_begin * kPStride + k;
+    const int nt = JnG.tile_count;
+    double a4[4] = {0.0, 0.0, 0.0, 0.0};
+    int t = 0;
+    for (; t + 4 <= nt; t += 4) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) a4[u] += __ldcg(src + (size_t)(t + u) * kPStride);
+    }
+    for (; t < nt; ++t) a4[0] += __ldcg(src + (size_t)t * kPStride);
+    acc = (a4[0] + a4[1]) + (a4[2] + a4[3]);
     red[k] = acc;
   }
   __syncthreads();
+  if (stamp) g_phase[9] = clock64();
   if (threadIdx.x >= 32) return;
+  // the job's inputs and state move to shared memory in one parallel round trip
+  JobIn* sJn = reinterpret_cast<JobIn*>(red + kTailJobOff);
+  JobState* sS = reinterpret_cast<JobState*>(red + kTailStateOff);
+  {
+    typedef unsigned long long u64;
+    constexpr int NJ = sizeof(JobIn) / 8, NS = sizeof(JobState) / 8;
+    static_assert(sizeof(JobIn) % 8 == 0 && sizeof(JobState) % 8 == 0 && NJ <= 96 && NS <= 32, "staging");
+    const u64* a = reinterpret_cast<const u64*>(&JnG);
+    const u64* c = reinterpret_cast<const u64*>(&SG);
+    const int l = threadIdx.x;
+    u64 r0 = 0, r1 = 0, r2 = 0, r3 = 0;  // all loads issued before any store
+    if (l < NJ) r0 = a[l];
+    if (l + 32 < NJ) r1 = a[l + 32];
+    if (l + 64 < NJ) r2 = a[l + 64];
+    if (l < NS) r3 = c[l];
+    u64* b = reinterpret_cast<u64*>(sJn);
+    u64* d = reinterpret_cast<u64*>(sS);
+    if (l < NJ) b[l] = r0;
+    if (l + 32 < NJ) b[l + 32] = r1;
+    if (l + 64 < NJ) b[l + 64] = r2;
+    if (l < NS) d[l] = r3;
+  }
+  __syncwarp();
+  if (stamp) g_phase[10] = clock64();
+  tail_warp(*sJn, *sS, O, log, lins, red, M);
+  __syncwarp();
+  {
+    const unsigned long long* c = reinterpret_cast<const unsigned long long*>(sS);
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(&SG);
+    if (threadIdx.x < (int)(sizeof(JobState) / 8)) d[threadIdx.x] = c[threadIdx.x];
+  }
+  if (stamp) g_phase[15] = clock64();
+}
+
+// Warp 0 of the last block: unpack, prior, solve, update, termination test.
+__device__ void tail_warp(const JobIn& Jn, JobState& S, JobOut& O, kds_stats* log, LinDev* lins, double* red, int M) {
   const int lane = threadIdx.x;
   const int kind = Jn.kind;
   const int Dk = kind == 0 ? 6 : (kind == 1 ? 12 : 18);
@@ -531,36 +611,56 @@ __device__ __noinline__ void job_tail(const JobIn& Jn, JobState& S, JobOut& O, k
     return;
   }
   __syncwarp();
-  // Cholesky, lower triangle of sA
+  if (g_phase_on && lane == 0) g_phase[11] = clock64();
+  // Cholesky of the lower triangle of sA: per pivot one square root and reciprocal,
+  // the column scaled by the lanes, the trailing update spread over all lanes.
+  double* sinv = sx + 12;  // reciprocals of diag(L)
   bool ok = true;
   for (int k = 0; k < D; ++k) {
     double d = sA[k * D + k];
     ok = ok && (d > 0.0);
     double lkk = sqrt(fmax(d, 1e-300));
+    double inv = 1.0 / lkk;
     __syncwarp();
-    if (lane > k && lane < D) sA[lane * D + k] /= lkk;
-    if (lane == k) sA[k * D + k] = lkk;
+    if (lane > k && lane < D) sA[lane * D + k] *= inv;
+    if (lane == k) {
+      sA[k * D + k] = lkk;
+      sinv[k] = inv;
+    }
     __syncwarp();
-    for (int i = k + 1; i < D; ++i) {
-      int j = k + 1 + lane;
-      if (j <= i) sA[i * D + j] -= sA[i * D + k] * sA[j * D + k];
+    // pairs (i, j), k < j <= i < D, enumerated row-major over the trailing triangle
+    const int m = D - k - 1;
+    const int npair = m * (m + 1) / 2;
+    for (int p = lane; p < npair; p += 32) {
+      int ii = 0;
+      while ((ii + 1) * (ii + 2) / 2 <= p) ++ii;
+      const int i = k + 1 + ii, j = k + 1 + (p - ii * (ii + 1) / 2);
+      sA[i * D + j] -= sA[i * D + k] * sA[j * D + k];
     }
     __syncwarp();
   }
-  // L y = -b, then L^T x = y
-  for (int i = 0; i < D; ++i) {
-    double part = (lane < i) ? sA[i * D + lane] * sy[lane] : 0.0;
-    double sum = warp_sum_d(part);
-    if (lane == 0) sy[i] = (-sb[i] - sum) / sA[i * D + i];
+  if (g_phase_on && lane == 0) g_phase[12] = clock64();
+  // L y = -b and L^T x = y by column sweeps
+  if (lane < D) sy[lane] = -sb[lane];
+  __syncwarp();
+  for (int k = 0; k < D; ++k) {
+    const double yk = sy[k] * sinv[k];
+    __syncwarp();
+    if (lane == k) sy[k] = yk;
+    if (lane > k && lane < D) sy[lane] -= sA[lane * D + k] * yk;
     __syncwarp();
   }
-  for (int i = D - 1; i >= 0; --i) {
-    double part = (lane > i && lane < D) ? sA[lane * D + i] * sx[lane] : 0.0;
-    double sum = warp_sum_d(part);
-    if (lane == 0) sx[i] = (sy[i] - sum) / sA[i * D + i];
+  if (lane < D) sx[lane] = sy[lane];
+  __syncwarp();
+  for (int k = D - 1; k >= 0; --k) {
+    const double xk = sx[k] * sinv[k];
+    __syncwarp();
+    if (lane == k) sx[k] = xk;
+    if (lane < k) sx[lane] -= sA[k * D + lane] * xk;
     __syncwarp();
   }
   if (lane != 0) return;
+  if (g_phase_on) g_phase[13] = clock64();
   double dx[12];
   for (int i = 0; i < D; ++i) dx[i] = ok ? sx[i] : 0.0;
   double pp = 0.0, pv = 0.0;
@@ -608,6 +708,7 @@ __device__ __noinline__ void job_tail(const JobIn& Jn, JobState& S, JobOut& O, k
   for (int i = 0; i < 12; ++i) O.X[i] = S.X[i];
   for (int i = 0; i < 6; ++i) O.v[i] = S.v[i];
   if (!S.done) refresh_caches(S, lins, Jn.lin_begin, Jn.lin_count);
+  if (g_phase_on) g_phase[14] = clock64();
   S.arrive = 0u;
 }
 
@@ -615,7 +716,7 @@ __device__ __noinline__ void job_tail(const JobIn& Jn, JobState& S, JobOut& O, k
 template <int KIND>
 __global__ void __launch_bounds__(kBlock, 4) k_linearize(const JobIn* __restrict__ jobs, JobState* states, JobOut* outs,
                                                       kds_stats* logs, LinDev* lins, const TileDev* __restrict__ tiles,
-                                                      int tile0, double* partials, int32_t* dbg_match,
+                                                      int tile0, int stage, double* partials, int32_t* dbg_match,
                                                       int32_t* dbg_status) {
   constexpr int D = KindDim<KIND>::D;
   constexpr int M = D * (D + 1) / 2 + D;
@@ -623,17 +724,46 @@ __global__ void __launch_bounds__(kBlock, 4) k_linearize(const JobIn* __restrict
   __shared__ float sfac[kWarps * 32 * kMaxFS];
   __shared__ double swp[kWarps * kPStride];
   __shared__ int s_last;
+  __shared__ __align__(8) unsigned long long s_mbar;
+  const bool stamp = g_phase_on && blockIdx.x == 0 && threadIdx.x == 0;
+  if (stamp) g_phase[0] = clock64();
   const int tile = tile0 + blockIdx.x;
   const TileDev T = tiles[tile];
   JobState& S = states[T.job];
   if (*(volatile int32_t*)&S.done) return;
   const JobIn& Jn = jobs[T.job];
   const LinDev& L = lins[T.lin];
+  // Top of the fixed tree: in BFS order the first nodes are the shallowest levels.
+  // One thread issues a TMA bulk copy (cp.async.bulk, no multicast) of them into
+  // shared memory while the block loads the rest of its inputs.
+  extern __shared__ float4 sDyn[];
+  const DNode* sN = reinterpret_cast<const DNode*>(sDyn);
+  int nst = min(stage, L.f_num_nodes);
+  const uint32_t bytes = (uint32_t)nst * (uint32_t)sizeof(DNode);
+  const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&s_mbar);
+  if (threadIdx.x == 0 && bytes > 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(sDyn)),
+                 "l"(L.fnodes), "r"(bytes), "r"(mbar)
+                 : "memory");
+  }
   if (threadIdx.x < (int)(sizeof(CacheF) / 4))
     reinterpret_cast<float*>(&sC)[threadIdx.x] = reinterpret_cast<const float*>(&L.cache)[threadIdx.x];
   __syncthreads();
-  tile_body<KIND>(Jn, L, sC, T, swp, sfac, dbg_match, dbg_status);
+  if (bytes > 0 && !mbar_wait(mbar, 0u)) {
+    // copy not observed complete: record it, wait once more (bounded), then read
+    // the whole tree from global memory
+    g_kernel_error = 1;
+    mbar_wait(mbar, 0u);
+    nst = 0;
+  }
+  if (stamp) g_phase[1] = clock64();
+  tile_body<KIND>(Jn, L, sC, T, sN, nst, swp, sfac, dbg_match, dbg_status);
   __syncthreads();
+  if (stamp) g_phase[2] = clock64();
   double* P = partials + (size_t)tile * kPStride;
   for (int k = threadIdx.x; k < kPStride; k += blockDim.x) {
     if (k >= M && k < kPStats) continue;
@@ -649,6 +779,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_linearize(const JobIn* __restrict
     s_last = (prev == (unsigned)(Jn.tile_count - 1)) ? 1 : 0;
   }
   __syncthreads();
+  if (stamp) g_phase[3] = clock64();
   if (!s_last) return;
   __threadfence();
   job_tail(Jn, S, outs[T.job], logs ? logs + (size_t)T.job * kMaxLog : nullptr, lins, partials, swp, M);
@@ -843,6 +974,12 @@ int Runner::max_launches() const {
   return m;
 }
 
+int phase_stamps(int on, unsigned long long* out16) {
+  if (on >= 0) KDS_CK(cudaMemcpyToSymbol(g_phase_on, &on, sizeof(int)));
+  if (out16) KDS_CK(cudaMemcpyFromSymbol(out16, g_phase, sizeof(unsigned long long) * 16));
+  return KDS_OK;
+}
+
 int Runner::ensure_events(int n) {
   while ((int)prof_ev.size() < n) {
     cudaEvent_t e;
@@ -879,19 +1016,31 @@ int Runner::enqueue(cudaStream_t s, int32_t* dbg_match, int32_t* dbg_status) {
     if (rc) return rc;
   }
   int ev = 0;
+  const int stage = stage_nodes;
+  const size_t stage_bytes = (size_t)stage * sizeof(DNode);
+  if (stage_bytes > 48 * 1024 && !smem_attr_set) {
+    for (int k = 0; k < 3; ++k) {
+      const void* f = k == 0 ? (const void*)k_linearize<0> : (k == 1 ? (const void*)k_linearize<1> : (const void*)k_linearize<2>);
+      KDS_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    }
+    smem_attr_set = true;
+  }
   for (int i = 0; i < L; ++i) {
     for (int kind = 0; kind < 3; ++kind) {
       if (!kind_count[kind]) continue;
       if (profiling) KDS_CK(cudaEventRecordWithFlags(prof_ev[ev++], s, cudaEventRecordExternal));
       if (kind == 0)
-        k_linearize<0><<<kind_count[0], kBlock, 0, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
-                                                        kind_begin[0], d_partials, dbg_match, dbg_status);
+        k_linearize<0><<<kind_count[0], kBlock, stage_bytes, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins,
+                                                                     d_tiles, kind_begin[0], stage, d_partials,
+                                                                     dbg_match, dbg_status);
       else if (kind == 1)
-        k_linearize<1><<<kind_count[1], kBlock, 0, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
-                                                        kind_begin[1], d_partials, dbg_match, dbg_status);
+        k_linearize<1><<<kind_count[1], kBlock, stage_bytes, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins,
+                                                                     d_tiles, kind_begin[1], stage, d_partials,
+                                                                     dbg_match, dbg_status);
       else
-        k_linearize<2><<<kind_count[2], kBlock, 0, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
-                                                        kind_begin[2], d_partials, dbg_match, dbg_status);
+        k_linearize<2><<<kind_count[2], kBlock, stage_bytes, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins,
+                                                                     d_tiles, kind_begin[2], stage, d_partials,
+                                                                     dbg_match, dbg_status);
       ::kds::count_launch();
       if (profiling) KDS_CK(cudaEventRecordWithFlags(prof_ev[ev++], s, cudaEventRecordExternal));
     }
@@ -910,6 +1059,7 @@ int Runner::run(cudaStream_t s, bool use_graph, int32_t* dbg_match, int32_t* dbg
   key.push_back(max_launches());
   for (int k = 0; k < 3; ++k) { key.push_back(kind_begin[k]); key.push_back(kind_count[k]); }
   key.push_back(profiling ? 1 : 0);
+  key.push_back(stage_nodes);
   if (key != graph_key) {
     drop_graph();
     cudaStream_t cs;
@@ -941,6 +1091,14 @@ int Runner::fetch(cudaStream_t s, std::vector<JobOut>& outs, std::vector<kds_sta
     KDS_CK(cudaMemcpyAsync(logs->data(), d_logs, sizeof(kds_stats) * kMaxLog * num_jobs, cudaMemcpyDeviceToHost, s));
   }
   KDS_CK(cudaStreamSynchronize(s));
+  int err = 0;
+  KDS_CK(cudaMemcpyFromSymbol(&err, g_kernel_error, sizeof(int)));
+  if (err) {
+    int zero = 0;
+    KDS_CK(cudaMemcpyToSymbol(g_kernel_error, &zero, sizeof(int)));
+    set_error("a bounded wait for a tree-top copy gave up; results were computed from global memory");
+    return KDS_ERR_TIMEOUT;
+  }
   return KDS_OK;
 }
 

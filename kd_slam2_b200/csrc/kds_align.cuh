@@ -112,6 +112,9 @@ struct Runner {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   std::vector<int64_t> graph_key;
+  // number of top fixed-tree nodes each block stages in shared memory (32 B each)
+  int stage_nodes = 2047;
+  bool smem_attr_set = false;
   // optional event pair per linearization launch (measurement only)
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;
@@ -131,5 +134,7 @@ struct Runner {
 };
 
 int count_touched(Runner& R, int kind, int64_t fixed_nodes, int64_t* out, cudaStream_t s);
+// on: 1/0 enables/disables the phase stamps (-1 leaves it); out16 (nullable) receives them
+int phase_stamps(int on, unsigned long long* out16);
 
 }  // namespace kds

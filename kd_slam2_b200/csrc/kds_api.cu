@@ -572,7 +572,12 @@ int kds_aligner_linearize_debug(kds_aligner* a, const float caches[36], const fl
 int kds_aligner_set_profiling(kds_aligner* a, int32_t on) {
   CHECK_A(a);
   a->runner.profiling = on != 0;
-  return KDS_OK;
+  return phase_stamps(on != 0 ? 1 : 0, nullptr);
+}
+
+int kds_phase_stamps(uint64_t* out16) {
+  if (!out16) return KDS_ERR_INVALID_ARG;
+  return phase_stamps(-1, reinterpret_cast<unsigned long long*>(out16));
 }
 
 int kds_aligner_get_profile(const kds_aligner* a, double* mean_ms, int32_t* launches) {

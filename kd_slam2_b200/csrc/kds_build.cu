@@ -38,6 +38,7 @@ constexpr int kGridBlocks = 148 * 4;
 constexpr int kLevelBlocks = 64;
 constexpr int kLevelsPerSync = 4;
 constexpr int kMaxDepth = 64;
+constexpr int kUnroll = 4;  // loads in flight per lane in the warp-per-node kernel
 
 // ---------------------------------------------------------------------------
 // 128-bit two's complement fixed point (units of 2^-64)
@@ -210,12 +211,18 @@ __device__ void jacobi3(const double Ain[3][3], double ev[3], double V[3][3]) {
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) { a[i][j] = Ain[i][j]; V[i][j] = (i == j) ? 1.0 : 0.0; }
   for (int sweep = 0; sweep < 8; ++sweep) {
+    if (a[0][1] == 0.0 && a[0][2] == 0.0 && a[1][2] == 0.0) break;
     for (int pq = 0; pq < 3; ++pq) {
       int p = (pq == 2) ? 1 : 0;
       int q = (pq == 0) ? 1 : 2;
       int r = 3 - p - q;
       double apq = a[p][q];
-      if (apq == 0.0) continue;
+      // negligible off-diagonal: set to zero (same rule in the CPU oracle)
+      if (fabs(apq) <= 1e-18 * (fabs(a[p][p]) + fabs(a[q][q]))) {
+        a[p][q] = 0.0;
+        a[q][p] = 0.0;
+        continue;
+      }
       double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
       double t = 1.0 / (fabs(theta) + sqrt(theta * theta + 1.0));
       if (theta < 0.0) t = -t;
@@ -257,7 +264,7 @@ __device__ void jacobi3(const double Ain[3][3], double ev[3], double V[3][3]) {
 // FlatLeafPolicy_::fillMetadata over CountLeafPolicy_ and LabelPolicyBase_
 // (kd/tree/flat_leaf_policy_.h:52-108, count_leaf_policy_.h:27-43,
 // label_policy_base_impl_.h:12-97) on FP64 statistics.
-__device__ void decide(const Moments& M, int64_t n, BNode& nd, const BuildParams& P) {
+__device__ __noinline__ void decide(const Moments& M, int64_t n, BNode& nd, const BuildParams& P) {
   for (int i = 0; i < 3; ++i) { nd.mean[i] = 0.f; nd.dir[i] = 0.f; }
   nd.dts_mean = 0.0;
   nd.dts_cov = 0.0;
@@ -406,23 +413,35 @@ __global__ void k_ingest(const float* xyz, const double* st, int64_t n, float4* 
   }
 }
 
-// One block per tree: ts_start = min stamp (label_policy_base_impl_.h:28-35); dt range check.
-__global__ void k_tree_prep(const double* sts, const int64_t* off, int R, double* ts0, LevelState* ls) {
-  __shared__ double sm[kThreads];
-  int r = blockIdx.x;
-  if (r >= R) return;
-  int64_t b = off[r], e = off[r + 1];
-  double m = 1.0e308;
-  for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) m = fmin(m, sts[i]);
-  sm[threadIdx.x] = m;
-  __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) sm[threadIdx.x] = fmin(sm[threadIdx.x], sm[threadIdx.x + s]);
-    __syncthreads();
-  }
-  double t0 = (e > b) ? sm[0] : 0.0;
-  if (threadIdx.x == 0) ts0[r] = t0;
-  for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x)
+// Order-preserving map of finite doubles to unsigned 64-bit keys.
+__device__ __forceinline__ unsigned long long dkey(double d) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(d);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dkey_inv(unsigned long long k) {
+  unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
+// ts_start of each tree = min stamp (label_policy_base_impl_.h:28-35); blockIdx.y = tree.
+__global__ void k_tree_min(const double* sts, const int64_t* off, unsigned long long* tsmin) {
+  const int r = blockIdx.y;
+  const int64_t b = off[r], e = off[r + 1];
+  unsigned long long m = ~0ull;
+  for (int64_t i = b + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e; i += (int64_t)gridDim.x * blockDim.x)
+    m = min(m, dkey(sts[i]));
+  for (int off2 = 16; off2 > 0; off2 >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, off2));
+  if ((threadIdx.x & 31) == 0 && m != ~0ull) atomicMin(&tsmin[r], m);
+}
+
+// decodes ts_start and checks the dt range of every point; blockIdx.y = tree.
+__global__ void k_tree_check(const double* sts, const int64_t* off, const unsigned long long* tsmin, double* ts0,
+                             LevelState* ls) {
+  const int r = blockIdx.y;
+  const int64_t b = off[r], e = off[r + 1];
+  const double t0 = (e > b) ? dkey_inv(tsmin[r]) : 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) ts0[r] = t0;
+  for (int64_t i = b + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e; i += (int64_t)gridDim.x * blockDim.x)
     if (!(sts[i] - t0 < 65536.0)) ls->error = 2;
 }
 
@@ -456,7 +475,7 @@ struct PointBufs {
 };
 
 // Warp per small node: moments, decision, stable partition (or leaf placement).
-__global__ void __launch_bounds__(kThreads) k_small(BNode* nodes, const LevelState* ls, PointBufs B,
+__global__ void __launch_bounds__(kThreads, 2) k_small(BNode* nodes, const LevelState* ls, PointBufs B,
                                                     const double* ts0, BuildParams P) {
   const int lb = ls->lb, le = ls->le, cur = ls->cur;
   if (lb >= le) return;
@@ -468,7 +487,9 @@ __global__ void __launch_bounds__(kThreads) k_small(BNode* nodes, const LevelSta
   int32_t* iout = B.id[cur ^ 1];
   const int lane = threadIdx.x & 31;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int ni = lb + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); ni < le; ni += nwarps) {
+  // consecutive nodes go to different blocks (SMs) first
+  const int wslot = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
+  for (int ni = lb + wslot; ni < le; ni += nwarps) {
     BNode nd = nodes[ni];
     int s = nd.start, e = nd.end;
     int n = e - s;
@@ -476,36 +497,70 @@ __global__ void __launch_bounds__(kThreads) k_small(BNode* nodes, const LevelSta
     double t0 = ts0[nd.tree];
     Moments M;
     for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
-    for (int i = s + lane; i < e; i += 32) moments_add_point(M, pin[i], sin_[i], t0);
+    // lane l owns points s + 32*k + l, k < K (K <= 32); loads issued kUnroll at a time
+    const int K = (n + 31) >> 5;
+    for (int k0 = 0; k0 < K; k0 += kUnroll) {
+      float4 pv[kUnroll];
+      double sv[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        int i = s + ((k0 + u) << 5) + lane;
+        if (i < e) { pv[u] = pin[i]; sv[u] = sin_[i]; }
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        int i = s + ((k0 + u) << 5) + lane;
+        if (i < e) moments_add_point(M, pv[u], sv[u], t0);
+      }
+    }
     for (int off = 16; off > 0; off >>= 1)
       for (int k = 0; k < 11; ++k) M.s[k] = u128_add(M.s[k], shfl_xor_u128(M.s[k], off));
     decide(M, n, nd, P);
     if (nd.split) {
-      int nl = 0;
-      for (int base = s; base < e; base += 32) {
-        int i = base + lane;
-        bool left = false;
-        if (i < e) left = which_side_f(nd.mean, nd.dir, pin[i]);
-        nl += __popc(__ballot_sync(0xffffffffu, left));
-      }
-      int cl = 0, cr = 0;
-      unsigned lt = (1u << lane) - 1u;
-      for (int base = s; base < e; base += 32) {
-        int i = base + lane;
-        bool valid = i < e;
-        bool left = false;
-        float4 p;
-        if (valid) { p = pin[i]; left = which_side_f(nd.mean, nd.dir, p); }
-        unsigned bl = __ballot_sync(0xffffffffu, valid && left);
-        unsigned br = __ballot_sync(0xffffffffu, valid && !left);
-        if (valid) {
-          int dst = left ? (s + cl + __popc(bl & lt)) : (s + nl + cr + __popc(br & lt));
-          pout[dst] = p;
-          sout[dst] = sin_[i];
-          iout[dst] = iin[i];
+      // side of each owned point as a bit mask, then a stable move with independent loads
+      unsigned bits = 0u;
+      for (int k0 = 0; k0 < K; k0 += kUnroll) {
+        float4 pv[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          int i = s + ((k0 + u) << 5) + lane;
+          if (i < e) pv[u] = pin[i];
         }
-        cl += __popc(bl);
-        cr += __popc(br);
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          int i = s + ((k0 + u) << 5) + lane;
+          if (i < e && which_side_f(nd.mean, nd.dir, pv[u])) bits |= 1u << (k0 + u);
+        }
+      }
+      int nl = __popc(bits);
+      for (int off = 16; off > 0; off >>= 1) nl += __shfl_xor_sync(0xffffffffu, nl, off);
+      const unsigned lt = (1u << lane) - 1u;
+      int cl = 0, cr = 0;
+      for (int k0 = 0; k0 < K; k0 += kUnroll) {
+        float4 pv[kUnroll];
+        double sv[kUnroll];
+        int iv[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          int i = s + ((k0 + u) << 5) + lane;
+          if (i < e) { pv[u] = pin[i]; sv[u] = sin_[i]; iv[u] = iin[i]; }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          int i = s + ((k0 + u) << 5) + lane;
+          bool valid = i < e;
+          bool left = valid && ((bits >> (k0 + u)) & 1u);
+          unsigned bl = __ballot_sync(0xffffffffu, left);
+          unsigned br = __ballot_sync(0xffffffffu, valid && !left);
+          if (valid) {
+            int dst = left ? (s + cl + __popc(bl & lt)) : (s + nl + cr + __popc(br & lt));
+            pout[dst] = pv[u];
+            sout[dst] = sv[u];
+            iout[dst] = iv[u];
+          }
+          cl += __popc(bl);
+          cr += __popc(br);
+        }
       }
       nd.mid = s + nl;
     } else {
@@ -906,6 +961,7 @@ struct BuildWs {
   int32_t *chunk_nl, *chunk_loff, *big_list, *node_chunk0;
   U128* acc;
   double* ts0;
+  unsigned long long* tsmin;
   int64_t* off;
   LevelState* ls;
   int32_t* level_begin;
@@ -925,7 +981,7 @@ int ws_alloc(BuildWs& w, int64_t n, int R, cudaStream_t s) {
   size_t bytes = 2 * carve_size<float4>(n) + 2 * carve_size<double>(n) + 3 * carve_size<int32_t>(n) +
                  carve_size<BNode>(cn) + 4 * carve_size<int32_t>(cn) + carve_size<int32_t>(ntiles) +
                  carve_size<Chunk>(w.chunk_cap) + 4 * carve_size<int32_t>(w.chunk_cap) +
-                 carve_size<U128>((size_t)11 * (n / kBig + 2)) + carve_size<double>(R) +
+                 carve_size<U128>((size_t)11 * (n / kBig + 2)) + 2 * carve_size<double>(R) +
                  carve_size<int64_t>(R + 1) + carve_size<LevelState>(1) + carve_size<int32_t>(kMaxDepth + 2) +
                  carve_size<int32_t>(kLevelBlocks) + 7 * carve_size<int32_t>(G) + 3 * carve_size<int32_t>(R) +
                  carve_size<int32_t>(8) + carve_size<TreeDev>(R) + 256;
@@ -957,6 +1013,7 @@ int ws_alloc(BuildWs& w, int64_t n, int R, cudaStream_t s) {
   w.node_chunk0 = carve<int32_t>(p, w.chunk_cap);
   w.acc = carve<U128>(p, (size_t)11 * (n / kBig + 2));
   w.ts0 = carve<double>(p, R);
+  w.tsmin = carve<unsigned long long>(p, R);
   w.off = carve<int64_t>(p, R + 1);
   w.ls = carve<LevelState>(p, 1);
   w.level_begin = carve<int32_t>(p, kMaxDepth + 2);
@@ -1035,8 +1092,14 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   KDS_CK(cudaMemcpyAsync(w.off, off.data(), sizeof(int64_t) * (R + 1), cudaMemcpyHostToDevice, s));
   k_ingest<<<nblk(N, kThreads), kThreads, 0, s>>>(d_xyz, d_st, N, w.B.p[0], w.B.s[0], w.B.id[0], w.ls);
   count_launch();
-  k_tree_prep<<<R, kThreads, 0, s>>>(w.B.s[0], w.off, R, w.ts0, w.ls);
-  count_launch();
+  {
+    KDS_CK(cudaMemsetAsync(w.tsmin, 0xff, sizeof(unsigned long long) * R, s));
+    dim3 g((unsigned)std::min<int64_t>(std::max<int64_t>((max_size + kThreads - 1) / kThreads, 1), 64), (unsigned)R);
+    k_tree_min<<<g, kThreads, 0, s>>>(w.B.s[0], w.off, w.tsmin);
+    k_tree_check<<<g, kThreads, 0, s>>>(w.B.s[0], w.off, w.tsmin, w.ts0, w.ls);
+    count_launch();
+    count_launch();
+  }
   k_init_roots<<<(R + 127) / 128, 128, 0, s>>>(w.nodes, w.off, R, w.ls, w.level_begin);
   count_launch();
   KDS_CK(cudaGetLastError());

@@ -16,7 +16,9 @@
 //    reference sums in float with StableAdder_, kd/utils/stable_adder_.h:21-74).
 //  * Mean, covariance and eigen decomposition are FP64; the eigensolver is cyclic
 //    Jacobi (Golub & Van Loan, sec. 8.5) with a fixed sweep count, which uses only
-//    IEEE-exact + - * / sqrt.  The reference uses Eigen's computeDirect in float.
+//    IEEE-exact + - * / sqrt; a rotation is skipped (off-diagonal set to zero) when
+//    |a_pq| <= 1e-18 (|a_pp| + |a_qq|), and the sweeps stop once all off-diagonals are
+//    zero.  The reference uses Eigen's computeDirect in float.
 //  * Partitions are stable (left points keep their order, then right points); the
 //    reference swaps with the range end (kd/tree/node_impl_.h:12-26).  Leaf membership
 //    does not depend on this order because the sums are order independent.
@@ -79,12 +81,18 @@ void jacobi3(const double Ain[3][3], double ev[3], double V[3][3]) {
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) { a[i][j] = Ain[i][j]; V[i][j] = (i == j) ? 1.0 : 0.0; }
   for (int sweep = 0; sweep < 8; ++sweep) {
+    if (a[0][1] == 0.0 && a[0][2] == 0.0 && a[1][2] == 0.0) break;
     for (int pq = 0; pq < 3; ++pq) {
       int p = (pq == 2) ? 1 : 0;
       int q = (pq == 0) ? 1 : 2;
       int r = 3 - p - q;
       double apq = a[p][q];
-      if (apq == 0.0) continue;
+      // negligible off-diagonal: set to zero and skip the rotation
+      if (std::fabs(apq) <= 1e-18 * (std::fabs(a[p][p]) + std::fabs(a[q][q]))) {
+        a[p][q] = 0.0;
+        a[q][p] = 0.0;
+        continue;
+      }
       double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
       double t = 1.0 / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
       if (theta < 0.0) t = -t;

@@ -263,6 +263,28 @@ int kds_batch_create(kds_batch** out);
 int kds_batch_run(kds_batch* b, kds_job* jobs, int32_t num_jobs, int32_t use_graph, void* stream);
 void kds_batch_free(kds_batch* b);
 
+/* One linearization that allocates no memory.  This entry point has no counterpart in
+ * the reference; it serves callers that cannot allocate device memory while they run
+ * (real-time loops that reserve all memory at start-up, code that must not call
+ * cudaMalloc/cudaFree because those can block on the device or on allocator locks).
+ *
+ * It computes what kds_aligner_build_quadratic_form computes for a single fixed tree
+ * (D = 6 for KDS_ICP, 12 for KDS_CTICP): H (row-major D*D), b (D) and stats at pose X,
+ * velocities v (CT only, NULL = zero), fixed pose fixed_X and fixed velocities fixed_v
+ * (NULL = zero).  Its scratch (about 0.8 MB) is one static device array of the library,
+ * held by every GPU that loads the library until the process exits; the trees and the
+ * outputs are the caller's.  At most 65,536 moving leaves per call: larger moving trees
+ * return KDS_ERR_CAPACITY.
+ *
+ * The first call on each device resolves the array's address and sets kernel
+ * attributes; make that first call before any stream capture.  All calls share the
+ * array, so calls that overlap on the GPU (other streams, other threads) race on it.
+ * The call blocks until its results have reached the host.  H, b, stats may be NULL. */
+int kds_linearize_static(const kds_tree* fixed, const kds_tree* moving, int32_t type,
+                         const kds_aligner_params* params, const double X[12], const double fixed_X[12],
+                         const double v[6], const double fixed_v[6], int32_t stats_mode, void* stream, double* H,
+                         double* b, kds_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -171,6 +171,8 @@ SIGNATURES = {
     "kds_batch_create": (C.c_int, [C.POINTER(_P)]),
     "kds_batch_run": (C.c_int, [_P, C.POINTER(Job), _I32, _I32, _P]),
     "kds_batch_free": (None, [_P]),
+    "kds_linearize_static": (C.c_int, [_P, _P, _I32, C.POINTER(AlignerParams), _P, _P, _P, _P, _I32, _P, _P, _P,
+                                       C.POINTER(Stats)]),
 }
 
 

@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "kds_align.cuh"
@@ -1099,6 +1100,156 @@ int Runner::fetch(cudaStream_t s, std::vector<JobOut>& outs, std::vector<kds_sta
     set_error("a bounded wait for a tree-top copy gave up; results were computed from global memory");
     return KDS_ERR_TIMEOUT;
   }
+  return KDS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// One linearization (buildQuadraticForm) that allocates nothing.
+//
+// Some callers cannot allocate device memory when they linearize: a real-time
+// odometry or bundle-adjustment loop that reserves all of its memory at start-up and
+// must not call cudaMalloc/cudaFree afterwards (they can block on the device and on
+// allocator locks), or code that must not touch the allocator while it enqueues work.
+// For them the scratch of k_linearize -- the job, state and output records, the
+// fixed-entry record, the tile list and one FP64 partial per tile -- lives in one
+// file-scope device array.  Every call on a device shares that array: calls that
+// overlap on the GPU (other streams, other host threads) race on it, and it keeps the
+// last call's contents.  The tile list is rebuilt and the job state reset by every
+// call; each tile writes its own partial before the last tile reads them.
+namespace {
+
+constexpr int kStaticMaxTiles = 512;  // 512 tiles x 128 = 65,536 moving surfels per call
+constexpr int kStaticStage = 2047;    // fixed-tree nodes staged per block (64 KB)
+
+struct StaticScratch {
+  JobIn job;
+  JobState state;
+  JobOut out;
+  LinDev lin;
+  TileDev tiles[kStaticMaxTiles];
+  double partials[(size_t)kStaticMaxTiles * kPStride];
+};
+
+__device__ __align__(256) unsigned char g_static_scratch[sizeof(StaticScratch)];
+
+std::mutex g_static_mu;
+StaticScratch* g_static_ptr[64] = {nullptr};
+
+// Writes the job and fixed-entry records and the tile list into the scratch.
+__global__ void k_static_setup(StaticScratch* scr, JobIn job, LinDev lin, int ntiles) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    scr->job = job;
+    scr->lin = lin;
+  }
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+    TileDev d;
+    d.job = 0;
+    d.lin = 0;
+    d.leaf_begin = t * kBlock;
+    d.leaf_end = min((t + 1) * kBlock, job.m_num_leaves);
+    scr->tiles[t] = d;
+  }
+}
+
+// First call on a device, with that device current: resolves the array's device
+// address and raises the kernels' dynamic shared-memory limit.
+int static_setup(StaticScratch** out) {
+  int dev = 0;
+  KDS_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) { set_error("device ordinal %d out of range", dev); return KDS_ERR_INVALID_ARG; }
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || p == nullptr) return cuda_status(e, "cudaGetSymbolAddress(g_static_scratch)", __FILE__, __LINE__);
+    const int bytes = kStaticStage * (int)sizeof(DNode);
+    KDS_CK(cudaFuncSetAttribute((const void*)k_linearize<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    KDS_CK(cudaFuncSetAttribute((const void*)k_linearize<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    g_static_ptr[dev] = reinterpret_cast<StaticScratch*>(p);
+  }
+  *out = g_static_ptr[dev];
+  return KDS_OK;
+}
+
+}  // namespace
+
+int linearize_static(const TreeDev& fixed, const TreeDev& moving, int32_t type, const kds_aligner_params& P,
+                     const double* X, const double* Xf, const double* v, const double* fv, int32_t stats_mode,
+                     cudaStream_t s, double* H, double* b, kds_stats* stats) {
+  const int64_t nl = moving.num_leaves;
+  const int64_t ntiles = (nl + kBlock - 1) / kBlock;
+  if (ntiles > kStaticMaxTiles) {
+    set_error("kds_linearize_static: %lld moving leaves exceed the static maximum of %d", (long long)nl,
+              kStaticMaxTiles * kBlock);
+    return KDS_ERR_CAPACITY;
+  }
+  StaticScratch* scr = nullptr;
+  int rc = static_setup(&scr);
+  if (rc) return rc;
+  JobIn J;
+  memset(&J, 0, sizeof(J));
+  J.m_md = moving.leaf_md;
+  J.m_nrm = moving.leaf_nrm;
+  J.m_num_leaves = (int32_t)nl;
+  J.kind = type == KDS_ICP ? 0 : 1;
+  J.mode = KDS_JOB_LINEARIZE;
+  J.stats_mode = stats_mode;
+  J.lin_begin = 0;
+  J.lin_count = 1;
+  J.tile_begin = 0;
+  J.tile_count = (int32_t)ntiles;
+  J.P.kernel_threshold = P.kernel_threshold;
+  J.P.damping = P.damping;
+  J.P.max_error = P.max_error;
+  J.P.min_normal_cos = P.min_normal_cos;
+  J.P.min_good_measurements = P.min_good_measurements;
+  J.P.max_iterations = P.max_iterations;
+  J.P.velocity_damping = P.velocity_damping;
+  J.P.term_crit = P.term_crit;
+  J.P.d_pert = P.d_pert;
+  J.P.d_score = P.d_score;
+  for (int i = 0; i < 12; ++i) J.X0[i] = X[i];
+  for (int i = 0; i < 6; ++i) J.v0[i] = (type == KDS_ICP || !v) ? 0.0 : v[i];
+  LinDev L;
+  memset(&L, 0, sizeof(L));
+  L.fnodes = fixed.nodes;
+  L.fdts = fixed.dts_f;
+  L.f_num_nodes = (int32_t)fixed.num_nodes;
+  L.job = 0;
+  for (int i = 0; i < 12; ++i) L.Xf[i] = Xf[i];
+  for (int i = 0; i < 6; ++i) L.fv[i] = fv ? fv[i] : 0.0;
+  k_static_setup<<<1, 256, 0, s>>>(scr, J, L, (int)ntiles);
+  count_launch();
+  k_init_jobs<<<1, 128, 0, s>>>(&scr->job, &scr->state, &scr->out, &scr->lin, 1);
+  count_launch();
+  if (ntiles > 0) {
+    const size_t stage_bytes = (size_t)kStaticStage * sizeof(DNode);
+    if (J.kind == 0)
+      k_linearize<0><<<(unsigned)ntiles, kBlock, stage_bytes, s>>>(&scr->job, &scr->state, &scr->out, nullptr,
+                                                                  &scr->lin, scr->tiles, 0, kStaticStage,
+                                                                  scr->partials, nullptr, nullptr);
+    else
+      k_linearize<1><<<(unsigned)ntiles, kBlock, stage_bytes, s>>>(&scr->job, &scr->state, &scr->out, nullptr,
+                                                                  &scr->lin, scr->tiles, 0, kStaticStage,
+                                                                  scr->partials, nullptr, nullptr);
+    count_launch();
+  }
+  KDS_CK(cudaGetLastError());
+  JobOut O;
+  KDS_CK(cudaMemcpyAsync(&O, &scr->out, sizeof(JobOut), cudaMemcpyDeviceToHost, s));
+  KDS_CK(cudaStreamSynchronize(s));
+  int err = 0;
+  KDS_CK(cudaMemcpyFromSymbol(&err, g_kernel_error, sizeof(int)));
+  if (err) {
+    int zero = 0;
+    KDS_CK(cudaMemcpyToSymbol(g_kernel_error, &zero, sizeof(int)));
+    set_error("a bounded wait for a tree-top copy gave up; results were computed from global memory");
+    return KDS_ERR_TIMEOUT;
+  }
+  const int D = type == KDS_ICP ? 6 : 12;
+  if (H) memcpy(H, O.H, sizeof(double) * D * D);
+  if (b) memcpy(b, O.b, sizeof(double) * D);
+  if (stats) *stats = O.stats;
   return KDS_OK;
 }
 

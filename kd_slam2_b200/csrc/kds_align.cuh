@@ -137,4 +137,10 @@ int count_touched(Runner& R, int kind, int64_t fixed_nodes, int64_t* out, cudaSt
 // on: 1/0 enables/disables the phase stamps (-1 leaves it); out16 (nullable) receives them
 int phase_stamps(int on, unsigned long long* out16);
 
+// One linearization whose scratch is a file-scope device array (no allocation).
+// Rejects more than 65,536 moving leaves with KDS_ERR_CAPACITY.
+int linearize_static(const TreeDev& fixed, const TreeDev& moving, int32_t type, const kds_aligner_params& P,
+                     const double* X, const double* Xf, const double* v, const double* fv, int32_t stats_mode,
+                     cudaStream_t s, double* H, double* b, kds_stats* stats);
+
 }  // namespace kds

@@ -580,6 +580,19 @@ int kds_phase_stamps(uint64_t* out16) {
   return phase_stamps(-1, reinterpret_cast<unsigned long long*>(out16));
 }
 
+int kds_linearize_static(const kds_tree* fixed, const kds_tree* moving, int32_t type,
+                         const kds_aligner_params* params, const double X[12], const double fixed_X[12],
+                         const double v[6], const double fixed_v[6], int32_t stats_mode, void* stream, double* H,
+                         double* b, kds_stats* stats) {
+  KDS_INIT();
+  if (!fixed || !moving || !params || !X || !fixed_X || (type != KDS_ICP && type != KDS_CTICP)) {
+    set_error("kds_linearize_static: fixed, moving, params, X and fixed_X are required; type is KDS_ICP or KDS_CTICP");
+    return KDS_ERR_INVALID_ARG;
+  }
+  return linearize_static(fixed->d, moving->d, type, *params, X, fixed_X, v, fixed_v, stats_mode, as_stream(stream),
+                          H, b, stats);
+}
+
 int kds_aligner_get_profile(const kds_aligner* a, double* mean_ms, int32_t* launches) {
   CHECK_A(a);
   int n = 0;

@@ -1,0 +1,103 @@
+// Test driver for include/kds.hpp.
+//   adapter_main conf <file.conf>
+//       prints the parameters that the conf blocks configure (no device needed)
+//   adapter_main align <file.conf> <fixed.bin> <moving.bin> <x0.bin> <v0.bin> <out.bin>
+//       builds both trees with the conf's TreeGeneratorB2003D, runs the conf's
+//       CTICPB2003D and writes [result, X(12), v(6)] as doubles
+// A cloud file is int64 n, then n*3 float32 xyz, then n float64 stamps.
+#include <cstdio>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "kds.hpp"
+
+using namespace kds_b200;
+
+static void read_cloud(const std::string& path, std::vector<float>& xyz, std::vector<double>& st) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) throw std::runtime_error("cannot open " + path);
+  int64_t n = 0;
+  f.read(reinterpret_cast<char*>(&n), sizeof(n));
+  xyz.resize((size_t)n * 3);
+  st.resize((size_t)n);
+  f.read(reinterpret_cast<char*>(xyz.data()), (std::streamsize)(xyz.size() * sizeof(float)));
+  f.read(reinterpret_cast<char*>(st.data()), (std::streamsize)(st.size() * sizeof(double)));
+  if (!f) throw std::runtime_error("short read " + path);
+}
+
+template <size_t N>
+static std::array<double, N> read_vec(const std::string& path) {
+  std::array<double, N> v;
+  std::ifstream f(path, std::ios::binary);
+  f.read(reinterpret_cast<char*>(v.data()), sizeof(double) * N);
+  if (!f) throw std::runtime_error("short read " + path);
+  return v;
+}
+
+static const ConfObject* find_type(const std::vector<ConfObject>& objs, const char* type) {
+  for (auto& o : objs)
+    if (o.type == type) return &o;
+  throw std::runtime_error(std::string("no block of type ") + type);
+}
+
+static int conf_mode(const std::string& path) {
+  auto objs = ConfReader::load(path);
+  TreeGeneratorB2003D gen;
+  ConfReader::configure(gen, *find_type(objs, "TreeGeneratorB2003D"));
+  const kds_tree_params& t = gen.params();
+  std::printf("tree %d %d %d %d %.9g %.9g %.9g %.9g\n", t.propagate_normal, t.tree_min_good_leaves, t.leaf_min_points,
+              t.leaf_max_points, t.leaf_density, t.leaf_min_normal_incidence, t.leaf_eigenvalue_threshold,
+              t.leaf_normal_eigenratio);
+  const char* types[2] = {"CTICPB2003D", "ICPB2003D"};
+  for (const char* ty : types) {
+    const int32_t type = std::string(ty) == "CTICPB2003D" ? KDS_CTICP : KDS_ICP;
+    kds_aligner_params p = ConfReader::aligner_params(type, *find_type(objs, ty), objs);
+    std::printf("%s %.9g %.9g %.9g %.9g %d %d %.9g %d %.9g %.9g\n", ty, p.kernel_threshold, p.damping, p.max_error,
+                p.min_normal_cos, p.min_good_measurements, p.max_iterations, p.velocity_damping, p.term_crit, p.d_pert,
+                p.d_score);
+  }
+  return 0;
+}
+
+static int align_mode(char** argv) {
+  auto objs = ConfReader::load(argv[2]);
+  TreeGeneratorB2003D gen;
+  ConfReader::configure(gen, *find_type(objs, "TreeGeneratorB2003D"));
+  std::vector<float> xf, xm;
+  std::vector<double> sf, sm;
+  read_cloud(argv[3], xf, sf);
+  read_cloud(argv[4], xm, sm);
+  TreePtr fixed = gen.makeTree(xf.data(), sf.data(), (int64_t)sf.size());
+  TreePtr moving = gen.makeTree(xm.data(), sm.data(), (int64_t)sm.size());
+  if (!fixed || !moving) throw std::runtime_error("tree rejected");
+  CTICPB2003D a;
+  ConfReader::configure(a, *find_type(objs, "CTICPB2003D"), objs);
+  a.setFixed(*fixed);
+  a.setMoving(*moving);
+  a.setX(read_vec<12>(argv[5]));
+  a.setVelocities(read_vec<6>(argv[6]));
+  int r = a.compute();
+  Pose X = a.getX();
+  Vector6 v = a.velocities();
+  std::vector<double> out;
+  out.push_back((double)r);
+  out.insert(out.end(), X.begin(), X.end());
+  out.insert(out.end(), v.begin(), v.end());
+  std::ofstream f(argv[7], std::ios::binary);
+  f.write(reinterpret_cast<const char*>(out.data()), (std::streamsize)(out.size() * sizeof(double)));
+  std::printf("result %d inliers %d\n", r, a.stats().num_inliers);
+  return 0;
+}
+
+int main(int argc, char** argv) {
+  try {
+    if (argc >= 3 && std::string(argv[1]) == "conf") return conf_mode(argv[2]);
+    if (argc >= 8 && std::string(argv[1]) == "align") return align_mode(argv);
+    std::fprintf(stderr, "usage: adapter_main conf <file> | align <conf> <fixed> <moving> <x0> <v0> <out>\n");
+    return 2;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "error: %s\n", e.what());
+    return 1;
+  }
+}

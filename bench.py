@@ -1,22 +1,27 @@
 #!/usr/bin/env python3
-"""Benchmark: CT-ICP with deskew of a 64x1024 spinning-LiDAR scan against a resident
-1M-surfel local-map KD-tree, 15 Gauss-Newton iterations, on one B200.
+"""Benchmark: served scan-to-map registration vs the plain GPU drop-in on one B200.
 
-One step = one alignment request: GPU surfel KD-tree build of the 65,536-ray scan
-(per-point stamps over a 0.1 s sweep, sensor at 10 m/s and 30 deg/s yaw) followed by
-CTICPB2003D::compute against the map tree built beforehand from 20 prior deskewed
-scans.  Metric: alignments/s (and per-request latency percentiles).
+Workload (seeded, synthetic): 16 sensor streams in one box scene, beam mix
+16/32/64/128 (16,384-262,144 rays per scan), 20 scans per stream = 320 requests,
+70% CT-ICP with per-point stamps (15 iterations) / 30% rigid ICP (10 iterations).
+Each stream's local map starts as 5 static prior scans and is rebuilt on the device
+from the stream's last 5 registered scans (deskewed with the estimated velocities).
 
-  value   inputs resident in HBM when each step starts (kds_tree_build on device
-          pointers); L2 flushed by a 512 MB write between steps (outside the timing)
-  e2e     the same request through the C ABI with host buffers: scan points and
-          stamps copied host->device inside the timed step, pose/velocity/stats read
-          back to the host
-  --impl reference   the reference's CPU path (oracle/ restatement, MODE_REF32:
-          TreeGenerator build + CTICP_CPU_ with std::async chunks) on the host cores.
+One step = serving the whole trace with every request arriving at t = 0 (the
+saturated trace): moving-tree builds, registrations and map rebuilds, start to
+drain.  Metric: alignments/s; beside it p50/p99 request latency under Poisson
+arrivals at 10 Hz per stream, and the same trace through the plain drop-in (one
+request at a time through kds_tree_build + kds_aligner_compute).
 
-Multi-GPU (torchrun): each rank runs an independent replica of the workload (the path
-has no data-path exchange); value = all ranks' alignments / max-over-ranks time.
+  value   request points resident in HBM when a step starts
+  e2e     request points in page-locked host memory, copied inside the step; results
+          read back to the host by the server every tick
+  --impl reference   the reference's CPU path (oracle/ restatement, MODE_REF32: tree
+          build + ICP_CPU_/CTICP_CPU_ with std::async chunks) on the host cores, on a
+          bounded sample of the same requests (against the streams' initial maps).
+
+Multi-GPU (torchrun): each rank serves an independent replica of the trace (the path
+has no data-path exchange); value = all ranks' requests / max-over-ranks time.
 """
 from __future__ import annotations
 
@@ -36,46 +41,26 @@ sys.path.insert(0, ROOT)
 METRIC = "ICP alignments/s + p50/p99 latency: served vs plain GPU at pose err ≤1e-5"
 UNIT = "alignments/s"
 
-SCENE_SEED = 1001
-MAP_SCANS = 20
-MAP_BEAMS = 128
-MAP_COLS = 8192
-SCAN_BEAMS = 64
-SCAN_COLS = 1024
-ELEV = (-22.5, 22.5)
-VEL = np.array([10.0, 0.0, 0.0, 0.0, 0.0, np.deg2rad(30.0)])
-TREE_PARAMS = dict(leaf_max_points=16)
-ALIGN_PARAMS = dict(max_iterations=15, max_error=0.5, velocity_damping=10.0)
-
-
-def make_workload():
-    from kd_slam2_b200 import synth
-    boxes = synth.scene(SCENE_SEED)
-    map_pts = []
-    for k in range(MAP_SCANS):
-        P = synth.pose((-20.0 + k, 0.0, 1.8))
-        xyz, _ = synth.scan(boxes, P, beams=MAP_BEAMS, cols=MAP_COLS, elev=ELEV, seed=3000 + k, threads=16)
-        map_pts.append(synth.transform(xyz, P))
-    map_xyz = np.concatenate(map_pts).astype(np.float32)
-    X_true = synth.pose((0.0, 0.0, 1.8))
-    xyz, st = synth.scan(boxes, X_true, vel=VEL, beams=SCAN_BEAMS, cols=SCAN_COLS, elev=ELEV, seed=2000,
-                         threads=16)
-    rng = np.random.default_rng(3000)
-    d = rng.normal(size=3); d /= np.linalg.norm(d)
-    a = rng.normal(size=3); a /= np.linalg.norm(a)
-    X0 = synth.pose(X_true[:, 3] + 0.1 * d, np.deg2rad(1.0) * a)
-    v0 = VEL + rng.normal(size=6) * np.array([0.5, 0.5, 0.1, 0.01, 0.01, 0.05])
-    return dict(map_xyz=map_xyz, xyz=xyz, st=st, X_true=X_true, X0=X0, v0=v0)
+TRACE_SEED = 5
+STREAMS = 16
+SCANS = 20
+RATE_HZ = 10.0
+TREE = dict(leaf_max_points=16)
+ICP = dict(max_error=0.5, max_iterations=10)
+CT = dict(max_error=0.5, max_iterations=15, velocity_damping=10.0)
+MAP_EVERY = 5
 
 
 def pose_err(A, B):
+    A = np.asarray(A).reshape(3, 4)
+    B = np.asarray(B).reshape(3, 4)
     dR = A[:, :3].T @ B[:, :3]
     c = np.clip((np.trace(dR) - 1) / 2, -1, 1)
     return float(np.linalg.norm(A[:, 3] - B[:, 3])), float(np.arccos(c))
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms while running."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -93,6 +78,7 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            time.sleep(0.3)  # let the first sample land before the timed region
         except Exception:
             self.proc = None
         return self
@@ -130,82 +116,123 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_reference_run(wl, map_export, steps: int, max_seconds: float, threads: int):
-    """The reference CPU path (oracle MODE_REF32) on the same request: tree build + CT-ICP."""
+def make_traces():
+    """(saturated trace, Poisson trace): the same scans, guesses and request types."""
+    from kd_slam2_b200 import streams
+    poi = streams.make_trace(TRACE_SEED, num_streams=STREAMS, scans_per_stream=SCANS, rate_hz=RATE_HZ, threads=16)
+    return streams.saturated(poi), poi
+
+
+def config_block(tr):
+    n = [len(r.xyz) for r in tr.requests]
+    return {
+        "workload": "served registration: %d streams (beams 16/32/64/128, 16k-262k rays), %d scans each "
+                    "(%d requests, %d%% CT-ICP / %d%% rigid ICP), per-stream local maps rebuilt every %d scans; "
+                    "saturated arrivals" % (STREAMS, SCANS, len(tr.requests),
+                                            round(100 * np.mean([r.kind for r in tr.requests])),
+                                            round(100 * (1 - np.mean([r.kind for r in tr.requests]))), MAP_EVERY),
+        "requests": len(tr.requests), "points_total": int(np.sum(n)), "points_min": int(np.min(n)),
+        "points_max": int(np.max(n)), "initial_map_points": [int(len(s.map_xyz)) for s in tr.streams],
+        "tree": TREE, "icp": ICP, "ct": CT, "map_every": MAP_EVERY, "trace_seed": TRACE_SEED,
+        "l2": "inputs larger than L2: %.0f MB of request points per step plus 16 resident maps" % (
+            20 * np.sum(n) / 1e6),
+    }
+
+
+def cpu_sample(tr, max_seconds: float, threads: int):
+    """The reference CPU path (oracle MODE_REF32) on the requests of the first map window
+    (against each stream's initial map): tree build + ICP/CT-ICP per request."""
     from oracle import orc
-    M = orc.OTree.from_nodes(map_export["mean"], map_export["dir"], map_export["dts_mean"], map_export["left"],
-                             map_export["right"])
-    tp = orc.tree_params(**TREE_PARAMS)
-    ap = orc.align_params(**ALIGN_PARAMS)
-    times = []
+    tp = orc.tree_params(**TREE)
+    maps = {}
+    times, n_done = [], 0
     t_start = time.perf_counter()
-    last = None
-    for i in range(steps):
+    for r in tr.requests:
+        if r.seq >= MAP_EVERY:
+            continue
+        if r.stream not in maps:
+            m = tr.streams[r.stream].map_xyz
+            maps[r.stream] = orc.OTree.build(m, np.zeros(len(m)), tp)
         t0 = time.perf_counter()
-        T = orc.OTree.build(wl["xyz"], wl["st"], tp)
-        last = orc.align(orc.KIND_CT, orc.MODE_REF32, M, T, ap, wl["X0"], v0=wl["v0"], num_threads=threads)
+        T = orc.OTree.build(r.xyz, r.stamps, tp)
+        if r.kind == 1:
+            orc.align(orc.KIND_CT, orc.MODE_REF32, maps[r.stream], T, orc.align_params(**CT), r.X0, v0=r.v0,
+                      num_threads=threads)
+        else:
+            orc.align(orc.KIND_ICP, orc.MODE_REF32, maps[r.stream], T, orc.align_params(**ICP), r.X0,
+                      num_threads=threads)
         times.append(time.perf_counter() - t0)
-        if time.perf_counter() - t_start > max_seconds and i >= 2:
+        n_done += 1
+        if time.perf_counter() - t_start > max_seconds:
             break
-    return times, last, M
+    return times
 
 
-def fp64_reference(wl, M):
+def accuracy_sample(tr, results, count: int = 6):
+    """Pose error of served results against the oracle (FP64 and the product's mixed
+    semantics) for requests against the initial maps."""
     from oracle import orc
-    T = orc.OTree.build(wl["xyz"], wl["st"], orc.tree_params(**TREE_PARAMS))
-    return orc.align(orc.KIND_CT, orc.MODE_FP64, M, T, orc.align_params(**ALIGN_PARAMS), wl["X0"], v0=wl["v0"])
+    tp = orc.tree_params(**TREE)
+    out = {"t_vs_fp64_m": [], "r_vs_fp64_rad": [], "t_vs_mixed_m": [], "r_vs_mixed_rad": []}
+    maps = {}
+    for r, q in zip(tr.requests, results):
+        if r.seq != 0 or len(out["t_vs_fp64_m"]) >= count or len(r.xyz) > 70000:
+            continue
+        if r.stream not in maps:
+            m = tr.streams[r.stream].map_xyz
+            maps[r.stream] = orc.OTree.build(m, np.zeros(len(m)), tp)
+        T = orc.OTree.build(r.xyz, r.stamps, tp)
+        kind = orc.KIND_CT if r.kind == 1 else orc.KIND_ICP
+        P = orc.align_params(**(CT if r.kind == 1 else ICP))
+        v0 = r.v0 if r.kind == 1 else None
+        r64 = orc.align(kind, orc.MODE_FP64, maps[r.stream], T, P, r.X0, v0=v0)
+        rmx = orc.align(kind, orc.MODE_MIXED, maps[r.stream], T, P, r.X0, v0=v0)
+        a, b = pose_err(q["X"], r64["X"])
+        c, d = pose_err(q["X"], rmx["X"])
+        out["t_vs_fp64_m"].append(a)
+        out["r_vs_fp64_rad"].append(b)
+        out["t_vs_mixed_m"].append(c)
+        out["r_vs_mixed_rad"].append(d)
+    return {k: float(np.max(v)) if v else None for k, v in out.items()} | {"requests": len(out["t_vs_fp64_m"])}
 
 
 def run_reference_arm(args):
-    import kd_slam2_b200 as kds
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    wl = make_workload()
-    # the map tree: the reference aligns against a tree loaded from a tree bag; here it is
-    # built once on the GPU and handed to the CPU path as a node array
-    gen = kds.TreeGeneratorB2003D(**TREE_PARAMS)
-    Mg = gen.make_tree(wl["map_xyz"])
-    me = Mg.export()
+    from kd_slam2_b200 import streams
+    tr, _ = make_traces()
     threads = min(os.cpu_count() or 1, 8)
-    n_steps = max(1, args.steps)
-    cpu_reference_run(wl, me, max(1, args.warmup), 1e9, threads)
-    times, last, _ = cpu_reference_run(wl, me, n_steps, 120.0, threads)
-    ms = 1e3 * float(np.mean(times))
-    val = 1e3 / ms
+    cpu_sample(tr, 2.0 * max(1, args.warmup) / 3.0, threads)  # warm-up
+    step_times = []
+    n_total = 0
+    for _ in range(max(1, args.steps)):
+        ts = cpu_sample(tr, 20.0, threads)
+        step_times.append(float(np.sum(ts)))
+        n_total += len(ts)
+    val = n_total / float(np.sum(step_times))
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": len(times), "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": config_block(wl, Mg),
+        "steps": len(step_times), "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(step_times)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_block(tr),
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{len(times)} full requests (oracle TreeGenerator build single-threaded + "
-                                   f"CTICP_CPU_ 15 iterations, {threads} std::async chunks)"},
+                         "sample": "each step: up to 20 s of the trace's first-window requests in order "
+                                   f"(oracle tree build + ICP_CPU_/CTICP_CPU_ MODE_REF32, {threads} chunks) "
+                                   "against the streams' initial maps"},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "latency_ms": {"p50": 1e3 * float(np.percentile(times, 50)), "p99": 1e3 * float(np.percentile(times, 99))},
     }
     print(json.dumps(line), flush=True)
-
-
-def config_block(wl, Mg, scan_leaves=None):
-    return {
-        "workload": "CT-ICP with deskew: 64x1024 scan (65,536 rays, %d returns) vs 1M-surfel local map "
-                    "(%d good leaves from %d prior deskewed scans), 15 iterations" % (
-                        len(wl["xyz"]), Mg.num_leaves, MAP_SCANS),
-        "scan_points": int(len(wl["xyz"])), "scan_leaves": scan_leaves, "map_points": int(len(wl["map_xyz"])),
-        "map_leaves": int(Mg.num_leaves), "map_nodes": int(Mg.num_nodes), "iterations": 15,
-        "tree": TREE_PARAMS, "aligner": ALIGN_PARAMS, "l2": "flushed (512 MB write) between timed steps",
-        "scene_seed": SCENE_SEED,
-    }
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kds", choices=["kds", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain drop-in comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -230,60 +257,13 @@ def main():
         return
 
     import kd_slam2_b200 as kds
+    from kd_slam2_b200 import streams
     kds.init(local)
-    stream = torch.cuda.Stream()
-    sh = stream.cuda_stream
-    wl = make_workload()
-    gen = kds.TreeGeneratorB2003D(**TREE_PARAMS)
-    with torch.cuda.stream(stream):
-        Mg = gen.make_tree(wl["map_xyz"], stream=sh)
-    d_xyz = torch.from_numpy(wl["xyz"]).cuda()
-    d_st = torch.from_numpy(wl["st"]).cuda()
-    h_xyz = torch.from_numpy(wl["xyz"]).pin_memory()
-    h_st = torch.from_numpy(wl["st"]).pin_memory()
-    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
-    aligner = kds.CTICPB2003D(**ALIGN_PARAMS)
-    aligner.set_stream(sh)
-    aligner.set_fixed(Mg)
-
-    def step(device_inputs: bool):
-        if device_inputs:
-            t = gen.make_tree(d_xyz, d_st, device=True, stream=sh)
-        else:
-            t = gen.make_tree(h_xyz.numpy(), h_st.numpy(), stream=sh)
-        aligner.set_moving(t)
-        aligner.set_x(wl["X0"])
-        aligner.set_velocities(wl["v0"])
-        ret = aligner.compute()
-        X = aligner.get_x()
-        return t, ret, X
-
-    def timed(device_inputs: bool, n: int):
-        times = []
-        for _ in range(n):
-            with torch.cuda.stream(stream):
-                flush.random_(0, 255)
-            stream.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            t, ret, X = step(device_inputs)
-            e1.record(stream)
-            e1.synchronize()
-            times.append(e0.elapsed_time(e1))
-            t.free()
-        return times
-
-    # warm-up (also builds the CUDA graph of the Gauss-Newton launches)
-    for _ in range(args.warmup):
-        t, ret, X = step(True)
-        t.free()
-    timed(True, 2)
-    scan_tree, ret, X_gpu = step(True)
-    scan_leaves = scan_tree.num_leaves
-    aligner.set_x(X_gpu)
-    touched = aligner.count_touched_nodes()
-    scan_tree.free()
+    sat, poi = make_traces()
+    dev_inputs = [(torch.from_numpy(r.xyz).cuda(), torch.from_numpy(r.stamps).cuda()) for r in sat.requests]
+    host_inputs = [(torch.from_numpy(r.xyz).pin_memory(), torch.from_numpy(r.stamps).pin_memory())
+                   for r in sat.requests]
+    torch.cuda.synchronize()
 
     def barrier():
         torch.cuda.synchronize()
@@ -291,121 +271,135 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- timed region: device-resident inputs
+    def serve_step(inputs, **kw):
+        """One served pass over the saturated trace, timed on the device: events on the
+        current stream around start..drain with a device synchronize on both sides."""
+        srv = kds.Server(tree=TREE, icp=ICP, ct=CT, map_every=MAP_EVERY, **kw)
+        try:
+            for st in sat.streams:
+                srv.add_stream(st.map_xyz, st.max_points)
+            tickets = [srv.submit(r.stream, r.kind, x, s, r.X0, r.v0, r.arrival)
+                       for r, (x, s) in zip(sat.requests, inputs)]
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            srv.start()
+            srv.drain(600.0)
+            torch.cuda.synchronize()
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            res = [srv.result(t) for t in tickets]
+            stats = srv.stats()
+        finally:
+            srv.free()
+        return ms, res, stats
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    for _ in range(args.warmup):
+        serve_step(dev_inputs)
+
+    # ---- timed: device-resident inputs
     launches0 = kds.lib().kds_launch_count()
-    aligner.set_profiling(True)
-    prof = []
-    barrier()
+    times, stats_list = [], []
     with ClockSampler(local) as clk:
-        times = []
         for _ in range(args.steps):
-            times += timed(True, 1)
-            prof.append(aligner.profile())
-    barrier()
-    st16 = np.zeros(16, np.uint64)
-    kds.lib().kds_phase_stamps(st16.ctypes.data)
-    aligner.set_profiling(False)
-    launches = kds.lib().kds_launch_count() - launches0
-    d = lambda a, b: int(st16[b]) - int(st16[a])
-    phases = {"first_block": {"stage_tree_top": d(0, 1), "leaves": d(1, 2), "publish": d(2, 3)},
-              "gn_block": {"sum_partials": d(8, 9), "stage_state": d(9, 10), "unpack": d(10, 11),
-                           "factorize": d(11, 12), "solve": d(12, 13), "update": d(13, 14),
-                           "write_back": d(14, 15)},
-              "unit": "SM cycles"}
-    ms = float(np.mean(times))
-    total_s = float(np.sum(times)) / 1e3
-    if dist:
-        tt = torch.tensor([total_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_s = float(tt.item())
-    value = world * args.steps / total_s
+            ms, served, st = serve_step(dev_inputs)
+            times.append(ms)
+            stats_list.append(st)
+    launches = (kds.lib().kds_launch_count() - launches0) // max(1, args.steps)
+    n_req = len(sat.requests)
+    total_s = max_over_ranks(float(np.sum(times)) / 1e3)
+    value = world * n_req * args.steps / total_s
+    ms_step = float(np.mean(times))
 
-    # ---- e2e: host buffers through the C ABI
-    barrier()
-    e2e_times = timed(False, args.steps)
-    barrier()
-    e2e_total = float(np.sum(e2e_times)) / 1e3
-    if dist:
-        tt = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_total = float(tt.item())
-    e2e_value = world * args.steps / e2e_total
-    h2d = int(wl["xyz"].nbytes + wl["st"].nbytes)
-    d2h = 2 * 8 * (12 + 6) + 4 * 2 + 36  # pose, velocities, result codes and stats read back
+    # ---- e2e: page-locked host inputs copied inside the step
+    e2e_times, e2e_stats = [], None
+    for _ in range(args.steps):
+        ms, served_h, e2e_stats = serve_step(host_inputs)
+        e2e_times.append(ms)
+    e2e_total = max_over_ranks(float(np.sum(e2e_times)) / 1e3)
+    e2e_value = world * n_req * args.steps / e2e_total
+    same_host_dev = all(np.array_equal(a["X"], b["X"]) for a, b in zip(served, served_h))
 
-    # ---- phase breakdown (device-resident): tree build alone, alignment alone
-    def phase_times(n):
-        tb, ta = [], []
-        for _ in range(n):
-            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-            e0.record(stream)
-            t = gen.make_tree(d_xyz, d_st, device=True, stream=sh)
-            e1.record(stream)
-            aligner.set_moving(t)
-            aligner.set_x(wl["X0"])
-            aligner.set_velocities(wl["v0"])
-            aligner.compute()
-            e2.record(stream)
-            e2.synchronize()
-            tb.append(e0.elapsed_time(e1))
-            ta.append(e1.elapsed_time(e2))
-            t.free()
-        return float(np.median(tb)), float(np.median(ta))
-
-    build_ms, align_ms = phase_times(10)
-
-    # ---- roofline of the dominant kernel (fused CT linearization, k_linearize<1>)
-    lin_ms = float(np.mean([p[0] for p in prof if p[1] > 0])) if prof else None
-    tiles = (scan_leaves + 127) // 128
-    alg_bytes = 32 * scan_leaves + 32 * touched + tiles * 97 * 8 * 2
-    import json as _j
+    # ---- profile pass (untimed): device time and algorithmic bytes of the linearizations
+    _, _, pst = serve_step(dev_inputs, profile=1)
     peaks = {}
     try:
-        peaks = _j.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = alg_bytes / (lin_ms * 1e-3) / 1e9 if lin_ms else None
-    roofline = {"bound": "hbm", "kernel": "k_linearize<1> (fused CT-ICP linearization + GN step)",
-                "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": None,
-                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                "alg_bytes_per_launch": alg_bytes, "launch_ms": lin_ms,
-                "model": "32 B x moving surfels + 32 B x distinct fixed nodes touched (%d) + "
-                         "97 doubles x 2 per tile partial" % touched}
+    achieved = pst["alg_bytes"] / (pst["lin_ms"] * 1e-3) / 1e9 if pst["lin_ms"] > 0 else None
+    roofline = {"bound": "hbm", "kernel": "k_linearize<0>/<1> (fused ICP / CT-ICP linearization + GN step), "
+                                          "one launch per kind per tick",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                "traffic": None, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "alg_bytes_per_launch": pst["alg_bytes"] / max(1, 2 * pst["lin_ticks"]),
+                "launch_ms": pst["lin_ms"] / max(1, 2 * pst["lin_ticks"]),
+                "model": "per registration iteration: 32 B x moving surfels + 32 B x distinct fixed nodes "
+                         "touched + (M+7) doubles x 2 per tile partial; summed over the run / summed device "
+                         "time of the linearization launches",
+                "ticks": pst["lin_ticks"], "mean_registrations_per_tick": pst["mean_active"]}
 
-    # ---- accuracy against ground truth
-    et, er = pose_err(X_gpu, wl["X_true"])
+    # ---- latency under Poisson arrivals (10 Hz per stream)
+    lat_srv, _, _ = streams.serve(poi, tree=TREE, icp=ICP, ct=CT, map_every=MAP_EVERY, timeout=600.0)
+    lat = np.array([1e3 * (q["t_done"] - q["t_arrival"]) for q in lat_srv])
+    lat_sat = np.array([1e3 * (q["t_done"] - q["t_arrival"]) for q in served])
+
+    # ---- the plain drop-in on the same trace
+    plain = None
+    if not args.no_plain:
+        p_ms, p_res, _ = serve_step(dev_inputs, serial=1)
+        p_val = n_req / (p_ms / 1e3)
+        same = all(np.array_equal(a["X"], b["X"]) and a["result"] == b["result"] for a, b in zip(served, p_res))
+        lat_p, _, _ = streams.serve(poi, serial=True, tree=TREE, icp=ICP, ct=CT, map_every=MAP_EVERY,
+                                    timeout=600.0)
+        latp = np.array([1e3 * (q["t_done"] - q["t_arrival"]) for q in lat_p])
+        plain = {"value": p_val, "unit": UNIT, "ms_per_step": p_ms, "served_over_plain": value / world / p_val,
+                 "results_identical_to_served": bool(same),
+                 "latency_ms_poisson": {"p50": float(np.percentile(latp, 50)), "p99": float(np.percentile(latp, 99))}}
+
+    st0 = stats_list[-1]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": config_block(wl, Mg, scan_leaves),
-        "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "p50_ms": float(np.percentile(e2e_times, 50)), "p99_ms": float(np.percentile(e2e_times, 99))},
+        "config": config_block(sat),
+        "latency_ms": {"poisson_10hz_per_stream": {"p50": float(np.percentile(lat, 50)),
+                                                    "p99": float(np.percentile(lat, 99))},
+                       "saturated": {"p50": float(np.percentile(lat_sat, 50)),
+                                     "p99": float(np.percentile(lat_sat, 99))}},
+        "plain": plain,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(e2e_stats["h2d_bytes"]),
+                "d2h_bytes_per_step": int(e2e_stats["d2h_bytes"]), "results_identical_to_device_inputs":
+                    bool(same_host_dev)},
         "gpu_launches": int(launches),
-        "breakdown_ms": {"tree_build": build_ms, "align_15_iters": align_ms, "linearize_launch": lin_ms},
-        "linearize_phases": phases,
+        "served": {"ticks": st0["ticks"], "mean_registrations_per_tick": st0["mean_active"],
+                   "build_passes": st0["build_passes"], "trees_built": st0["built_trees"],
+                   "map_rebuilds": st0["map_builds"], "peak_reserved_bytes": st0["peak_reserved"],
+                   "hbm_cap_bytes": st0["hbm_cap"]},
         "roofline": roofline,
         "clocks": clk.summary(),
-        "accuracy": {"ret": int(ret), "t_err_vs_truth_m": et, "r_err_vs_truth_rad": er},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        me = Mg.export()
         threads = min(os.cpu_count() or 1, 8)
-        ctimes, last, M = cpu_reference_run(wl, me, 1000, 12.0, threads)
-        r64 = fp64_reference(wl, M)
-        t64, r64e = pose_err(X_gpu, r64["X"])
-        line["cpu_baseline"] = {"value": 1.0 / float(np.mean(ctimes)), "unit": UNIT, "cores": threads,
+        ctimes = cpu_sample(sat, 12.0, threads)
+        line["cpu_baseline"] = {"value": len(ctimes) / float(np.sum(ctimes)), "unit": UNIT, "cores": threads,
                                 "kind": "port",
-                                "sample": f"{len(ctimes)} full requests in ~12 s: oracle tree build "
-                                          f"(single thread) + CT-ICP MODE_REF32 with {threads} chunks"}
-        line["accuracy"].update({"t_err_vs_fp64_m": t64, "r_err_vs_fp64_rad": r64e,
-                                 "fp64_ret": int(r64["ret"])})
+                                "sample": f"{len(ctimes)} requests of the first map window in ~12 s: oracle tree "
+                                          f"build + ICP_CPU_/CTICP_CPU_ MODE_REF32 with {threads} chunks, against "
+                                          "the streams' initial maps"}
+        line["accuracy"] = accuracy_sample(sat, served)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del aligner
     if dist:
         dist.barrier()
         dist.destroy_process_group()

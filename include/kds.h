@@ -263,6 +263,83 @@ int kds_batch_create(kds_batch** out);
 int kds_batch_run(kds_batch* b, kds_job* jobs, int32_t num_jobs, int32_t use_graph, void* stream);
 void kds_batch_free(kds_batch* b);
 
+/* ------------------------------------------------------------------------------
+ * Served registration (no reference counterpart: the reference runs one tracker
+ * thread with one aligner per role, kd/tracker/tracker_proc_.h:82).  Many sensor
+ * streams submit scan-to-map ICP / CT-ICP registrations; each stream's local surfel
+ * map stays on the device and is rebuilt from the stream's last map_every
+ * registered scans (world frame, deskewed with the estimated velocities); requests
+ * are admitted by device memory and run with continuous batching.  Every
+ * registration computes exactly what kds_tree_build + kds_aligner_compute compute
+ * (CT: TreeAlignerBase_::compute, kd/icp/tree_aligner_base_.h:100-115).
+ * ------------------------------------------------------------------------------ */
+typedef struct kds_server kds_server;
+
+typedef struct {
+  int32_t max_slots;        /* registrations on the device at once (512) */
+  int32_t map_every;        /* map rebuilt from the last map_every scans of a stream (5) */
+  int32_t max_build_trees;  /* trees per build pass (64) */
+  int32_t serial;           /* 1: plain drop-in, one request at a time via the per-call API (0) */
+  int32_t profile;          /* 1: time the linearization launches of every tick and count the
+                               fixed nodes each registration touches (0; adds work) */
+  int32_t max_tiles;        /* tile arena per aligner kind, 128 moving surfels per tile (32768) */
+  int64_t hbm_cap;          /* admission cap in bytes; 0: 90% of the free memory at create */
+  int64_t max_build_points; /* points per build pass (16 Mi) */
+  kds_tree_params tree;     /* scans and maps */
+  kds_aligner_params icp;   /* KDS_ICP requests */
+  kds_aligner_params ct;    /* KDS_CTICP requests */
+} kds_server_params;
+
+typedef struct {
+  int32_t stream;        /* from kds_server_add_stream */
+  int32_t type;          /* KDS_ICP / KDS_CTICP */
+  int64_t n;             /* points */
+  const float* xyz;      /* n*3, host or device memory; must stay valid until the request has finished */
+  const double* stamps;  /* n, host or device memory, or NULL */
+  double X0[12];         /* initial guess (3x4 row-major) */
+  double v0[6];          /* initial velocities (CT) */
+  double arrival;        /* seconds after kds_server_start at which the request arrives */
+} kds_request;
+
+typedef struct {
+  int32_t status;        /* KDS_OK, KDS_ERR_TREE_REJECTED, KDS_ERR_ADMISSION */
+  int32_t result;        /* compute()'s return value */
+  int32_t iterations;
+  int32_t map_version;
+  kds_stats stats;
+  double X[12];
+  double v[6];
+  double t_arrival, t_admit, t_built, t_done; /* seconds after kds_server_start */
+} kds_result;
+
+typedef struct {
+  int64_t submitted, completed, ticks, build_passes, map_builds, built_trees;
+  int64_t hbm_cap, peak_reserved;
+  double mean_active;      /* registrations per tick */
+  double lin_ms;           /* device time of the linearization launches (profile = 1) */
+  int64_t lin_ticks;       /* ticks timed */
+  int64_t leaf_iterations; /* moving surfels linearized, summed over ticks */
+  double alg_bytes;        /* profile = 1: algorithmic bytes of the linearizations (32 B per moving
+                              surfel + 32 B per distinct fixed node touched + tile partials, per iteration) */
+  int64_t h2d_bytes;       /* request points copied from host memory */
+  int64_t d2h_bytes;       /* results read back to the host */
+} kds_server_stats;
+
+void kds_server_params_default(kds_server_params* p);
+int kds_server_create(const kds_server_params* p, kds_server** out);
+/* Adds a stream with its initial map (world-frame points, host) before start;
+ * max_scan_points bounds the scans it will submit. */
+int kds_server_add_stream(kds_server* s, const float* map_xyz, int64_t n, int64_t max_scan_points,
+                          int32_t* stream_id);
+/* Queues a request (arrivals non-decreasing); the ticket identifies its result. */
+int kds_server_submit(kds_server* s, const kds_request* r, int64_t* ticket);
+int kds_server_start(kds_server* s);
+/* Waits for every submitted request (timeout_s <= 0: no limit). */
+int kds_server_drain(kds_server* s, double timeout_s);
+int kds_server_wait(kds_server* s, int64_t ticket, double timeout_s, kds_result* out);
+int kds_server_get_stats(kds_server* s, kds_server_stats* st);
+void kds_server_free(kds_server* s);
+
 /* One linearization that allocates no memory.  This entry point has no counterpart in
  * the reference; it serves callers that cannot allocate device memory while they run
  * (real-time loops that reserve all memory at start-up, code that must not call

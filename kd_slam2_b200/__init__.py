@@ -412,6 +412,92 @@ class Batch:
         return arr
 
 
+# ---------------------------------------------------------------------------- serving
+class Server:
+    """Served registration for many sensor streams (kds_server_*).
+
+    Streams are added with their initial map before start(); requests are submitted
+    with an arrival time (seconds after start).  The host arrays of a request are kept
+    alive by this object until the server is freed.  serial=True runs the plain
+    drop-in: one request at a time through the per-call API.
+    """
+
+    def __init__(self, tree=None, icp=None, ct=None, **params):
+        p = L.ServerParams()
+        _lib.kds_server_params_default(C.byref(p))
+        for k, v in params.items():
+            if not hasattr(p, k):
+                raise AttributeError(f"Server has no parameter {k}")
+            setattr(p, k, v)
+        for name, kw in (("tree", tree), ("icp", icp), ("ct", ct)):
+            for k, v in (kw or {}).items():
+                setattr(getattr(p, name), k, v)
+        self.params = p
+        h = C.c_void_p()
+        _check(_lib.kds_server_create(C.byref(p), C.byref(h)), "kds_server_create")
+        self._h = h
+        self._keep = []
+
+    def __del__(self):
+        self.free()
+
+    def free(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.kds_server_free(self._h)
+            self._h = C.c_void_p(None)
+        self._keep = []
+
+    def add_stream(self, map_xyz, max_scan_points: int) -> int:
+        m = np.ascontiguousarray(map_xyz, np.float32).reshape(-1, 3)
+        sid = C.c_int32()
+        _check(_lib.kds_server_add_stream(self._h, m.ctypes.data, len(m), int(max_scan_points), C.byref(sid)),
+               "kds_server_add_stream")
+        return sid.value
+
+    def submit(self, stream: int, kind: int, xyz, stamps=None, X0=None, v0=None, arrival: float = 0.0) -> int:
+        """xyz/stamps: numpy arrays, or torch tensors (device or pinned host memory)."""
+        r = L.Request()
+        if hasattr(xyz, "data_ptr"):  # torch tensor: float32 [n, 3] and float64 [n], contiguous
+            assert xyz.is_contiguous() and (stamps is None or stamps.is_contiguous())
+            self._keep.append((xyz, stamps))
+            r.n = int(xyz.shape[0])
+            r.xyz = xyz.data_ptr()
+            r.stamps = None if stamps is None else stamps.data_ptr()
+        else:
+            x = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+            st = None if stamps is None else np.ascontiguousarray(stamps, np.float64)
+            self._keep.append((x, st))
+            r.n = len(x)
+            r.xyz = x.ctypes.data
+            r.stamps = None if st is None else st.ctypes.data
+        r.stream = stream
+        r.type = kind
+        r.X0[:] = list(_pose12(identity() if X0 is None else X0))
+        r.v0[:] = list(np.zeros(6) if v0 is None else np.asarray(v0, np.float64))
+        r.arrival = float(arrival)
+        t = C.c_int64()
+        _check(_lib.kds_server_submit(self._h, C.byref(r), C.byref(t)), "kds_server_submit")
+        return t.value
+
+    def start(self) -> None:
+        _check(_lib.kds_server_start(self._h), "kds_server_start")
+
+    def drain(self, timeout: float = 0.0) -> None:
+        _check(_lib.kds_server_drain(self._h, float(timeout)), "kds_server_drain")
+
+    def result(self, ticket: int, timeout: float = 0.0) -> dict:
+        r = L.Result()
+        _check(_lib.kds_server_wait(self._h, int(ticket), float(timeout), C.byref(r)), "kds_server_wait")
+        return {"status": r.status, "result": r.result, "iterations": r.iterations, "map_version": r.map_version,
+                "stats": r.stats.as_dict(), "X": np.array(r.X[:]).reshape(3, 4), "v": np.array(r.v[:]),
+                "t_arrival": r.t_arrival, "t_admit": r.t_admit, "t_built": r.t_built, "t_done": r.t_done}
+
+    def stats(self) -> dict:
+        s = L.ServerStats()
+        _check(_lib.kds_server_get_stats(self._h, C.byref(s)), "kds_server_get_stats")
+        return s.as_dict()
+
+
 def make_job(kind: int, fixed: Tree, moving: Tree, params: L.AlignerParams, X=None, fixed_X=None, v=None,
              fixed_v=None, mode: int = L.KDS_JOB_COMPUTE, stats_mode: bool = False) -> L.Job:
     j = L.Job()
@@ -444,5 +530,5 @@ def tree_params(**kw) -> L.TreeParams:
     return p
 
 
-__all__ = ["Tree", "TreeGeneratorB2003D", "ICPB2003D", "CTICPB2003D", "Batch", "make_job", "aligner_params",
+__all__ = ["Tree", "TreeGeneratorB2003D", "ICPB2003D", "CTICPB2003D", "Batch", "Server", "make_job", "aligner_params",
            "tree_params", "identity", "init", "KdsError"]

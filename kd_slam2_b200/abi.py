@@ -118,6 +118,74 @@ class Job(C.Structure):
     ]
 
 
+class ServerParams(C.Structure):
+    _fields_ = [
+        ("max_slots", C.c_int32),
+        ("map_every", C.c_int32),
+        ("max_build_trees", C.c_int32),
+        ("serial", C.c_int32),
+        ("profile", C.c_int32),
+        ("max_tiles", C.c_int32),
+        ("hbm_cap", C.c_int64),
+        ("max_build_points", C.c_int64),
+        ("tree", TreeParams),
+        ("icp", AlignerParams),
+        ("ct", AlignerParams),
+    ]
+
+
+class Request(C.Structure):
+    _fields_ = [
+        ("stream", C.c_int32),
+        ("type", C.c_int32),
+        ("n", C.c_int64),
+        ("xyz", C.c_void_p),
+        ("stamps", C.c_void_p),
+        ("X0", C.c_double * 12),
+        ("v0", C.c_double * 6),
+        ("arrival", C.c_double),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("result", C.c_int32),
+        ("iterations", C.c_int32),
+        ("map_version", C.c_int32),
+        ("stats", Stats),
+        ("X", C.c_double * 12),
+        ("v", C.c_double * 6),
+        ("t_arrival", C.c_double),
+        ("t_admit", C.c_double),
+        ("t_built", C.c_double),
+        ("t_done", C.c_double),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64),
+        ("completed", C.c_int64),
+        ("ticks", C.c_int64),
+        ("build_passes", C.c_int64),
+        ("map_builds", C.c_int64),
+        ("built_trees", C.c_int64),
+        ("hbm_cap", C.c_int64),
+        ("peak_reserved", C.c_int64),
+        ("mean_active", C.c_double),
+        ("lin_ms", C.c_double),
+        ("lin_ticks", C.c_int64),
+        ("leaf_iterations", C.c_int64),
+        ("alg_bytes", C.c_double),
+        ("h2d_bytes", C.c_int64),
+        ("d2h_bytes", C.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 # Every entry point declared in include/kds.h: name -> (restype, argtypes)
 _P = C.c_void_p
 _I32 = C.c_int32
@@ -171,6 +239,15 @@ SIGNATURES = {
     "kds_batch_create": (C.c_int, [C.POINTER(_P)]),
     "kds_batch_run": (C.c_int, [_P, C.POINTER(Job), _I32, _I32, _P]),
     "kds_batch_free": (None, [_P]),
+    "kds_server_params_default": (None, [C.POINTER(ServerParams)]),
+    "kds_server_create": (C.c_int, [C.POINTER(ServerParams), C.POINTER(_P)]),
+    "kds_server_add_stream": (C.c_int, [_P, _P, _I64, _I64, C.POINTER(_I32)]),
+    "kds_server_submit": (C.c_int, [_P, C.POINTER(Request), C.POINTER(_I64)]),
+    "kds_server_start": (C.c_int, [_P]),
+    "kds_server_drain": (C.c_int, [_P, C.c_double]),
+    "kds_server_wait": (C.c_int, [_P, _I64, C.c_double, C.POINTER(Result)]),
+    "kds_server_get_stats": (C.c_int, [_P, C.POINTER(ServerStats)]),
+    "kds_server_free": (None, [_P]),
     "kds_linearize_static": (C.c_int, [_P, _P, _I32, C.POINTER(AlignerParams), _P, _P, _P, _P, _I32, _P, _P, _P,
                                        C.POINTER(Stats)]),
 }

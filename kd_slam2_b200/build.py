@@ -28,6 +28,7 @@ UNITS = [
     ("kds_build.cu", ["-fmad=false"]),
     ("kds_align.cu", []),
     ("kds_api.cu", []),
+    ("kds_serve.cu", ["-fmad=false"]),
 ]
 
 

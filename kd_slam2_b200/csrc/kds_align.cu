@@ -787,9 +787,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_linearize(const JobIn* __restrict
 }
 
 // Resets control state, seeds state from the job inputs and writes the first caches.
-__global__ void k_init_jobs(const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins, int num_jobs) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= num_jobs) return;
+__device__ void init_job(int j, const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins) {
   const JobIn& Jn = jobs[j];
   JobState& S = states[j];
   for (int i = 0; i < 12; ++i) S.X[i] = Jn.X0[i];
@@ -819,6 +817,12 @@ __global__ void k_init_jobs(const JobIn* jobs, JobState* states, JobOut* outs, L
     return;
   }
   if (!Jn.keep_cache) refresh_caches(S, lins, Jn.lin_begin, Jn.lin_count);
+}
+
+__global__ void k_init_jobs(const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins, int num_jobs) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= num_jobs) return;
+  init_job(j, jobs, states, outs, lins);
 }
 
 // ---------------------------------------------------------------------------
@@ -1100,6 +1104,100 @@ int Runner::fetch(cudaStream_t s, std::vector<JobOut>& outs, std::vector<kds_sta
     set_error("a bounded wait for a tree-top copy gave up; results were computed from global memory");
     return KDS_ERR_TIMEOUT;
   }
+  return KDS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Served-loop helpers (kds_serve.cu): jobs addressed by slot.
+namespace {
+
+__global__ void k_admit_slots(const int32_t* slots, int n, const JobIn* new_jobs, const LinDev* new_lins,
+                              JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int slot = slots[i];
+  jobs[slot] = new_jobs[i];
+  lins[slot] = new_lins[i];
+  init_job(slot, jobs, states, outs, lins);
+}
+
+__global__ void k_collect(int n, const JobState* states, const JobOut* outs, const unsigned long long* touched,
+                          SlotResult* res) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int done = *(const volatile int32_t*)&states[j].done;
+  res[j].done = done;
+  if (!done) return;
+  res[j].touched = touched ? touched[j] : 0ull;
+  const JobOut& O = outs[j];
+  res[j].result = O.result;
+  res[j].iterations = O.iterations;
+  res[j].stats = O.stats;
+  for (int k = 0; k < 12; ++k) res[j].X[k] = O.X[k];
+  for (int k = 0; k < 6; ++k) res[j].v[k] = O.v[k];
+}
+
+}  // namespace
+
+static_assert(kBlock == kTileSurfels, "tile size");
+
+int linearize_smem_setup() {
+  const int bytes = kStageNodes * (int)sizeof(DNode);
+  KDS_CK(cudaFuncSetAttribute((const void*)k_linearize<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  KDS_CK(cudaFuncSetAttribute((const void*)k_linearize<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  KDS_CK(cudaFuncSetAttribute((const void*)k_linearize<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  return KDS_OK;
+}
+
+int launch_admit_slots(const int32_t* d_slots, int n, const JobIn* new_jobs, const LinDev* new_lins, JobIn* jobs,
+                       JobState* states, JobOut* outs, LinDev* lins, cudaStream_t s) {
+  if (n <= 0) return KDS_OK;
+  k_admit_slots<<<(n + 127) / 128, 128, 0, s>>>(d_slots, n, new_jobs, new_lins, jobs, states, outs, lins);
+  count_launch();
+  KDS_CK(cudaGetLastError());
+  return KDS_OK;
+}
+
+int launch_linearize(int kind, int ntiles, const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins,
+                     const TileDev* tiles, double* partials, cudaStream_t s) {
+  if (ntiles <= 0) return KDS_OK;
+  const size_t stage_bytes = (size_t)kStageNodes * sizeof(DNode);
+  if (kind == 0)
+    k_linearize<0><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kStageNodes,
+                                                       partials, nullptr, nullptr);
+  else if (kind == 1)
+    k_linearize<1><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kStageNodes,
+                                                       partials, nullptr, nullptr);
+  else
+    k_linearize<2><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kStageNodes,
+                                                       partials, nullptr, nullptr);
+  count_launch();
+  KDS_CK(cudaGetLastError());
+  return KDS_OK;
+}
+
+int launch_collect(int n, const JobState* states, const JobOut* outs, const unsigned long long* touched,
+                   SlotResult* res, cudaStream_t s) {
+  if (n <= 0) return KDS_OK;
+  k_collect<<<(n + 127) / 128, 128, 0, s>>>(n, states, outs, touched, res);
+  count_launch();
+  KDS_CK(cudaGetLastError());
+  return KDS_OK;
+}
+
+int launch_touch(int kind, const JobIn* jobs, const LinDev* lins, int slot, int num_leaves, uint32_t* bitmap,
+                 int64_t words, unsigned long long* count, cudaStream_t s) {
+  KDS_CK(cudaMemsetAsync(bitmap, 0, (size_t)words * 4, s));
+  KDS_CK(cudaMemsetAsync(count, 0, sizeof(unsigned long long), s));
+  const int g = (num_leaves + 255) / 256;
+  if (g > 0) {
+    if (kind == 0) k_touch<0><<<g, 256, 0, s>>>(jobs + slot, lins, bitmap);
+    else k_touch<1><<<g, 256, 0, s>>>(jobs + slot, lins, bitmap);
+    count_launch();
+  }
+  k_popc<<<64, 256, 0, s>>>(bitmap, words, count);
+  count_launch();
+  KDS_CK(cudaGetLastError());
   return KDS_OK;
 }
 

@@ -137,6 +137,30 @@ int count_touched(Runner& R, int kind, int64_t fixed_nodes, int64_t* out, cudaSt
 // on: 1/0 enables/disables the phase stamps (-1 leaves it); out16 (nullable) receives them
 int phase_stamps(int on, unsigned long long* out16);
 
+// Served-loop helpers.  In the served loop a slot index is both the job index and the
+// fixed-entry index; the tiles of each kind live in their own arena.
+struct SlotResult {
+  int32_t done, result, iterations, pad_;
+  kds_stats stats;
+  double X[12];
+  double v[6];
+  unsigned long long touched;  // distinct fixed nodes the descents visit at the initial state (profiling)
+};
+constexpr int kStageNodes = 2047;
+constexpr int kTileSurfels = 128;  // moving surfels per tile = threads per k_linearize block  // fixed-tree nodes each block stages in shared memory
+// Copies n admitted job records into their slots and initialises those jobs.
+int launch_admit_slots(const int32_t* d_slots, int n, const JobIn* new_jobs, const LinDev* new_lins, JobIn* jobs,
+                       JobState* states, JobOut* outs, LinDev* lins, cudaStream_t s);
+int launch_linearize(int kind, int ntiles, const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins,
+                     const TileDev* tiles, double* partials, cudaStream_t s);
+int launch_collect(int n, const JobState* states, const JobOut* outs, const unsigned long long* touched,
+                   SlotResult* res, cudaStream_t s);
+// Counts the distinct fixed nodes that the descents of job `slot` visit at its current
+// caches into *count (bitmap: words zeroed 32-bit words of scratch).
+int launch_touch(int kind, const JobIn* jobs, const LinDev* lins, int slot, int num_leaves, uint32_t* bitmap,
+                 int64_t words, unsigned long long* count, cudaStream_t s);
+int linearize_smem_setup();
+
 // One linearization whose scratch is a file-scope device array (no allocation).
 // Rejects more than 65,536 moving leaves with KDS_ERR_CAPACITY.
 int linearize_static(const TreeDev& fixed, const TreeDev& moving, int32_t type, const kds_aligner_params& P,

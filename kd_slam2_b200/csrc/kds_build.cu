@@ -972,19 +972,28 @@ struct BuildWs {
   int32_t chunk_cap;
 };
 
+// Bytes of the build workspace for n points in R clouds.
+size_t ws_bytes(int64_t n, int R) {
+  const int64_t cn = 2 * n + 4096 + 4 * (int64_t)R;
+  const int64_t chunk_cap = n / kChunk + n / kBig + 16;
+  const int64_t ntiles = cn / 4096 + 2;
+  const int64_t G = (int64_t)(kMaxDepth + 2) * R;
+  return 2 * carve_size<float4>(n) + 2 * carve_size<double>(n) + 3 * carve_size<int32_t>(n) +
+         carve_size<BNode>(cn) + 4 * carve_size<int32_t>(cn) + carve_size<int32_t>(ntiles) +
+         carve_size<Chunk>(chunk_cap) + 4 * carve_size<int32_t>(chunk_cap) +
+         carve_size<U128>((size_t)11 * (n / kBig + 2)) + 2 * carve_size<double>(R) + carve_size<int64_t>(R + 1) +
+         carve_size<LevelState>(1) + carve_size<int32_t>(kMaxDepth + 2) + carve_size<int32_t>(kLevelBlocks) +
+         7 * carve_size<int32_t>(G) + 3 * carve_size<int32_t>(R) + carve_size<int32_t>(8) + carve_size<TreeDev>(R) +
+         256;
+}
+
 int ws_alloc(BuildWs& w, int64_t n, int R, cudaStream_t s) {
   w.cap_nodes = 2 * n + 4096 + 4 * (int64_t)R;
   w.chunk_cap = (int32_t)(n / kChunk + n / kBig + 16);
   const int64_t cn = w.cap_nodes;
   const int64_t ntiles = cn / 4096 + 2;
   const int64_t G = (int64_t)(kMaxDepth + 2) * R;
-  size_t bytes = 2 * carve_size<float4>(n) + 2 * carve_size<double>(n) + 3 * carve_size<int32_t>(n) +
-                 carve_size<BNode>(cn) + 4 * carve_size<int32_t>(cn) + carve_size<int32_t>(ntiles) +
-                 carve_size<Chunk>(w.chunk_cap) + 4 * carve_size<int32_t>(w.chunk_cap) +
-                 carve_size<U128>((size_t)11 * (n / kBig + 2)) + 2 * carve_size<double>(R) +
-                 carve_size<int64_t>(R + 1) + carve_size<LevelState>(1) + carve_size<int32_t>(kMaxDepth + 2) +
-                 carve_size<int32_t>(kLevelBlocks) + 7 * carve_size<int32_t>(G) + 3 * carve_size<int32_t>(R) +
-                 carve_size<int32_t>(8) + carve_size<TreeDev>(R) + 256;
+  const size_t bytes = ws_bytes(n, R);
   cudaError_t e = cudaMallocAsync(&w.block, bytes, s);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -1033,6 +1042,8 @@ int ws_alloc(BuildWs& w, int64_t n, int R, cudaStream_t s) {
 }
 
 }  // namespace
+
+size_t forest_workspace_bytes(int64_t n, int R) { return ws_bytes(std::max<int64_t>(n, 1), std::max(R, 1)); }
 
 // Builds R trees from R clouds stored back to back (offsets[R+1] on the host).
 // out[r] = NULL and status[r] = KDS_ERR_TREE_REJECTED where makeTree returns nullptr.

@@ -100,6 +100,7 @@ def load() -> C.CDLL:
         "orc_expmap": (None, [C.c_int32, P, P]),
         "orc_iso_mul": (None, [P, P, P]),
         "orc_jacobi3": (None, [P, P, P]),
+        "orc_fx_floor": (None, [C.c_double, C.POINTER(C.c_int64), C.POINTER(C.c_uint64)]),
         "orc_warp_leaf": (None, [P, C.c_float, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
@@ -214,6 +215,13 @@ def linearize(kind: int, fixed: OTree, moving: OTree, caches36, params: AlignPar
                       1 if stats_mode else 0, match.ctypes.data, status.ctypes.data, H.ctypes.data, b.ctypes.data,
                       C.byref(st))
     return match, status, H.reshape(D, D), b, st.as_dict()
+
+
+def fx_floor(v: float) -> int:
+    """floor(v * 2^64) as computed by the oracle's moment sums (a Python int)."""
+    hi, lo = C.c_int64(), C.c_uint64()
+    load().orc_fx_floor(float(v), C.byref(hi), C.byref(lo))
+    return hi.value * (1 << 64) + lo.value
 
 
 def sincosf(x: float):

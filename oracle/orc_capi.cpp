@@ -162,4 +162,6 @@ void orc_jacobi3(const double* A9, double* ev3, double* V9) {
   for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) V9[i * 3 + j] = V[i][j];
 }
 
+void orc_fx_floor(double v, int64_t* hi, uint64_t* lo) { orc::fx_floor_parts(v, hi, lo); }
+
 }  // extern "C"

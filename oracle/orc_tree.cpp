@@ -38,12 +38,34 @@ namespace orc {
 
 typedef __int128 i128;
 
+// floor(v * 2^64) exactly, from the integer mantissa and exponent of v (|v| < 2^62).
+// Splitting v into floor(v) and a fraction in double is not exact for small negative
+// v (1 - |v| can need more than 53 bits), so the floor is formed with integer shifts.
 static inline i128 fx_of(double v) {
-  double hi = std::floor(v);
-  double lo = (v - hi) * 0x1p64;
-  uint64_t lo_u = (uint64_t)lo;
-  return (i128)(int64_t)hi * ((i128)1 << 64) + (i128)lo_u;
+  if (v == 0.0) return 0;
+  int ex = 0;
+  const double fr = std::frexp(std::fabs(v), &ex);   // |v| = fr * 2^ex, fr in [0.5, 1)
+  const uint64_t m = (uint64_t)std::ldexp(fr, 53);   // exact 53-bit integer
+  const int sh = ex - 53 + 64;                       // |v| * 2^64 = m * 2^sh
+  i128 mag = 0;
+  bool rem = false;
+  if (sh >= 0) {
+    mag = (i128)m << sh;
+  } else if (sh > -64) {
+    mag = (i128)(m >> (-sh));
+    rem = (m & ((1ull << (-sh)) - 1ull)) != 0ull;
+  } else {
+    rem = true;
+  }
+  if (v < 0.0) return -mag - (rem ? 1 : 0);
+  return mag;
 }
+void fx_floor_parts(double v, int64_t* hi, uint64_t* lo) {
+  const i128 q = fx_of(v);
+  *hi = (int64_t)(q >> 64);
+  *lo = (uint64_t)q;
+}
+
 static inline double fx_to_d(i128 q) {
   int64_t hi = (int64_t)(q >> 64);
   uint64_t lo = (uint64_t)q;

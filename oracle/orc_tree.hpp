@@ -43,5 +43,8 @@ struct Tree {
 
 Tree build_tree(const float* xyz, const double* stamps, int64_t n, const TreeParams& P);
 void jacobi3(const double A[3][3], double ev[3], double V[3][3]);
+// floor(v * 2^64) as a 128-bit two's complement integer (hi, lo): the fixed-point
+// grid of the per-node moment sums.
+void fx_floor_parts(double v, int64_t* hi, uint64_t* lo);
 
 }  // namespace orc

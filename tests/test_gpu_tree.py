@@ -159,3 +159,31 @@ def test_morph_and_isometry_match_oracle(scene):
     assert np.array_equal(ref.view(np.uint32), e3["mean"][10].view(np.uint32))
     L = G3.extract_compressed_leaves()
     assert np.array_equal(L[:, :3], e3["mean"][e3["leaves"]])
+
+
+def test_tree_build_bit_exact_on_stream_scans():
+    """Scans of the served-registration trace (moving sensors, skewed stamps)."""
+    from kd_slam2_b200 import streams
+    tr = streams.make_trace(7, num_streams=4, scans_per_stream=2, saturate=True, beam_mix=(16, 32), map_scans=2)
+    for r in tr.requests:
+        O, G = build_both(r.xyz, r.stamps, leaf_max_points=16)
+        assert O.accepted and G is not None
+        assert_same_tree(O, G)
+    for s in tr.streams:  # the initial maps, world frame, no stamps
+        O, G = build_both(s.map_xyz, None, leaf_max_points=16)
+        assert_same_tree(O, G)
+
+
+def test_tree_build_bit_exact_near_the_origin():
+    """Many tiny products of mixed sign: the fixed-point floor of small negative values
+    (where 1 - |v| does not fit a double) must agree between the GPU and the oracle."""
+    rng = np.random.default_rng(21)
+    n = 20000
+    xyz = np.empty((n, 3), np.float32)
+    xyz[:, 0] = rng.uniform(-0.05, 0.05, n)
+    xyz[:, 1] = rng.uniform(-0.05, 0.05, n)
+    xyz[:, 2] = -1.0 + rng.normal(scale=1e-4, size=n)  # a plane 1 m below the sensor
+    st = rng.uniform(0.0, 0.1, n)
+    O, G = build_both(xyz, st, leaf_max_points=16, leaf_density=0.0)
+    assert O.accepted and G is not None
+    assert_same_tree(O, G)

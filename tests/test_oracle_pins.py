@@ -193,3 +193,20 @@ def test_jacobi3_matches_eigh():
         assert np.allclose(ev, w, atol=1e-12 * scale, rtol=1e-10)
         assert np.allclose(V.T @ V, np.eye(3), atol=1e-12)
         assert np.allclose(A @ V, V * ev, atol=1e-10 * scale)
+
+
+def test_fixed_point_floor_is_exact():
+    """The moment sums put every float product on a 2^-64 grid by flooring; the floor
+    must be exact for every sign and magnitude -- in particular for small negative
+    products, where 1 - |v| does not fit a double (checked against exact rationals)."""
+    from fractions import Fraction
+    rng = np.random.default_rng(11)
+    f32 = lambda a: np.float32(a)
+    vals = [0.0, -0.0, 1.0, -1.0, 2.0 ** -70, -(2.0 ** -70), -(2.0 ** -64), 2.0 ** -64, -3.25, 3599.9]
+    for _ in range(3000):
+        a = f32(rng.choice([rng.normal() * 30.0, rng.normal() * 1e-3, rng.normal() * 1e-7]))
+        b = f32(rng.choice([rng.normal() * 30.0, rng.normal() * 1e-3, 1.0]))
+        vals.append(float(a) * float(b))  # exact in double: 24 x 24 bit mantissas
+    for v in vals:
+        want = math.floor(Fraction(v) * (1 << 64))
+        assert orc.fx_floor(v) == want, v

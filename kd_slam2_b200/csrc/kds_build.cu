@@ -38,7 +38,9 @@ constexpr int kGridBlocks = 148 * 4;
 constexpr int kLevelBlocks = 64;
 constexpr int kLevelsPerSync = 4;
 constexpr int kMaxDepth = 64;
-constexpr int kUnroll = 4;  // loads in flight per lane in the warp-per-node kernel
+constexpr int kUnroll = 4;  // loads in flight per lane in the warp-per-node phases
+constexpr int kGroup = 128;   // small nodes per block and round
+constexpr int kSmallBlocks = 148 * 2;
 
 // ---------------------------------------------------------------------------
 // 128-bit two's complement fixed point (units of 2^-64)
@@ -264,7 +266,8 @@ __device__ void jacobi3(const double Ain[3][3], double ev[3], double V[3][3]) {
 // FlatLeafPolicy_::fillMetadata over CountLeafPolicy_ and LabelPolicyBase_
 // (kd/tree/flat_leaf_policy_.h:52-108, count_leaf_policy_.h:27-43,
 // label_policy_base_impl_.h:12-97) on FP64 statistics.
-__device__ __noinline__ void decide(const Moments& M, int64_t n, BNode& nd, const BuildParams& P) {
+// Sd: the node's 11 moment sums converted to double (fx_to_d of the exact sums).
+__device__ __noinline__ void decide(const double* Sd, int64_t n, BNode& nd, const BuildParams& P) {
   for (int i = 0; i < 3; ++i) { nd.mean[i] = 0.f; nd.dir[i] = 0.f; }
   nd.dts_mean = 0.0;
   nd.dts_cov = 0.0;
@@ -274,8 +277,6 @@ __device__ __noinline__ void decide(const Moments& M, int64_t n, BNode& nd, cons
   bool is_bad = true;
   if (n > 0) {
     double dn = (double)n;
-    double Sd[11];
-    for (int k = 0; k < 11; ++k) Sd[k] = fx_to_d(M.s[k]);
     nd.dts_mean = Sd[9] / dn;
     nd.dts_cov = Sd[10] / dn - nd.dts_mean * nd.dts_mean;
     for (int i = 0; i < 3; ++i) mean_d[i] = Sd[6 + i] / dn;
@@ -474,11 +475,18 @@ struct PointBufs {
   int32_t* perm;  // final point order (global indices)
 };
 
-// Warp per small node: moments, decision, stable partition (or leaf placement).
+// Small nodes (<= kBig points), block-phased so that the warps of a block run the same
+// code together: each round a block takes up to kGroup consecutive nodes of the level;
+//   A) warp per node: exact moments, reduced across the warp, staged as doubles;
+//   B) thread per node: the leaf/split decision (FP64 eigensolver), 1 node per thread;
+//   C) warp per node: stable partition by whichSide (or leaf placement).
 __global__ void __launch_bounds__(kThreads, 2) k_small(BNode* nodes, const LevelState* ls, PointBufs B,
                                                     const double* ts0, BuildParams P) {
+  __shared__ double sS[kGroup][12];  // 11 sums as doubles, then n (-1: large node)
+  __shared__ BNode sN[kGroup];
   const int lb = ls->lb, le = ls->le, cur = ls->cur;
-  if (lb >= le) return;
+  const int L = le - lb;
+  if (L <= 0) return;
   const float4* pin = B.p[cur];
   const double* sin_ = B.s[cur];
   const int32_t* iin = B.id[cur];
@@ -486,88 +494,124 @@ __global__ void __launch_bounds__(kThreads, 2) k_small(BNode* nodes, const Level
   double* sout = B.s[cur ^ 1];
   int32_t* iout = B.id[cur ^ 1];
   const int lane = threadIdx.x & 31;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  // consecutive nodes go to different blocks (SMs) first
-  const int wslot = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
-  for (int ni = lb + wslot; ni < le; ni += nwarps) {
-    BNode nd = nodes[ni];
-    int s = nd.start, e = nd.end;
-    int n = e - s;
-    if (n > kBig) continue;
-    double t0 = ts0[nd.tree];
-    Moments M;
-    for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
-    // lane l owns points s + 32*k + l, k < K (K <= 32); loads issued kUnroll at a time
-    const int K = (n + 31) >> 5;
-    for (int k0 = 0; k0 < K; k0 += kUnroll) {
-      float4 pv[kUnroll];
-      double sv[kUnroll];
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        int i = s + ((k0 + u) << 5) + lane;
-        if (i < e) { pv[u] = pin[i]; sv[u] = sin_[i]; }
+  const int warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  const int g = min(max((L + (int)gridDim.x - 1) / (int)gridDim.x, 1), kGroup);
+  for (int base = lb + (int)blockIdx.x * g; base < le; base += (int)gridDim.x * g) {
+    const int cnt = min(g, le - base);
+    // A) moments; lane l owns points s + 32*k + l, loads issued kUnroll at a time
+    for (int j = warp; j < cnt; j += nw) {
+      const int s = nodes[base + j].start, e = nodes[base + j].end;
+      const int n = e - s;
+      if (n > kBig) {
+        if (lane == 0) sS[j][11] = -1.0;
+        continue;
       }
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        int i = s + ((k0 + u) << 5) + lane;
-        if (i < e) moments_add_point(M, pv[u], sv[u], t0);
-      }
-    }
-    for (int off = 16; off > 0; off >>= 1)
-      for (int k = 0; k < 11; ++k) M.s[k] = u128_add(M.s[k], shfl_xor_u128(M.s[k], off));
-    decide(M, n, nd, P);
-    if (nd.split) {
-      // side of each owned point as a bit mask, then a stable move with independent loads
-      unsigned bits = 0u;
-      for (int k0 = 0; k0 < K; k0 += kUnroll) {
-        float4 pv[kUnroll];
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-          int i = s + ((k0 + u) << 5) + lane;
-          if (i < e) pv[u] = pin[i];
-        }
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-          int i = s + ((k0 + u) << 5) + lane;
-          if (i < e && which_side_f(nd.mean, nd.dir, pv[u])) bits |= 1u << (k0 + u);
-        }
-      }
-      int nl = __popc(bits);
-      for (int off = 16; off > 0; off >>= 1) nl += __shfl_xor_sync(0xffffffffu, nl, off);
-      const unsigned lt = (1u << lane) - 1u;
-      int cl = 0, cr = 0;
+      const double t0 = ts0[nodes[base + j].tree];
+      Moments M;
+      for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
+      const int K = (n + 31) >> 5;
       for (int k0 = 0; k0 < K; k0 += kUnroll) {
         float4 pv[kUnroll];
         double sv[kUnroll];
-        int iv[kUnroll];
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
           int i = s + ((k0 + u) << 5) + lane;
-          if (i < e) { pv[u] = pin[i]; sv[u] = sin_[i]; iv[u] = iin[i]; }
+          if (i < e) { pv[u] = pin[i]; sv[u] = sin_[i]; }
         }
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
           int i = s + ((k0 + u) << 5) + lane;
-          bool valid = i < e;
-          bool left = valid && ((bits >> (k0 + u)) & 1u);
-          unsigned bl = __ballot_sync(0xffffffffu, left);
-          unsigned br = __ballot_sync(0xffffffffu, valid && !left);
-          if (valid) {
-            int dst = left ? (s + cl + __popc(bl & lt)) : (s + nl + cr + __popc(br & lt));
-            pout[dst] = pv[u];
-            sout[dst] = sv[u];
-            iout[dst] = iv[u];
-          }
-          cl += __popc(bl);
-          cr += __popc(br);
+          if (i < e) moments_add_point(M, pv[u], sv[u], t0);
         }
       }
-      nd.mid = s + nl;
-    } else {
-      for (int i = s + lane; i < e; i += 32) B.perm[i] = iin[i];
-      nd.mid = e;
+      for (int off = 16; off > 0; off >>= 1)
+        for (int k = 0; k < 11; ++k) M.s[k] = u128_add(M.s[k], shfl_xor_u128(M.s[k], off));
+      if (lane < 11) {
+        U128 q = M.s[0];
+#pragma unroll
+        for (int k = 1; k < 11; ++k)
+          if (lane == k) q = M.s[k];
+        sS[j][lane] = fx_to_d(q);
+      }
+      if (lane == 0) sS[j][11] = (double)n;
     }
-    if (lane == 0) nodes[ni] = nd;
+    __syncthreads();
+    // B) decisions
+    if ((int)threadIdx.x < cnt) {
+      const int j = threadIdx.x;
+      if (sS[j][11] >= 0.0) {
+        BNode nd = nodes[base + j];
+        decide(&sS[j][0], nd.end - nd.start, nd, P);
+        sN[j] = nd;
+      }
+    }
+    __syncthreads();
+    // C) partition
+    for (int j = warp; j < cnt; j += nw) {
+      if (sS[j][11] < 0.0) continue;
+      const int s = sN[j].start, e = sN[j].end;
+      const int K = (e - s + 31) >> 5;
+      int mid = e;
+      if (sN[j].split) {
+        const float mean[3] = {sN[j].mean[0], sN[j].mean[1], sN[j].mean[2]};
+        const float dir[3] = {sN[j].dir[0], sN[j].dir[1], sN[j].dir[2]};
+        // side of each owned point as a bit mask, then a stable move with independent loads
+        unsigned bits = 0u;
+        for (int k0 = 0; k0 < K; k0 += kUnroll) {
+          float4 pv[kUnroll];
+#pragma unroll
+          for (int u = 0; u < kUnroll; ++u) {
+            int i = s + ((k0 + u) << 5) + lane;
+            if (i < e) pv[u] = pin[i];
+          }
+#pragma unroll
+          for (int u = 0; u < kUnroll; ++u) {
+            int i = s + ((k0 + u) << 5) + lane;
+            if (i < e && which_side_f(mean, dir, pv[u])) bits |= 1u << (k0 + u);
+          }
+        }
+        int nl = __popc(bits);
+        for (int off = 16; off > 0; off >>= 1) nl += __shfl_xor_sync(0xffffffffu, nl, off);
+        const unsigned lt = (1u << lane) - 1u;
+        int cl = 0, cr = 0;
+        for (int k0 = 0; k0 < K; k0 += kUnroll) {
+          float4 pv[kUnroll];
+          double sv[kUnroll];
+          int iv[kUnroll];
+#pragma unroll
+          for (int u = 0; u < kUnroll; ++u) {
+            int i = s + ((k0 + u) << 5) + lane;
+            if (i < e) { pv[u] = pin[i]; sv[u] = sin_[i]; iv[u] = iin[i]; }
+          }
+#pragma unroll
+          for (int u = 0; u < kUnroll; ++u) {
+            int i = s + ((k0 + u) << 5) + lane;
+            bool valid = i < e;
+            bool left = valid && ((bits >> (k0 + u)) & 1u);
+            unsigned bl = __ballot_sync(0xffffffffu, left);
+            unsigned br = __ballot_sync(0xffffffffu, valid && !left);
+            if (valid) {
+              int dst = left ? (s + cl + __popc(bl & lt)) : (s + nl + cr + __popc(br & lt));
+              pout[dst] = pv[u];
+              sout[dst] = sv[u];
+              iout[dst] = iv[u];
+            }
+            cl += __popc(bl);
+            cr += __popc(br);
+          }
+        }
+        mid = s + nl;
+      } else {
+        for (int i = s + lane; i < e; i += 32) B.perm[i] = iin[i];
+      }
+      __syncwarp();
+      if (lane == 0) {
+        sN[j].mid = mid;
+        nodes[base + j] = sN[j];
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -584,6 +628,13 @@ __global__ void k_big_plan(const BNode* nodes, LevelState* ls, Chunk* chunks, in
                            int32_t* node_chunk0, U128* acc) {
   __shared__ int sm[32];
   const int lb = ls->lb, le = ls->le;
+  if (ls->max_size <= kBig) {  // no large node on this level
+    if (threadIdx.x == 0) {
+      ls->num_chunks = 0;
+      ls->num_big = 0;
+    }
+    return;
+  }
   int carry_c = 0, carry_b = 0;
   for (int base = lb; base < le; base += blockDim.x) {
     int i = base + threadIdx.x;
@@ -653,9 +704,9 @@ __global__ void k_big_decide(BNode* nodes, const LevelState* ls, const int32_t* 
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += gridDim.x * blockDim.x) {
     int i = big_list[t];
     BNode nd = nodes[i];
-    Moments M;
-    for (int k = 0; k < 11; ++k) M.s[k] = acc[(size_t)t * 11 + k];
-    decide(M, nd.end - nd.start, nd, P);
+    double Sd[11];
+    for (int k = 0; k < 11; ++k) Sd[k] = fx_to_d(acc[(size_t)t * 11 + k]);
+    decide(Sd, nd.end - nd.start, nd, P);
     nodes[i] = nd;
   }
 }
@@ -1121,7 +1172,7 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   const int cb = std::min<int>(w.chunk_cap, kGridBlocks * 2);
   for (int round = 0; round < kMaxDepth; ++round) {
     for (int k = 0; k < kLevelsPerSync; ++k) {
-      k_small<<<kGridBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.B, w.ts0, P);
+      k_small<<<kSmallBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.B, w.ts0, P);
       count_launch();
       if (host_max > kBig) {
         k_big_plan<<<1, 1024, 0, s>>>(w.nodes, w.ls, w.chunks, w.chunk_cap, w.big_list, w.node_chunk0, w.acc);

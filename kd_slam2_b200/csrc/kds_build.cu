@@ -146,16 +146,54 @@ struct Moments {
   U128 s[11];
 };
 
+// Fast path of the same floors.  A float x with x == 0 or 2^-25 <= |x| < 2^15 has no
+// bit below 2^-48, so x = X * 2^-48 with an integer |X| < 2^63.  Then
+// floor(x * y * 2^64) = floor(X * Y / 2^32) (an arithmetic shift of the 128-bit
+// product) and floor(x * 2^64) = X * 2^16, both exact.
+__device__ __forceinline__ bool fx_grid48(float x, long long& X) {
+  X = __float2ll_rn(x * 0x1p48f);
+  const float a = fabsf(x);
+  return a == 0.0f || a >= 0x1p-25f;
+}
+__device__ __forceinline__ U128 fx_prod48(long long X, long long Y) {
+  const unsigned long long lo = (unsigned long long)X * (unsigned long long)Y;
+  const long long hi = __mul64hi(X, Y);
+  U128 r;
+  r.lo = (lo >> 32) | ((unsigned long long)hi << 32);
+  r.hi = (unsigned long long)(hi >> 32);
+  return r;
+}
+__device__ __forceinline__ U128 fx_single48(long long X) {
+  U128 r;
+  r.lo = (unsigned long long)X << 16;
+  r.hi = (unsigned long long)(X >> 48);
+  return r;
+}
+
 __device__ __forceinline__ void moments_add_point(Moments& M, float4 p, double st, double ts0) {
-  M.s[0] = u128_add(M.s[0], fx_ff(p.x, p.x));
-  M.s[1] = u128_add(M.s[1], fx_ff(p.x, p.y));
-  M.s[2] = u128_add(M.s[2], fx_ff(p.x, p.z));
-  M.s[3] = u128_add(M.s[3], fx_ff(p.y, p.y));
-  M.s[4] = u128_add(M.s[4], fx_ff(p.y, p.z));
-  M.s[5] = u128_add(M.s[5], fx_ff(p.z, p.z));
-  M.s[6] = u128_add(M.s[6], fx_f(p.x));
-  M.s[7] = u128_add(M.s[7], fx_f(p.y));
-  M.s[8] = u128_add(M.s[8], fx_f(p.z));
+  long long X, Y, Z;
+  const bool gx = fx_grid48(p.x, X), gy = fx_grid48(p.y, Y), gz = fx_grid48(p.z, Z);
+  if (gx && gy && gz) {
+    M.s[0] = u128_add(M.s[0], fx_prod48(X, X));
+    M.s[1] = u128_add(M.s[1], fx_prod48(X, Y));
+    M.s[2] = u128_add(M.s[2], fx_prod48(X, Z));
+    M.s[3] = u128_add(M.s[3], fx_prod48(Y, Y));
+    M.s[4] = u128_add(M.s[4], fx_prod48(Y, Z));
+    M.s[5] = u128_add(M.s[5], fx_prod48(Z, Z));
+    M.s[6] = u128_add(M.s[6], fx_single48(X));
+    M.s[7] = u128_add(M.s[7], fx_single48(Y));
+    M.s[8] = u128_add(M.s[8], fx_single48(Z));
+  } else {
+    M.s[0] = u128_add(M.s[0], fx_ff(p.x, p.x));
+    M.s[1] = u128_add(M.s[1], fx_ff(p.x, p.y));
+    M.s[2] = u128_add(M.s[2], fx_ff(p.x, p.z));
+    M.s[3] = u128_add(M.s[3], fx_ff(p.y, p.y));
+    M.s[4] = u128_add(M.s[4], fx_ff(p.y, p.z));
+    M.s[5] = u128_add(M.s[5], fx_ff(p.z, p.z));
+    M.s[6] = u128_add(M.s[6], fx_f(p.x));
+    M.s[7] = u128_add(M.s[7], fx_f(p.y));
+    M.s[8] = u128_add(M.s[8], fx_f(p.z));
+  }
   double dt = st - ts0;
   M.s[9] = u128_add(M.s[9], fx_d(dt));
   M.s[10] = u128_add(M.s[10], fx_d(dt * dt));

@@ -384,7 +384,8 @@ def main():
         "gpu_launches": int(launches),
         "served": {"ticks": st0["ticks"], "mean_registrations_per_tick": st0["mean_active"],
                    "build_passes": st0["build_passes"], "trees_built": st0["built_trees"],
-                   "map_rebuilds": st0["map_builds"], "peak_reserved_bytes": st0["peak_reserved"],
+                   "map_rebuilds": st0["map_builds"], "build_pass_ms": st0["build_ms"],
+                   "build_points": st0["build_points"], "peak_reserved_bytes": st0["peak_reserved"],
                    "hbm_cap_bytes": st0["hbm_cap"]},
         "roofline": roofline,
         "clocks": clk.summary(),

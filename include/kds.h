@@ -323,6 +323,8 @@ typedef struct {
                               surfel + 32 B per distinct fixed node touched + tile partials, per iteration) */
   int64_t h2d_bytes;       /* request points copied from host memory */
   int64_t d2h_bytes;       /* results read back to the host */
+  double build_ms;         /* wall time of the tree-build passes (requests and map rebuilds) */
+  int64_t build_points;    /* points those passes built */
 } kds_server_stats;
 
 void kds_server_params_default(kds_server_params* p);
@@ -338,6 +340,11 @@ int kds_server_start(kds_server* s);
 int kds_server_drain(kds_server* s, double timeout_s);
 int kds_server_wait(kds_server* s, int64_t ticket, double timeout_s, kds_result* out);
 int kds_server_get_stats(kds_server* s, kds_server_stats* st);
+/* Timeline of the served loop for diagnosis: rows of 4 doubles (kind, count, begin,
+ * end); kind 0 = a tree-build pass (count = points), kind 1 = a Gauss-Newton tick from
+ * its launch to the host reading its results (count = registrations in the tick);
+ * times in seconds after kds_server_start.  *n = rows recorded (may exceed cap). */
+int kds_server_get_trace(kds_server* s, double* rows4, int32_t cap, int32_t* n);
 void kds_server_free(kds_server* s);
 
 /* One linearization that allocates no memory.  This entry point has no counterpart in

@@ -492,6 +492,14 @@ class Server:
                 "stats": r.stats.as_dict(), "X": np.array(r.X[:]).reshape(3, 4), "v": np.array(r.v[:]),
                 "t_arrival": r.t_arrival, "t_admit": r.t_admit, "t_built": r.t_built, "t_done": r.t_done}
 
+    def trace(self) -> np.ndarray:
+        """Timeline rows (kind, count, begin_s, end_s): kind 0 build pass, 1 tick."""
+        n = C.c_int32()
+        _check(_lib.kds_server_get_trace(self._h, None, 0, C.byref(n)), "kds_server_get_trace")
+        out = np.zeros((max(n.value, 1), 4))
+        _check(_lib.kds_server_get_trace(self._h, out.ctypes.data, n.value, C.byref(n)), "kds_server_get_trace")
+        return out[:n.value]
+
     def stats(self) -> dict:
         s = L.ServerStats()
         _check(_lib.kds_server_get_stats(self._h, C.byref(s)), "kds_server_get_stats")

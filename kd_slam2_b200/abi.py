@@ -180,6 +180,8 @@ class ServerStats(C.Structure):
         ("alg_bytes", C.c_double),
         ("h2d_bytes", C.c_int64),
         ("d2h_bytes", C.c_int64),
+        ("build_ms", C.c_double),
+        ("build_points", C.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -247,6 +249,7 @@ SIGNATURES = {
     "kds_server_drain": (C.c_int, [_P, C.c_double]),
     "kds_server_wait": (C.c_int, [_P, _I64, C.c_double, C.POINTER(Result)]),
     "kds_server_get_stats": (C.c_int, [_P, C.POINTER(ServerStats)]),
+    "kds_server_get_trace": (C.c_int, [_P, _P, _I32, C.POINTER(_I32)]),
     "kds_server_free": (None, [_P]),
     "kds_linearize_static": (C.c_int, [_P, _P, _I32, C.POINTER(AlignerParams), _P, _P, _P, _P, _I32, _P, _P, _P,
                                        C.POINTER(Stats)]),

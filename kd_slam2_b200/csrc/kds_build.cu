@@ -40,7 +40,7 @@ constexpr int kLevelsPerSync = 4;
 constexpr int kMaxDepth = 64;
 constexpr int kUnroll = 4;  // loads in flight per lane in the warp-per-node phases
 constexpr int kGroup = 128;   // small nodes per block and round
-constexpr int kSmallBlocks = 148 * 2;
+constexpr int kSmallBlocks = 148 * 8;  // short-lived blocks: other streams' kernels interleave
 
 // ---------------------------------------------------------------------------
 // 128-bit two's complement fixed point (units of 2^-64)
@@ -436,6 +436,15 @@ __device__ __forceinline__ int block_scan(int v, int* sm, int* total) {
   return wprefix + x - v;
 }
 
+// The node range [b, e) of this block when gridDim.x blocks split the current level.
+__device__ __forceinline__ void level_range(const LevelState* ls, int& b, int& e) {
+  const int lb = ls->lb, le = ls->le;
+  const int nl = le - lb;
+  const int per = (nl + gridDim.x - 1) / gridDim.x;
+  b = lb + blockIdx.x * per;
+  e = min(b + per, le);
+}
+
 // ---------------------------------------------------------------------------
 // Kernels
 
@@ -661,23 +670,56 @@ struct Chunk {
   int32_t big;  // ordinal among the level's large nodes
 };
 
-// One block: lists the level's large nodes and their chunks (block scans with carry).
-__global__ void k_big_plan(const BNode* nodes, LevelState* ls, Chunk* chunks, int32_t chunk_cap, int32_t* big_list,
-                           int32_t* node_chunk0, U128* acc) {
+// Large nodes of the level and their kChunk-point chunks, listed in node order by
+// kLevelBlocks blocks over contiguous node ranges: per-block counts first, then each
+// block writes its list at the prefix of the blocks before it.
+__global__ void k_big_sums(const BNode* nodes, const LevelState* ls, int32_t* bbig) {
   __shared__ int sm[32];
-  const int lb = ls->lb, le = ls->le;
+  if (ls->max_size <= kBig) return;  // no large node on this level
+  int b, e;
+  level_range(ls, b, e);
+  int nc = 0, nb = 0;
+  for (int i = b + threadIdx.x; i < e; i += blockDim.x) {
+    const int n = nodes[i].end - nodes[i].start;
+    if (n > kBig) {
+      nc += (n + kChunk - 1) / kChunk;
+      nb += 1;
+    }
+  }
+  int tc, tb;
+  block_scan(nc, sm, &tc);
+  block_scan(nb, sm, &tb);
+  if (threadIdx.x == 0) {
+    bbig[2 * blockIdx.x] = tc;
+    bbig[2 * blockIdx.x + 1] = tb;
+  }
+}
+
+__global__ void k_big_plan(const BNode* nodes, LevelState* ls, const int32_t* bbig, Chunk* chunks, int32_t chunk_cap,
+                           int32_t* big_list, int32_t* node_chunk0, U128* acc) {
+  __shared__ int sm[32];
   if (ls->max_size <= kBig) {  // no large node on this level
-    if (threadIdx.x == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
       ls->num_chunks = 0;
       ls->num_big = 0;
     }
     return;
   }
-  int carry_c = 0, carry_b = 0;
-  for (int base = lb; base < le; base += blockDim.x) {
+  int b, e;
+  level_range(ls, b, e);
+  int carry_c = 0, carry_b = 0, all_c = 0, all_b = 0;
+  for (int k = 0; k < (int)gridDim.x; ++k) {
+    if (k < (int)blockIdx.x) {
+      carry_c += bbig[2 * k];
+      carry_b += bbig[2 * k + 1];
+    }
+    all_c += bbig[2 * k];
+    all_b += bbig[2 * k + 1];
+  }
+  for (int base = b; base < e; base += blockDim.x) {
     int i = base + threadIdx.x;
     int n = 0;
-    if (i < le) n = nodes[i].end - nodes[i].start;
+    if (i < e) n = nodes[i].end - nodes[i].start;
     bool big = n > kBig;
     int nc = big ? (n + kChunk - 1) / kChunk : 0;
     int tc, tb;
@@ -686,13 +728,13 @@ __global__ void k_big_plan(const BNode* nodes, LevelState* ls, Chunk* chunks, in
     if (big) {
       big_list[ob] = i;
       node_chunk0[ob] = oc;
-      int s = nodes[i].start, e = nodes[i].end;
+      int s = nodes[i].start, en = nodes[i].end;
       for (int k = 0; k < nc; ++k) {
         int c = oc + k;
         if (c < chunk_cap) {
           chunks[c].node = i;
           chunks[c].begin = s + k * kChunk;
-          chunks[c].end = min(s + (k + 1) * kChunk, e);
+          chunks[c].end = min(s + (k + 1) * kChunk, en);
           chunks[c].big = ob;
         }
       }
@@ -701,10 +743,10 @@ __global__ void k_big_plan(const BNode* nodes, LevelState* ls, Chunk* chunks, in
     carry_c += tc;
     carry_b += tb;
   }
-  if (threadIdx.x == 0) {
-    ls->num_chunks = min(carry_c, chunk_cap);
-    ls->num_big = carry_b;
-    if (carry_c > chunk_cap) ls->error = 1;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ls->num_chunks = min(all_c, chunk_cap);
+    ls->num_big = all_b;
+    if (all_c > chunk_cap) ls->error = 1;
   }
 }
 
@@ -836,13 +878,6 @@ __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, c
 }
 
 // ---- children ------------------------------------------------------------------------
-__device__ __forceinline__ void level_range(const LevelState* ls, int& b, int& e) {
-  const int lb = ls->lb, le = ls->le;
-  const int nl = le - lb;
-  const int per = (nl + gridDim.x - 1) / gridDim.x;
-  b = lb + blockIdx.x * per;
-  e = min(b + per, le);
-}
 
 __global__ void k_level_sums(const BNode* nodes, const LevelState* ls, int32_t* bsum) {
   __shared__ int sm[32];
@@ -863,6 +898,7 @@ __global__ void k_level_children(BNode* nodes, LevelState* ls, const int32_t* bs
   int pre = 0;
   for (int k = 0; k < (int)blockIdx.x; ++k) pre += bsum[k];
   int carry = 0;
+  int maxc = 0;  // largest child this thread created
   for (int base = b; base < e; base += blockDim.x) {
     int i = base + threadIdx.x;
     bool sp = (i < e) && nodes[i].split;
@@ -895,12 +931,14 @@ __global__ void k_level_children(BNode* nodes, LevelState* ls, const int32_t* bs
             c.par_has = nd.has_prop;
             for (int j = 0; j < 3; ++j) c.par_prop[j] = nd.prop[j];
             nodes[li + k] = c;
-            atomicMax(&ls->max_next, c.end - c.start);
+            maxc = max(maxc, c.end - c.start);
           }
         }
       }
     }
   }
+  for (int off = 16; off > 0; off >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, off));
+  if ((threadIdx.x & 31) == 0 && maxc > 0) atomicMax(&ls->max_next, maxc);
 }
 
 __global__ void k_level_advance(LevelState* ls, const int32_t* bsum, int nblocks, int32_t* level_begin) {
@@ -935,41 +973,61 @@ __global__ void k_alive(const BNode* nodes, int32_t lb, int32_t le, int32_t* ali
 }
 
 // group = (level, tree); nodes of one group are contiguous in global order
+// Counts per (level, tree) group; lanes with the same group combine their counts
+// before one atomic per group and warp.
 __global__ void k_group_counts(const BNode* nodes, int32_t total, const int32_t* alive, int R, int32_t* cnt,
                                int32_t* lcnt, int32_t* ucnt, int32_t* leaf_flag) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-    const BNode& nd = nodes[i];
-    int g = nd.level * R + nd.tree;
-    atomicAdd(&ucnt[nd.tree], 1);
-    int lf = 0;
-    if (alive[i]) {
-      atomicAdd(&cnt[g], 1);
-      if (nd.left < 0 && nd.right < 0) {
-        atomicAdd(&lcnt[g], 1);
-        lf = 1;
-      }
+  const int lane = threadIdx.x & 31;
+  for (int base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+    const int i = base + threadIdx.x;
+    const bool valid = i < total;
+    int tree = -1, g = -1;
+    bool al = false, leaf = false;
+    if (valid) {
+      const BNode& nd = nodes[i];
+      tree = nd.tree;
+      g = nd.level * R + nd.tree;
+      al = alive[i] != 0;
+      leaf = al && nd.left < 0 && nd.right < 0;
+      leaf_flag[i] = leaf ? 1 : 0;
     }
-    leaf_flag[i] = lf;
+    const unsigned pt = __match_any_sync(0xffffffffu, tree);
+    if (valid && lane == __ffs(pt) - 1) atomicAdd(&ucnt[tree], __popc(pt));
+    const unsigned pg = __match_any_sync(0xffffffffu, g);
+    const unsigned ba = __ballot_sync(0xffffffffu, al);
+    const unsigned bl = __ballot_sync(0xffffffffu, leaf);
+    if (valid && lane == __ffs(pg) - 1) {
+      const int c = __popc(pg & ba), lc = __popc(pg & bl);
+      if (c) atomicAdd(&cnt[g], c);
+      if (lc) atomicAdd(&lcnt[g], lc);
+    }
   }
 }
 
-// exclusive prefix over groups in (level, tree) order, and per-tree level offsets
+// Exclusive prefix over groups in (level, tree) order (one block, scans with carry),
+// and per-tree level offsets (one thread per tree).
 __global__ void k_group_tables(int depth, int R, const int32_t* cnt, const int32_t* lcnt, int32_t* gp, int32_t* lgp,
                                int32_t* to, int32_t* lto, int32_t* tot_nodes, int32_t* tot_leaves) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  int a = 0, la = 0;
-  for (int l = 0; l < depth; ++l)
-    for (int t = 0; t < R; ++t) {
-      int g = l * R + t;
-      gp[g] = a;
-      lgp[g] = la;
-      a += cnt[g];
-      la += lcnt[g];
+  __shared__ int sm[32];
+  const int G = depth * R;
+  int carry = 0, lcarry = 0;
+  for (int base = 0; base < G; base += blockDim.x) {
+    const int g = base + threadIdx.x;
+    const int c = g < G ? cnt[g] : 0, lc = g < G ? lcnt[g] : 0;
+    int tc, tl;
+    const int o = block_scan(c, sm, &tc);
+    const int lo = block_scan(lc, sm, &tl);
+    if (g < G) {
+      gp[g] = carry + o;
+      lgp[g] = lcarry + lo;
     }
-  for (int t = 0; t < R; ++t) {
+    carry += tc;
+    lcarry += tl;
+  }
+  for (int t = threadIdx.x; t < R; t += blockDim.x) {
     int s = 0, ls = 0;
     for (int l = 0; l < depth; ++l) {
-      int g = l * R + t;
+      const int g = l * R + t;
       to[g] = s;
       lto[g] = ls;
       s += cnt[g];
@@ -1055,6 +1113,7 @@ struct BuildWs {
   LevelState* ls;
   int32_t* level_begin;
   int32_t* bsum;
+  int32_t* bbig;  // per-block (chunks, large nodes) of the level
   int32_t *cnt, *lcnt, *ucnt, *gp, *lgp, *to, *lto, *tot_nodes, *tot_leaves, *scan_tot;
   TreeDev* trees;
   int64_t cap_nodes;
@@ -1072,6 +1131,7 @@ size_t ws_bytes(int64_t n, int R) {
          carve_size<Chunk>(chunk_cap) + 4 * carve_size<int32_t>(chunk_cap) +
          carve_size<U128>((size_t)11 * (n / kBig + 2)) + 2 * carve_size<double>(R) + carve_size<int64_t>(R + 1) +
          carve_size<LevelState>(1) + carve_size<int32_t>(kMaxDepth + 2) + carve_size<int32_t>(kLevelBlocks) +
+         carve_size<int32_t>(2 * kLevelBlocks) +
          7 * carve_size<int32_t>(G) + 3 * carve_size<int32_t>(R) + carve_size<int32_t>(8) + carve_size<TreeDev>(R) +
          256;
 }
@@ -1116,6 +1176,7 @@ int ws_alloc(BuildWs& w, int64_t n, int R, cudaStream_t s) {
   w.ls = carve<LevelState>(p, 1);
   w.level_begin = carve<int32_t>(p, kMaxDepth + 2);
   w.bsum = carve<int32_t>(p, kLevelBlocks);
+  w.bbig = carve<int32_t>(p, 2 * kLevelBlocks);
   w.cnt = carve<int32_t>(p, G);
   w.lcnt = carve<int32_t>(p, G);
   w.gp = carve<int32_t>(p, G);
@@ -1213,13 +1274,15 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
       k_small<<<kSmallBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.B, w.ts0, P);
       count_launch();
       if (host_max > kBig) {
-        k_big_plan<<<1, 1024, 0, s>>>(w.nodes, w.ls, w.chunks, w.chunk_cap, w.big_list, w.node_chunk0, w.acc);
+        k_big_sums<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig);
+        k_big_plan<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig, w.chunks, w.chunk_cap, w.big_list,
+                                                     w.node_chunk0, w.acc);
         k_big_moments<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.B, w.ts0, w.nodes, w.acc);
         k_big_decide<<<64, 128, 0, s>>>(w.nodes, w.ls, w.big_list, w.acc, P);
         k_big_count<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_nl);
         k_big_offsets<<<64, 128, 0, s>>>(w.nodes, w.ls, w.big_list, w.node_chunk0, w.chunk_nl, w.chunk_loff);
         k_big_scatter<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_loff);
-        for (int c = 0; c < 6; ++c) count_launch();
+        for (int c = 0; c < 7; ++c) count_launch();
       }
       k_level_sums<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum);
       k_level_children<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum, (int32_t)w.cap_nodes);
@@ -1260,7 +1323,7 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   if (rc) return rc;
   rc = scan_exclusive(w.leaf_flag, w.lrank, total, w.tile_sums, w.scan_tot, s);
   if (rc) return rc;
-  k_group_tables<<<1, 1, 0, s>>>(depth, R, w.cnt, w.lcnt, w.gp, w.lgp, w.to, w.lto, w.tot_nodes, w.tot_leaves);
+  k_group_tables<<<1, 1024, 0, s>>>(depth, R, w.cnt, w.lcnt, w.gp, w.lgp, w.to, w.lto, w.tot_nodes, w.tot_leaves);
   count_launch();
   std::vector<int32_t> tn(R), tl(R), tu(R);
   std::vector<double> ts0(R);

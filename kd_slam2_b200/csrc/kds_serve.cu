@@ -32,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -256,6 +257,12 @@ struct kds_server {
   int64_t ticks = 0, build_passes = 0, map_builds = 0, built_trees = 0;
   double sum_active = 0.0, lin_ms = 0.0, alg_bytes = 0.0;
   int64_t lin_launches = 0, leaf_iterations = 0, h2d_bytes = 0, d2h_bytes = 0;
+  double build_ms = 0.0;      // wall time of the build passes
+  // timeline: kind (0 build pass, 1 tick), count (points / registrations), begin, end [s]
+  std::vector<std::array<double, 4>> trace;
+  double tick_t0[2] = {0.0, 0.0};
+  int tick_n[2] = {0, 0};
+  int64_t build_points = 0;   // points built (requests and maps)
 };
 
 namespace {
@@ -414,6 +421,7 @@ void build_loop(kds_server* s) {
       }
     }
     // one forest pass over the maps and the admitted requests
+    const auto pass_t0 = std::chrono::steady_clock::now();
     const int R = (int)(maps.size() + batch.size());
     std::vector<int64_t> off(R + 1, 0);
     for (int i = 0; i < (int)maps.size(); ++i) off[i + 1] = off[i] + maps[i].points;
@@ -476,6 +484,12 @@ void build_loop(kds_server* s) {
       s->reserved -= transient;
       s->h2d_bytes += h2d;
       ++s->build_passes;
+      s->build_ms += 1e3 * seconds_since(pass_t0);
+      s->build_points += N;
+      {
+        const double t1 = seconds_since(s->t0);
+        s->trace.push_back({0.0, (double)N, t1 - seconds_since(pass_t0), t1});
+      }
       s->built_trees += R;
       for (int i = 0; i < (int)maps.size(); ++i) {
         cudaEventDestroy(maps[i].ready);
@@ -725,6 +739,8 @@ void gn_loop(kds_server* s) {
         for (Request* r : active_cur) s->leaf_iterations += r->tree->d.num_leaves;
         s->sum_active += (double)active_cur.size();
         ++s->ticks;
+        s->tick_t0[buf] = seconds_since(s->t0);
+        s->tick_n[buf] = (int)active_cur.size();
       }
     }
     if (rc) { fail_thread(s, rc); return; }
@@ -736,6 +752,7 @@ void gn_loop(kds_server* s) {
       cudaError_t e = cudaEventSynchronize(s->ev_tick[pb]);
       if (e != cudaSuccess) { fail_thread(s, cuda_status(e, "served tick", __FILE__, __LINE__)); return; }
       std::lock_guard<std::mutex> g(s->mu);
+      s->trace.push_back({1.0, (double)s->tick_n[pb], s->tick_t0[pb], seconds_since(s->t0)});
       if (s->P.profile) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, s->ev_lin[pb][0], s->ev_lin[pb][1]) == cudaSuccess) {
@@ -1155,6 +1172,16 @@ int kds_server_wait(kds_server* s, int64_t ticket, double timeout_s, kds_result*
   return KDS_OK;
 }
 
+int kds_server_get_trace(kds_server* s, double* rows4, int32_t cap, int32_t* n) {
+  if (!s || !n || (cap > 0 && !rows4)) return KDS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(s->mu);
+  *n = (int32_t)s->trace.size();
+  const int m = std::min<int>(cap, (int)s->trace.size());
+  for (int i = 0; i < m; ++i)
+    for (int k = 0; k < 4; ++k) rows4[4 * i + k] = s->trace[i][k];
+  return KDS_OK;
+}
+
 int kds_server_get_stats(kds_server* s, kds_server_stats* st) {
   if (!s || !st) return KDS_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> g(s->mu);
@@ -1174,6 +1201,8 @@ int kds_server_get_stats(kds_server* s, kds_server_stats* st) {
   st->alg_bytes = s->alg_bytes;
   st->h2d_bytes = s->h2d_bytes;
   st->d2h_bytes = s->d2h_bytes;
+  st->build_ms = s->build_ms;
+  st->build_points = s->build_points;
   return KDS_OK;
 }
 

@@ -39,7 +39,6 @@ constexpr int kLevelBlocks = 64;
 constexpr int kLevelsPerSync = 4;
 constexpr int kMaxDepth = 64;
 constexpr int kUnroll = 4;  // loads in flight per lane in the warp-per-node phases
-constexpr int kGroup = 128;   // small nodes per block and round
 constexpr int kSmallBlocks = 148 * 8;  // short-lived blocks: other streams' kernels interleave
 
 // ---------------------------------------------------------------------------
@@ -64,6 +63,12 @@ __device__ __forceinline__ void atomic_add_u128(U128* dst, U128 v) {
   unsigned long long old = atomicAdd(&dst->lo, v.lo);
   unsigned long long carry = (old + v.lo < old) ? 1ull : 0ull;
   atomicAdd(&dst->hi, v.hi + carry);
+}
+__host__ __device__ __forceinline__ U128 u128_sub(U128 a, U128 b) {
+  U128 r;
+  r.lo = a.lo - b.lo;
+  r.hi = a.hi - b.hi - (a.lo < b.lo ? 1ull : 0ull);
+  return r;
 }
 __host__ __device__ __forceinline__ double fx_to_d(U128 q) {
   long long hi = (long long)q.hi;
@@ -522,18 +527,71 @@ struct PointBufs {
   int32_t* perm;  // final point order (global indices)
 };
 
-// Small nodes (<= kBig points), block-phased so that the warps of a block run the same
-// code together: each round a block takes up to kGroup consecutive nodes of the level;
-//   A) warp per node: exact moments, reduced across the warp, staged as doubles;
-//   B) thread per node: the leaf/split decision (FP64 eigensolver), 1 node per thread;
-//   C) warp per node: stable partition by whichSide (or leaf placement).
-__global__ void __launch_bounds__(kThreads, 2) k_small(BNode* nodes, const LevelState* ls, PointBufs B,
-                                                    const double* ts0, BuildParams P) {
-  __shared__ double sS[kGroup][12];  // 11 sums as doubles, then n (-1: large node)
-  __shared__ BNode sN[kGroup];
+// Every node's 11 exact moment sums are kept in mom[node].  The roots' sums are
+// computed from their points; a split node hands its children their sums: the left
+// child's from one pass over its points after the partition, the right child's as the
+// parent's minus the left's (exact integer arithmetic).  So below the roots each point
+// is summed once per level only on the left side of its parent.
+
+// Warp-cooperative exact sums of points [b, e) of one point buffer.
+__device__ __forceinline__ void warp_moments(const float4* p, const double* st, int b, int e, double t0, int lane,
+                                             Moments& M) {
+  for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
+  for (int k0 = b; k0 < e; k0 += 32 * kUnroll) {
+    float4 pv[kUnroll];
+    double sv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int i = k0 + u * 32 + lane;
+      if (i < e) { pv[u] = p[i]; sv[u] = st[i]; }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int i = k0 + u * 32 + lane;
+      if (i < e) moments_add_point(M, pv[u], sv[u], t0);
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1)
+    for (int k = 0; k < 11; ++k) M.s[k] = u128_add(M.s[k], shfl_xor_u128(M.s[k], off));
+}
+
+// Level 0: warp per root of at most kBig points.
+__global__ void __launch_bounds__(kThreads) k_root_moments(const BNode* nodes, int R, PointBufs B, const double* ts0,
+                                                           U128* mom) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < R; r += nw) {
+    const int s = nodes[r].start, e = nodes[r].end;
+    if (e - s > kBig) continue;
+    Moments M;
+    warp_moments(B.p[0], B.s[0], s, e, ts0[nodes[r].tree], lane, M);
+    if (lane < 11) {
+      U128 q = M.s[0];
+#pragma unroll
+      for (int k = 1; k < 11; ++k)
+        if (lane == k) q = M.s[k];
+      mom[(size_t)r * 11 + lane] = q;
+    }
+  }
+}
+
+// Thread per node of the level: the leaf/split decision from its sums.
+__global__ void k_decide(BNode* nodes, const LevelState* ls, const U128* mom, BuildParams P) {
+  const int lb = ls->lb, le = ls->le;
+  for (int i = lb + blockIdx.x * blockDim.x + threadIdx.x; i < le; i += gridDim.x * blockDim.x) {
+    BNode nd = nodes[i];
+    double Sd[11];
+    for (int k = 0; k < 11; ++k) Sd[k] = fx_to_d(mom[(size_t)i * 11 + k]);
+    decide(Sd, nd.end - nd.start, nd, P);
+    nodes[i] = nd;
+  }
+}
+
+// Warp per node of at most kBig points, after its children are numbered: stable
+// partition by whichSide (or leaf point order), the children's ranges and sums.
+__global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelState* ls, PointBufs B,
+                                                         const double* ts0, U128* mom) {
   const int lb = ls->lb, le = ls->le, cur = ls->cur;
-  const int L = le - lb;
-  if (L <= 0) return;
   const float4* pin = B.p[cur];
   const double* sin_ = B.s[cur];
   const int32_t* iin = B.id[cur];
@@ -541,125 +599,88 @@ __global__ void __launch_bounds__(kThreads, 2) k_small(BNode* nodes, const Level
   double* sout = B.s[cur ^ 1];
   int32_t* iout = B.id[cur ^ 1];
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nw = blockDim.x >> 5;
-  const int g = min(max((L + (int)gridDim.x - 1) / (int)gridDim.x, 1), kGroup);
-  for (int base = lb + (int)blockIdx.x * g; base < le; base += (int)gridDim.x * g) {
-    const int cnt = min(g, le - base);
-    // A) moments; lane l owns points s + 32*k + l, loads issued kUnroll at a time
-    for (int j = warp; j < cnt; j += nw) {
-      const int s = nodes[base + j].start, e = nodes[base + j].end;
-      const int n = e - s;
-      if (n > kBig) {
-        if (lane == 0) sS[j][11] = -1.0;
-        continue;
-      }
-      const double t0 = ts0[nodes[base + j].tree];
-      Moments M;
-      for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
-      const int K = (n + 31) >> 5;
-      for (int k0 = 0; k0 < K; k0 += kUnroll) {
-        float4 pv[kUnroll];
-        double sv[kUnroll];
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-          int i = s + ((k0 + u) << 5) + lane;
-          if (i < e) { pv[u] = pin[i]; sv[u] = sin_[i]; }
-        }
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-          int i = s + ((k0 + u) << 5) + lane;
-          if (i < e) moments_add_point(M, pv[u], sv[u], t0);
-        }
-      }
-      for (int off = 16; off > 0; off >>= 1)
-        for (int k = 0; k < 11; ++k) M.s[k] = u128_add(M.s[k], shfl_xor_u128(M.s[k], off));
-      if (lane < 11) {
-        U128 q = M.s[0];
-#pragma unroll
-        for (int k = 1; k < 11; ++k)
-          if (lane == k) q = M.s[k];
-        sS[j][lane] = fx_to_d(q);
-      }
-      if (lane == 0) sS[j][11] = (double)n;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int wslot = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // consecutive nodes on different SMs
+  int maxc = 0;
+  for (int ni = lb + wslot; ni < le; ni += nwarps) {
+    const int s = nodes[ni].start, e = nodes[ni].end;
+    if (e - s > kBig) continue;
+    if (!nodes[ni].split) {
+      for (int i = s + lane; i < e; i += 32) B.perm[i] = iin[i];
+      if (lane == 0) nodes[ni].mid = e;
+      continue;
     }
-    __syncthreads();
-    // B) decisions
-    if ((int)threadIdx.x < cnt) {
-      const int j = threadIdx.x;
-      if (sS[j][11] >= 0.0) {
-        BNode nd = nodes[base + j];
-        decide(&sS[j][0], nd.end - nd.start, nd, P);
-        sN[j] = nd;
+    const float mean[3] = {nodes[ni].mean[0], nodes[ni].mean[1], nodes[ni].mean[2]};
+    const float dir[3] = {nodes[ni].dir[0], nodes[ni].dir[1], nodes[ni].dir[2]};
+    const int K = (e - s + 31) >> 5;
+    unsigned bits = 0u;
+    for (int k0 = 0; k0 < K; k0 += kUnroll) {
+      float4 pv[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        int i = s + ((k0 + u) << 5) + lane;
+        if (i < e) pv[u] = pin[i];
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        int i = s + ((k0 + u) << 5) + lane;
+        if (i < e && which_side_f(mean, dir, pv[u])) bits |= 1u << (k0 + u);
       }
     }
-    __syncthreads();
-    // C) partition
-    for (int j = warp; j < cnt; j += nw) {
-      if (sS[j][11] < 0.0) continue;
-      const int s = sN[j].start, e = sN[j].end;
-      const int K = (e - s + 31) >> 5;
-      int mid = e;
-      if (sN[j].split) {
-        const float mean[3] = {sN[j].mean[0], sN[j].mean[1], sN[j].mean[2]};
-        const float dir[3] = {sN[j].dir[0], sN[j].dir[1], sN[j].dir[2]};
-        // side of each owned point as a bit mask, then a stable move with independent loads
-        unsigned bits = 0u;
-        for (int k0 = 0; k0 < K; k0 += kUnroll) {
-          float4 pv[kUnroll];
+    int nl = __popc(bits);
+    for (int off = 16; off > 0; off >>= 1) nl += __shfl_xor_sync(0xffffffffu, nl, off);
+    const unsigned lt = (1u << lane) - 1u;
+    int cl = 0, cr = 0;
+    for (int k0 = 0; k0 < K; k0 += kUnroll) {
+      float4 pv[kUnroll];
+      double sv[kUnroll];
+      int iv[kUnroll];
 #pragma unroll
-          for (int u = 0; u < kUnroll; ++u) {
-            int i = s + ((k0 + u) << 5) + lane;
-            if (i < e) pv[u] = pin[i];
-          }
-#pragma unroll
-          for (int u = 0; u < kUnroll; ++u) {
-            int i = s + ((k0 + u) << 5) + lane;
-            if (i < e && which_side_f(mean, dir, pv[u])) bits |= 1u << (k0 + u);
-          }
-        }
-        int nl = __popc(bits);
-        for (int off = 16; off > 0; off >>= 1) nl += __shfl_xor_sync(0xffffffffu, nl, off);
-        const unsigned lt = (1u << lane) - 1u;
-        int cl = 0, cr = 0;
-        for (int k0 = 0; k0 < K; k0 += kUnroll) {
-          float4 pv[kUnroll];
-          double sv[kUnroll];
-          int iv[kUnroll];
-#pragma unroll
-          for (int u = 0; u < kUnroll; ++u) {
-            int i = s + ((k0 + u) << 5) + lane;
-            if (i < e) { pv[u] = pin[i]; sv[u] = sin_[i]; iv[u] = iin[i]; }
-          }
-#pragma unroll
-          for (int u = 0; u < kUnroll; ++u) {
-            int i = s + ((k0 + u) << 5) + lane;
-            bool valid = i < e;
-            bool left = valid && ((bits >> (k0 + u)) & 1u);
-            unsigned bl = __ballot_sync(0xffffffffu, left);
-            unsigned br = __ballot_sync(0xffffffffu, valid && !left);
-            if (valid) {
-              int dst = left ? (s + cl + __popc(bl & lt)) : (s + nl + cr + __popc(br & lt));
-              pout[dst] = pv[u];
-              sout[dst] = sv[u];
-              iout[dst] = iv[u];
-            }
-            cl += __popc(bl);
-            cr += __popc(br);
-          }
-        }
-        mid = s + nl;
-      } else {
-        for (int i = s + lane; i < e; i += 32) B.perm[i] = iin[i];
+      for (int u = 0; u < kUnroll; ++u) {
+        int i = s + ((k0 + u) << 5) + lane;
+        if (i < e) { pv[u] = pin[i]; sv[u] = sin_[i]; iv[u] = iin[i]; }
       }
-      __syncwarp();
-      if (lane == 0) {
-        sN[j].mid = mid;
-        nodes[base + j] = sN[j];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        int i = s + ((k0 + u) << 5) + lane;
+        bool valid = i < e;
+        bool left = valid && ((bits >> (k0 + u)) & 1u);
+        unsigned bl = __ballot_sync(0xffffffffu, left);
+        unsigned br = __ballot_sync(0xffffffffu, valid && !left);
+        if (valid) {
+          int dst = left ? (s + cl + __popc(bl & lt)) : (s + nl + cr + __popc(br & lt));
+          pout[dst] = pv[u];
+          sout[dst] = sv[u];
+          iout[dst] = iv[u];
+        }
+        cl += __popc(bl);
+        cr += __popc(br);
       }
     }
-    __syncthreads();
+    const int mid = s + nl;
+    __syncwarp();  // the left points written by the warp are read back below
+    Moments ML;
+    warp_moments(pout, sout, s, mid, ts0[nodes[ni].tree], lane, ML);
+    const int li = nodes[ni].left, ri = nodes[ni].right;
+    if (lane < 11) {
+      U128 q = ML.s[0];
+#pragma unroll
+      for (int k = 1; k < 11; ++k)
+        if (lane == k) q = ML.s[k];
+      const U128 m = mom[(size_t)ni * 11 + lane];
+      mom[(size_t)li * 11 + lane] = q;
+      mom[(size_t)ri * 11 + lane] = u128_sub(m, q);
+    }
+    if (lane == 0) {
+      nodes[ni].mid = mid;
+      nodes[li].start = s;
+      nodes[li].end = mid;
+      nodes[ri].start = mid;
+      nodes[ri].end = e;
+      maxc = max(maxc, max(mid - s, e - mid));
+    }
   }
+  if (lane == 0 && maxc > 0) atomicMax(&ls->max_next, maxc);
 }
 
 // ---- large nodes ------------------------------------------------------------------
@@ -696,7 +717,7 @@ __global__ void k_big_sums(const BNode* nodes, const LevelState* ls, int32_t* bb
 }
 
 __global__ void k_big_plan(const BNode* nodes, LevelState* ls, const int32_t* bbig, Chunk* chunks, int32_t chunk_cap,
-                           int32_t* big_list, int32_t* node_chunk0, U128* acc) {
+                           int32_t* big_list, int32_t* node_chunk0, U128* acc, U128* accl) {
   __shared__ int sm[32];
   if (ls->max_size <= kBig) {  // no large node on this level
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -738,7 +759,10 @@ __global__ void k_big_plan(const BNode* nodes, LevelState* ls, const int32_t* bb
           chunks[c].big = ob;
         }
       }
-      for (int k = 0; k < 11; ++k) acc[(size_t)ob * 11 + k] = u128_zero();
+      for (int k = 0; k < 11; ++k) {
+        acc[(size_t)ob * 11 + k] = u128_zero();
+        accl[(size_t)ob * 11 + k] = u128_zero();
+      }
     }
     carry_c += tc;
     carry_b += tb;
@@ -778,17 +802,11 @@ __global__ void __launch_bounds__(kThreads) k_big_moments(const Chunk* chunks, c
   }
 }
 
-__global__ void k_big_decide(BNode* nodes, const LevelState* ls, const int32_t* big_list, const U128* acc,
-                             BuildParams P) {
+// Level 0: the sums of the large roots, from the chunk accumulators.
+__global__ void k_big_to_mom(const LevelState* ls, const int32_t* big_list, const U128* acc, U128* mom) {
   const int nb = ls->num_big;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += gridDim.x * blockDim.x) {
-    int i = big_list[t];
-    BNode nd = nodes[i];
-    double Sd[11];
-    for (int k = 0; k < 11; ++k) Sd[k] = fx_to_d(acc[(size_t)t * 11 + k]);
-    decide(Sd, nd.end - nd.start, nd, P);
-    nodes[i] = nd;
-  }
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb * 11; t += gridDim.x * blockDim.x)
+    mom[(size_t)big_list[t / 11] * 11 + t % 11] = acc[t];
 }
 
 __global__ void k_big_count(const Chunk* chunks, const LevelState* ls, const BNode* nodes, const PointBufs B,
@@ -812,7 +830,7 @@ __global__ void k_big_count(const Chunk* chunks, const LevelState* ls, const BNo
   }
 }
 
-__global__ void k_big_offsets(BNode* nodes, const LevelState* ls, const int32_t* big_list,
+__global__ void k_big_offsets(BNode* nodes, LevelState* ls, const int32_t* big_list,
                               const int32_t* node_chunk0, const int32_t* chunk_nl, int32_t* chunk_loff) {
   const int nb = ls->num_big, nc = ls->num_chunks;
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
@@ -823,6 +841,13 @@ __global__ void k_big_offsets(BNode* nodes, const LevelState* ls, const int32_t*
     for (int c = c0; c < c1; ++c) { chunk_loff[c] = acc; acc += chunk_nl[c]; }
     BNode& nd = nodes[i];
     nd.mid = nd.split ? nd.start + acc : nd.end;
+    if (nd.split) {
+      nodes[nd.left].start = nd.start;
+      nodes[nd.left].end = nd.mid;
+      nodes[nd.right].start = nd.mid;
+      nodes[nd.right].end = nd.end;
+      atomicMax(&ls->max_next, max(nd.mid - nd.start, nd.end - nd.mid));
+    }
   }
 }
 
@@ -877,6 +902,54 @@ __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, c
   }
 }
 
+// Sums of the left children of the level's large split nodes: the part of each chunk
+// that lies in [start, mid) of its node, read from the partitioned buffer.
+__global__ void __launch_bounds__(kThreads) k_big_leftmom(const Chunk* chunks, const LevelState* ls,
+                                                          const PointBufs B, const double* ts0, const BNode* nodes,
+                                                          U128* accl) {
+  __shared__ U128 sm[kThreads / 32][11];
+  const int nc = ls->num_chunks, nxt = ls->cur ^ 1;
+  const float4* pts = B.p[nxt];
+  const double* st = B.s[nxt];
+  for (int ci = blockIdx.x; ci < nc; ci += gridDim.x) {
+    const Chunk c = chunks[ci];
+    const BNode& nd = nodes[c.node];
+    if (!nd.split) continue;  // uniform per block
+    const int e = min(c.end, nd.mid);
+    if (c.begin >= e) continue;
+    const double t0 = ts0[nd.tree];
+    Moments M;
+    for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
+    for (int i = c.begin + threadIdx.x; i < e; i += blockDim.x) moments_add_point(M, pts[i], st[i], t0);
+    for (int off = 16; off > 0; off >>= 1)
+      for (int k = 0; k < 11; ++k) M.s[k] = u128_add(M.s[k], shfl_xor_u128(M.s[k], off));
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+      for (int k = 0; k < 11; ++k) sm[w][k] = M.s[k];
+    __syncthreads();
+    if (threadIdx.x < 11) {
+      U128 t = u128_zero();
+      for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) t = u128_add(t, sm[ww][threadIdx.x]);
+      atomic_add_u128(&accl[(size_t)c.big * 11 + threadIdx.x], t);
+    }
+    __syncthreads();
+  }
+}
+
+// Children's sums of the large split nodes: left from accl, right = parent - left.
+__global__ void k_big_childmom(const BNode* nodes, const LevelState* ls, const int32_t* big_list, const U128* accl,
+                               U128* mom) {
+  const int nb = ls->num_big;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb * 11; t += gridDim.x * blockDim.x) {
+    const int b = t / 11, k = t % 11;
+    const int i = big_list[b];
+    if (!nodes[i].split) continue;
+    const U128 l = accl[t];
+    mom[(size_t)nodes[i].left * 11 + k] = l;
+    mom[(size_t)nodes[i].right * 11 + k] = u128_sub(mom[(size_t)i * 11 + k], l);
+  }
+}
+
 // ---- children ------------------------------------------------------------------------
 
 __global__ void k_level_sums(const BNode* nodes, const LevelState* ls, int32_t* bsum) {
@@ -898,7 +971,6 @@ __global__ void k_level_children(BNode* nodes, LevelState* ls, const int32_t* bs
   int pre = 0;
   for (int k = 0; k < (int)blockIdx.x; ++k) pre += bsum[k];
   int carry = 0;
-  int maxc = 0;  // largest child this thread created
   for (int base = b; base < e; base += blockDim.x) {
     int i = base + threadIdx.x;
     bool sp = (i < e) && nodes[i].split;
@@ -921,9 +993,7 @@ __global__ void k_level_children(BNode* nodes, LevelState* ls, const int32_t* bs
           nd.right = li + 1;
           for (int k = 0; k < 2; ++k) {
             BNode c;
-            memset(&c, 0, sizeof(c));
-            c.start = k == 0 ? nd.start : nd.mid;
-            c.end = k == 0 ? nd.mid : nd.end;
+            memset(&c, 0, sizeof(c));  // start/end: set by the partition
             c.level = nd.level + 1;
             c.tree = nd.tree;
             c.left = c.right = -1;
@@ -931,14 +1001,11 @@ __global__ void k_level_children(BNode* nodes, LevelState* ls, const int32_t* bs
             c.par_has = nd.has_prop;
             for (int j = 0; j < 3; ++j) c.par_prop[j] = nd.prop[j];
             nodes[li + k] = c;
-            maxc = max(maxc, c.end - c.start);
           }
         }
       }
     }
   }
-  for (int off = 16; off > 0; off >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, off));
-  if ((threadIdx.x & 31) == 0 && maxc > 0) atomicMax(&ls->max_next, maxc);
 }
 
 __global__ void k_level_advance(LevelState* ls, const int32_t* bsum, int nblocks, int32_t* level_begin) {
@@ -1107,6 +1174,8 @@ struct BuildWs {
   Chunk* chunks;
   int32_t *chunk_nl, *chunk_loff, *big_list, *node_chunk0;
   U128* acc;
+  U128* accl;  // left-child sums of the level's large nodes
+  U128* mom;   // exact sums of every node (11 per node)
   double* ts0;
   unsigned long long* tsmin;
   int64_t* off;
@@ -1129,7 +1198,7 @@ size_t ws_bytes(int64_t n, int R) {
   return 2 * carve_size<float4>(n) + 2 * carve_size<double>(n) + 3 * carve_size<int32_t>(n) +
          carve_size<BNode>(cn) + 4 * carve_size<int32_t>(cn) + carve_size<int32_t>(ntiles) +
          carve_size<Chunk>(chunk_cap) + 4 * carve_size<int32_t>(chunk_cap) +
-         carve_size<U128>((size_t)11 * (n / kBig + 2)) + 2 * carve_size<double>(R) + carve_size<int64_t>(R + 1) +
+         2 * carve_size<U128>((size_t)11 * (n / kBig + 2)) + carve_size<U128>((size_t)11 * cn) + 2 * carve_size<double>(R) + carve_size<int64_t>(R + 1) +
          carve_size<LevelState>(1) + carve_size<int32_t>(kMaxDepth + 2) + carve_size<int32_t>(kLevelBlocks) +
          carve_size<int32_t>(2 * kLevelBlocks) +
          7 * carve_size<int32_t>(G) + 3 * carve_size<int32_t>(R) + carve_size<int32_t>(8) + carve_size<TreeDev>(R) +
@@ -1170,6 +1239,8 @@ int ws_alloc(BuildWs& w, int64_t n, int R, cudaStream_t s) {
   w.big_list = carve<int32_t>(p, w.chunk_cap);
   w.node_chunk0 = carve<int32_t>(p, w.chunk_cap);
   w.acc = carve<U128>(p, (size_t)11 * (n / kBig + 2));
+  w.accl = carve<U128>(p, (size_t)11 * (n / kBig + 2));
+  w.mom = carve<U128>(p, (size_t)11 * cn);
   w.ts0 = carve<double>(p, R);
   w.tsmin = carve<unsigned long long>(p, R);
   w.off = carve<int64_t>(p, R + 1);
@@ -1271,23 +1342,41 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   const int cb = std::min<int>(w.chunk_cap, kGridBlocks * 2);
   for (int round = 0; round < kMaxDepth; ++round) {
     for (int k = 0; k < kLevelsPerSync; ++k) {
-      k_small<<<kSmallBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.B, w.ts0, P);
-      count_launch();
+      const bool level0 = round == 0 && k == 0;
+      if (level0) {  // the roots' sums
+        k_root_moments<<<kGridBlocks, kThreads, 0, s>>>(w.nodes, R, w.B, w.ts0, w.mom);
+        count_launch();
+        if (host_max > kBig) {
+          k_big_sums<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig);
+          k_big_plan<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig, w.chunks, w.chunk_cap, w.big_list,
+                                                       w.node_chunk0, w.acc, w.accl);
+          k_big_moments<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.B, w.ts0, w.nodes, w.acc);
+          k_big_to_mom<<<64, 256, 0, s>>>(w.ls, w.big_list, w.acc, w.mom);
+          for (int c = 0; c < 4; ++c) count_launch();
+        }
+      }
+      k_decide<<<kGridBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.mom, P);
+      k_level_sums<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum);
+      k_level_children<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum, (int32_t)w.cap_nodes);
+      k_small_part<<<kSmallBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.B, w.ts0, w.mom);
+      for (int c = 0; c < 4; ++c) count_launch();
       if (host_max > kBig) {
-        k_big_sums<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig);
-        k_big_plan<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig, w.chunks, w.chunk_cap, w.big_list,
-                                                     w.node_chunk0, w.acc);
-        k_big_moments<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.B, w.ts0, w.nodes, w.acc);
-        k_big_decide<<<64, 128, 0, s>>>(w.nodes, w.ls, w.big_list, w.acc, P);
+        if (!level0) {
+          k_big_sums<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig);
+          k_big_plan<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig, w.chunks, w.chunk_cap, w.big_list,
+                                                       w.node_chunk0, w.acc, w.accl);
+          count_launch();
+          count_launch();
+        }
         k_big_count<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_nl);
         k_big_offsets<<<64, 128, 0, s>>>(w.nodes, w.ls, w.big_list, w.node_chunk0, w.chunk_nl, w.chunk_loff);
         k_big_scatter<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_loff);
-        for (int c = 0; c < 7; ++c) count_launch();
+        k_big_leftmom<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.B, w.ts0, w.nodes, w.accl);
+        k_big_childmom<<<64, 256, 0, s>>>(w.nodes, w.ls, w.big_list, w.accl, w.mom);
+        for (int c = 0; c < 5; ++c) count_launch();
       }
-      k_level_sums<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum);
-      k_level_children<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum, (int32_t)w.cap_nodes);
       k_level_advance<<<1, 1, 0, s>>>(w.ls, w.bsum, kLevelBlocks, w.level_begin);
-      for (int c = 0; c < 3; ++c) count_launch();
+      count_launch();
     }
     KDS_CK(cudaGetLastError());
     KDS_CK(cudaMemcpyAsync(&hls, w.ls, sizeof(LevelState), cudaMemcpyDeviceToHost, s));

@@ -261,6 +261,15 @@ int kds_batch_create(kds_batch** out);
 /* Runs all jobs; with use_graph != 0 the launches are captured once into a CUDA
  * graph and replayed while the job set keeps its shape. */
 int kds_batch_run(kds_batch* b, kds_job* jobs, int32_t num_jobs, int32_t use_graph, void* stream);
+/* Launch-shape autotuner for a job set (no reference counterpart): times the batched
+ * launches for each candidate configuration -- tree-top nodes staged in shared memory
+ * per block (0, 1023, 2047) x tiles of the larger jobs first or in job order -- keeps
+ * the fastest in the batch handle for the following kds_batch_run calls, and reports
+ * its index (config = stage index + 3 * order) and the mean milliseconds of all six
+ * (ms_out: 6 doubles, may be NULL).  The jobs are read, not modified; results do not
+ * depend on the configuration. */
+int kds_batch_autotune(kds_batch* b, kds_job* jobs, int32_t num_jobs, void* stream, int32_t* chosen,
+                       double* ms_out);
 void kds_batch_free(kds_batch* b);
 
 /* ------------------------------------------------------------------------------

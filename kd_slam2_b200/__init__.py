@@ -406,6 +406,15 @@ class Batch:
             _lib.kds_batch_free(self._h)
             self._h = C.c_void_p(None)
 
+    def autotune(self, jobs, stream=None):
+        """Chooses the launch configuration for this job set; returns (index, ms per config)."""
+        arr = (L.Job * len(jobs))(*jobs)
+        chosen = C.c_int32()
+        ms = np.zeros(6)
+        _check(_lib.kds_batch_autotune(self._h, arr, len(jobs), stream, C.byref(chosen), ms.ctypes.data),
+               "kds_batch_autotune")
+        return chosen.value, ms
+
     def run(self, jobs, use_graph: bool = True, stream=None):
         arr = (L.Job * len(jobs))(*jobs)
         _check(_lib.kds_batch_run(self._h, arr, len(jobs), 1 if use_graph else 0, stream), "kds_batch_run")

@@ -240,6 +240,7 @@ SIGNATURES = {
     "kds_aligner_free": (None, [_P]),
     "kds_batch_create": (C.c_int, [C.POINTER(_P)]),
     "kds_batch_run": (C.c_int, [_P, C.POINTER(Job), _I32, _I32, _P]),
+    "kds_batch_autotune": (C.c_int, [_P, C.POINTER(Job), _I32, _P, C.POINTER(_I32), _P]),
     "kds_batch_free": (None, [_P]),
     "kds_server_params_default": (None, [C.POINTER(ServerParams)]),
     "kds_server_create": (C.c_int, [C.POINTER(ServerParams), C.POINTER(_P)]),

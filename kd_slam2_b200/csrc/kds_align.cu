@@ -939,9 +939,14 @@ int Runner::setup(const std::vector<JobIn>& jobs_in, const std::vector<LinDev>& 
   h_jobs = jobs_in;
   h_lins = lins_in;
   h_tiles.clear();
+  std::vector<int> order(h_jobs.size());
+  for (size_t j = 0; j < order.size(); ++j) order[j] = (int)j;
+  if (order_by_size)
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return h_jobs[a].m_num_leaves > h_jobs[b].m_num_leaves; });
   for (int kind = 0; kind < 3; ++kind) {
     kind_begin[kind] = (int)h_tiles.size();
-    for (size_t j = 0; j < h_jobs.size(); ++j) {
+    for (int j : order) {
       JobIn& Jn = h_jobs[j];
       if (Jn.kind != kind) continue;
       Jn.tile_begin = (int32_t)h_tiles.size();
@@ -1065,6 +1070,7 @@ int Runner::run(cudaStream_t s, bool use_graph, int32_t* dbg_match, int32_t* dbg
   for (int k = 0; k < 3; ++k) { key.push_back(kind_begin[k]); key.push_back(kind_count[k]); }
   key.push_back(profiling ? 1 : 0);
   key.push_back(stage_nodes);
+  key.push_back(order_by_size);
   if (key != graph_key) {
     drop_graph();
     cudaStream_t cs;

@@ -114,6 +114,8 @@ struct Runner {
   std::vector<int64_t> graph_key;
   // number of top fixed-tree nodes each block stages in shared memory (32 B each)
   int stage_nodes = 2047;
+  // tiles of larger jobs first (1) or in job order (0); tuned by kds_batch_autotune
+  int order_by_size = 0;
   bool smem_attr_set = false;
   // optional event pair per linearization launch (measurement only)
   bool profiling = false;

@@ -627,10 +627,9 @@ int kds_batch_create(kds_batch** out) {
   return KDS_OK;
 }
 
-int kds_batch_run(kds_batch* B, kds_job* jobs, int32_t num_jobs, int32_t use_graph, void* stream) {
-  if (!B || (num_jobs > 0 && !jobs) || num_jobs < 0) { set_error("kds_batch_run: bad arguments"); return KDS_ERR_INVALID_ARG; }
-  std::vector<JobIn> J(num_jobs);
-  std::vector<LinDev> lins;
+static int batch_inputs(kds_job* jobs, int32_t num_jobs, std::vector<JobIn>& J, std::vector<LinDev>& lins) {
+  J.assign(num_jobs, JobIn());
+  lins.clear();
   for (int j = 0; j < num_jobs; ++j) {
     kds_job& q = jobs[j];
     if (!q.fixed || !q.moving || (q.type != KDS_ICP && q.type != KDS_CTICP)) {
@@ -661,6 +660,65 @@ int kds_batch_run(kds_batch* B, kds_job* jobs, int32_t num_jobs, int32_t use_gra
     memcpy(L.Xf, q.fixed_X, sizeof(L.Xf));
     memcpy(L.fv, q.fixed_v, sizeof(L.fv));
     lins.push_back(L);
+  }
+  return KDS_OK;
+}
+
+// Candidate launch configurations of the autotuner: (tree-top nodes staged per block,
+// tiles of larger jobs first).
+static const int kTuneStage[3] = {0, 1023, 2047};
+
+int kds_batch_autotune(kds_batch* B, kds_job* jobs, int32_t num_jobs, void* stream, int32_t* chosen,
+                       double* ms_out) {
+  if (!B || num_jobs <= 0 || !jobs) { set_error("kds_batch_autotune: bad arguments"); return KDS_ERR_INVALID_ARG; }
+  std::vector<JobIn> J;
+  std::vector<LinDev> lins;
+  int rc = batch_inputs(jobs, num_jobs, J, lins);
+  if (rc) return rc;
+  cudaStream_t s = as_stream(stream);
+  cudaEvent_t e0, e1;
+  KDS_CK(cudaEventCreate(&e0));
+  KDS_CK(cudaEventCreate(&e1));
+  int best = -1;
+  double best_ms = 1e300;
+  for (int c = 0; c < 6 && rc == KDS_OK; ++c) {
+    B->runner.stage_nodes = kTuneStage[c % 3];
+    B->runner.order_by_size = c / 3;
+    double sum = 0.0;
+    for (int rep = 0; rep < 4 && rc == KDS_OK; ++rep) {  // one warm-up (graph capture), three timed
+      rc = B->runner.setup(J, lins, s);
+      if (rc) break;
+      if (cudaEventRecord(e0, s) != cudaSuccess) { rc = cuda_status(cudaGetLastError(), "autotune", __FILE__, __LINE__); break; }
+      rc = B->runner.run(s, true, nullptr, nullptr);
+      if (rc) break;
+      cudaEventRecord(e1, s);
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) { rc = cuda_status(e, "autotune", __FILE__, __LINE__); break; }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0) sum += ms;
+    }
+    if (rc) break;
+    const double mean = sum / 3.0;
+    if (ms_out) ms_out[c] = mean;
+    if (mean < best_ms) { best_ms = mean; best = c; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  B->runner.stage_nodes = kTuneStage[best % 3];
+  B->runner.order_by_size = best / 3;
+  if (chosen) *chosen = best;
+  return KDS_OK;
+}
+
+int kds_batch_run(kds_batch* B, kds_job* jobs, int32_t num_jobs, int32_t use_graph, void* stream) {
+  if (!B || (num_jobs > 0 && !jobs) || num_jobs < 0) { set_error("kds_batch_run: bad arguments"); return KDS_ERR_INVALID_ARG; }
+  std::vector<JobIn> J;
+  std::vector<LinDev> lins;
+  {
+    int rc0 = batch_inputs(jobs, num_jobs, J, lins);
+    if (rc0) return rc0;
   }
   cudaStream_t s = as_stream(stream);
   int rc = B->runner.setup(J, lins, s);

@@ -108,7 +108,9 @@ def test_first_window_matches_oracle(trace):
 def test_admission_under_a_small_cap(trace):
     served, _, _ = run(trace)
     biggest = max(len(r.xyz) for r in trace.requests)
-    cap = int(biggest * 600)  # room for about two requests with their build workspace
+    # room for about two of the largest requests with their build workspace (about 760 B per
+    # point: point buffers, node arrays and per-node exact sums of the forest build)
+    cap = int(biggest * 1600)
     capped, st, _ = run(trace, hbm_cap=cap)
     assert st["completed"] == len(trace.requests)
     assert st["hbm_cap"] == cap

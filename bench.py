@@ -168,6 +168,17 @@ def cpu_sample(tr, max_seconds: float, threads: int):
     return times
 
 
+def cpu_baseline_leg(tr, served, threads: int) -> dict:
+    """The CPU baseline leg: the reference's CPU path (the oracle port) timed on a bounded
+    sample of the trace, and the served results checked against the same oracle (all-FP64
+    and the product's mixed-precision semantics) on the requests against the initial maps."""
+    ctimes = cpu_sample(tr, 12.0, threads)
+    return {"value": len(ctimes) / float(np.sum(ctimes)), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(ctimes)} requests of the first map window in ~12 s: oracle tree build + "
+                      f"ICP_CPU_/CTICP_CPU_ MODE_REF32 with {threads} chunks, against the streams' initial maps",
+            "served_pose_error_vs_oracle": accuracy_sample(tr, served)}
+
+
 def accuracy_sample(tr, results, count: int = 6):
     """Pose error of served results against the oracle (FP64 and the product's mixed
     semantics) for requests against the initial maps."""
@@ -225,6 +236,74 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def batched_ba(steps: int):
+    """Batched bundle-adjustment pairs: keyframe trees in one forest pass, every pair (rigid
+    and CT-ICP) in one graph-captured launch sequence with autotuned launch shape, against
+    the plain per-pair kds_aligner_compute on a sample of the same pairs."""
+    import torch
+
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import ba
+    wl = ba.make_workload()
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    e0, e1 = ev(), ev()
+    trees = ba.build_trees(wl, TREE)  # warm-up pass
+    for t in trees:
+        if t is not None:
+            t.free()
+    torch.cuda.synchronize()
+    e0.record()
+    trees = ba.build_trees(wl, TREE)
+    e1.record()
+    e1.synchronize()
+    build_ms = e0.elapsed_time(e1)
+    jobs = ba.jobs(wl, trees, ICP, CT)
+    b = kds.Batch()
+    chosen, tune_ms = b.autotune(jobs)
+    res = b.run(jobs)
+    times = []
+    for _ in range(max(1, steps)):
+        torch.cuda.synchronize()
+        e0.record()
+        res = b.run(jobs)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    batch_ms = float(np.mean(times))
+    # plain: one aligner call per pair, on a sample
+    sample = list(range(0, len(jobs), max(1, len(jobs) // 200)))
+    aligners = {0: kds.ICPB2003D(**ICP), 1: kds.CTICPB2003D(**CT)}
+    same = True
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in sample:
+        p = wl.pairs[k]
+        a = aligners[p.kind]
+        a.set_fixed(trees[p.i])
+        a.set_moving(trees[p.j])
+        a.set_x(p.X0)
+        if p.kind == 1:
+            a.set_fixed_velocities(wl.keyframes[p.i].vel)
+            a.set_velocities(wl.keyframes[p.j].vel)
+        r = a.compute()
+        same = same and r == res[k].result and np.array_equal(np.asarray(a.get_x()).reshape(12),
+                                                              np.array(res[k].X[:]))
+    plain_s = (time.perf_counter() - t0) / len(sample)
+    n = [len(k.xyz) for k in wl.keyframes]
+    errs = np.array([pose_err(np.array(res[k].X[:]), wl.pairs[k].X_true) for k in range(len(jobs))])
+    return {
+        "workload": "200 keyframes on a 2 km loop (%d-%d points, log-uniform), %d pairs within 30 m, each "
+                    "aligned rigid (10 it.) and CT-ICP (15 it.) = %d jobs" % (min(n), max(n), len(wl.pairs) // 2,
+                                                                             len(jobs)),
+        "keyframe_points": int(np.sum(n)), "tree_build_ms": build_ms, "batch_ms": batch_ms,
+        "alignments_per_s": len(jobs) / (batch_ms / 1e3), "plain_alignments_per_s": 1.0 / plain_s,
+        "batched_over_plain": (len(jobs) / (batch_ms / 1e3)) * plain_s, "plain_sample": len(sample),
+        "results_identical_to_plain": bool(same), "autotune_config": int(chosen),
+        "autotune_ms": [float(x) for x in tune_ms],
+        "median_t_err_vs_truth_m": float(np.median(errs[:, 0])), "median_r_err_vs_truth_rad": float(np.median(errs[:, 1])),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -233,6 +312,7 @@ def main():
     ap.add_argument("--impl", default="kds", choices=["kds", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain drop-in comparison")
+    ap.add_argument("--no-ba", action="store_true", help="skip the batched bundle-adjustment section")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -390,15 +470,11 @@ def main():
         "roofline": roofline,
         "clocks": clk.summary(),
     }
+    if rank == 0 and not args.no_ba:
+        line["batched_ba"] = batched_ba(args.steps)
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = min(os.cpu_count() or 1, 8)
-        ctimes = cpu_sample(sat, 12.0, threads)
-        line["cpu_baseline"] = {"value": len(ctimes) / float(np.sum(ctimes)), "unit": UNIT, "cores": threads,
-                                "kind": "port",
-                                "sample": f"{len(ctimes)} requests of the first map window in ~12 s: oracle tree "
-                                          f"build + ICP_CPU_/CTICP_CPU_ MODE_REF32 with {threads} chunks, against "
-                                          "the streams' initial maps"}
-        line["accuracy"] = accuracy_sample(sat, served)
+        line["cpu_baseline"] = cpu_baseline_leg(sat, served, threads)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -4,9 +4,9 @@ graph would linearize (MultiViewICPFactor_ / MultiViewCTICPFactor_ call
 buildQuadraticForm once per pair, kd/map/multiview_icp_factor_impl_.h:10-62).
 
 The loop is a stadium-shaped 2 km track: two parallel straights 20 m apart joined by
-half circles.  A keyframe every 10 m (200 keyframes); each is a 128 x 2048 sweep of a
-sensor moving at 10 m/s along the track, cut to a log-uniform size in [20k, 260k]
-points.  Boxes stand along both sides of the track.  A pair is two keyframes closer
+half circles.  A keyframe every 10 m (200 keyframes); each is a 128 x 2048 sweep (a
+deskewed keyframe: the sensor pose is fixed over the sweep, the points keep their
+firing stamps), cut to a log-uniform size in [20k, 260k] points.  Boxes stand along both sides of the track.  A pair is two keyframes closer
 than 30 m; each pair is aligned rigidly (ICP) and with CT-ICP from a perturbed relative
 pose, moving = the later keyframe, fixed = the earlier one.
 """
@@ -22,7 +22,6 @@ from .streams import compose
 SPACING = 10.0
 LANE_GAP = 20.0
 LOOP_LEN = 2000.0
-SPEED = 10.0
 
 
 @dataclass
@@ -94,7 +93,7 @@ def make_workload(seed: int = 4, num_keyframes: int = 200, radius: float = 30.0,
     for k in range(num_keyframes):
         pos, yaw = track_pose(k * SPACING)
         X = synth.pose((pos[0], pos[1], 1.8), (0.0, 0.0, yaw))
-        vel = np.array([SPEED, 0.0, 0.0, 0.0, 0.0, 0.0])
+        vel = np.zeros(6)
         near = boxes[np.hypot((boxes[:, 0] + boxes[:, 3]) / 2 - pos[0], (boxes[:, 1] + boxes[:, 4]) / 2 - pos[1]) < 75]
         xyz, st = synth.scan(near, X, vel, beams=beams, cols=cols, elev=(-22.5, 22.5), seed=seed * 7919 + k,
                              threads=threads)

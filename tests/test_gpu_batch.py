@@ -1,0 +1,69 @@
+"""Batched bundle-adjustment pairs (kds_batch_run) and the launch autotuner.
+
+* Every pair of the batch -- rigid and CT-ICP, uneven sizes, one graph-captured launch
+  sequence -- gives the result of its own kds_aligner_compute, bit for bit.
+* The autotuner's configurations (tree-top staging, job order) change the launch shape
+  only: results are identical under the chosen one and under every other one.
+"""
+import numpy as np
+import pytest
+
+import kd_slam2_b200 as kds
+
+pytestmark = pytest.mark.gpu
+
+TREE = dict(leaf_max_points=16)
+ICP = dict(max_error=0.5, max_iterations=10)
+CT = dict(max_error=0.5, max_iterations=15, velocity_damping=10.0)
+
+
+@pytest.fixture(scope="module")
+def workload():
+    from kd_slam2_b200 import ba
+    wl = ba.make_workload(seed=9, num_keyframes=10, min_pts=8000, max_pts=40000, beams=64, cols=1024)
+    trees = ba.build_trees(wl, TREE)
+    assert all(t is not None for t in trees)
+    return wl, trees
+
+
+def outputs(arr):
+    return [(int(j.result), np.array(j.X[:]), np.array(j.v[:]), j.stats.num_inliers) for j in arr]
+
+
+def same(a, b):
+    for (ra, Xa, va, na), (rb, Xb, vb, nb) in zip(a, b):
+        assert ra == rb and na == nb
+        assert np.array_equal(Xa, Xb)
+        assert np.array_equal(va, vb)
+
+
+def test_batch_equals_per_pair_compute(workload):
+    from kd_slam2_b200 import ba
+    wl, trees = workload
+    jobs = ba.jobs(wl, trees, ICP, CT)
+    assert len(jobs) >= 8 and {p.kind for p in wl.pairs} == {0, 1}
+    res = outputs(kds.Batch().run(jobs, use_graph=True))
+    for p, (r, X, v, n) in zip(wl.pairs, res):
+        a = kds.CTICPB2003D(**CT) if p.kind == 1 else kds.ICPB2003D(**ICP)
+        a.set_fixed(trees[p.i])
+        a.set_moving(trees[p.j])
+        a.set_x(p.X0)
+        if p.kind == 1:
+            a.set_fixed_velocities(wl.keyframes[p.i].vel)
+            a.set_velocities(wl.keyframes[p.j].vel)
+        assert a.compute() == r
+        assert np.array_equal(np.asarray(a.get_x()).reshape(12), X)
+        if p.kind == 1:
+            assert np.array_equal(a.velocities(), v)
+
+
+def test_autotune_keeps_results(workload):
+    from kd_slam2_b200 import ba
+    wl, trees = workload
+    jobs = ba.jobs(wl, trees, ICP, CT)
+    ref = outputs(kds.Batch().run(jobs))
+    b = kds.Batch()
+    chosen, ms = b.autotune(jobs)
+    assert 0 <= chosen < 6 and np.all(ms > 0)
+    same(ref, outputs(b.run(jobs)))
+    same(ref, outputs(b.run(jobs)))  # graph replay

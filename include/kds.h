@@ -292,6 +292,7 @@ typedef struct {
   int32_t profile;          /* 1: time the linearization launches of every tick and count the
                                fixed nodes each registration touches (0; adds work) */
   int32_t max_tiles;        /* tile arena per aligner kind, 128 moving surfels per tile (32768) */
+  int32_t iters_per_tick;   /* Gauss-Newton iterations queued per tick (3) */
   int64_t hbm_cap;          /* admission cap in bytes; 0: 90% of the free memory at create */
   int64_t max_build_points; /* points per build pass (16 Mi) */
   kds_tree_params tree;     /* scans and maps */

@@ -126,6 +126,7 @@ class ServerParams(C.Structure):
         ("serial", C.c_int32),
         ("profile", C.c_int32),
         ("max_tiles", C.c_int32),
+        ("iters_per_tick", C.c_int32),
         ("hbm_cap", C.c_int64),
         ("max_build_points", C.c_int64),
         ("tree", TreeParams),

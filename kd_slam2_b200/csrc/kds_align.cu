@@ -1167,15 +1167,15 @@ int launch_admit_slots(const int32_t* d_slots, int n, const JobIn* new_jobs, con
 int launch_linearize(int kind, int ntiles, const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins,
                      const TileDev* tiles, double* partials, cudaStream_t s) {
   if (ntiles <= 0) return KDS_OK;
-  const size_t stage_bytes = (size_t)kStageNodes * sizeof(DNode);
+  const size_t stage_bytes = (size_t)kServeStage * sizeof(DNode);
   if (kind == 0)
-    k_linearize<0><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kStageNodes,
+    k_linearize<0><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kServeStage,
                                                        partials, nullptr, nullptr);
   else if (kind == 1)
-    k_linearize<1><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kStageNodes,
+    k_linearize<1><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kServeStage,
                                                        partials, nullptr, nullptr);
   else
-    k_linearize<2><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kStageNodes,
+    k_linearize<2><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kServeStage,
                                                        partials, nullptr, nullptr);
   count_launch();
   KDS_CK(cudaGetLastError());

@@ -148,7 +148,8 @@ struct SlotResult {
   double v[6];
   unsigned long long touched;  // distinct fixed nodes the descents visit at the initial state (profiling)
 };
-constexpr int kStageNodes = 2047;
+constexpr int kStageNodes = 2047;  // most fixed-tree nodes any launch stages in shared memory
+constexpr int kServeStage = 1023;  // nodes the served loop stages (a smaller stage leaves room for more blocks)
 constexpr int kTileSurfels = 128;  // moving surfels per tile = threads per k_linearize block  // fixed-tree nodes each block stages in shared memory
 // Copies n admitted job records into their slots and initialises those jobs.
 int launch_admit_slots(const int32_t* d_slots, int n, const JobIn* new_jobs, const LinDev* new_lins, JobIn* jobs,

@@ -214,8 +214,9 @@ struct kds_server {
   std::chrono::steady_clock::time_point t0;
   bool started = false, stopping = false;
   int device = 0;
-  cudaStream_t sA = nullptr, sB = nullptr;  // Gauss-Newton (high priority), build
-  std::thread th_build, th_gn;
+  // Gauss-Newton (highest priority), map rebuilds (middle), request trees (lowest)
+  cudaStream_t sA = nullptr, sB = nullptr, sM = nullptr;
+  std::thread th_build, th_map, th_gn;
   int thread_error = KDS_OK;
   char thread_error_text[256] = {0};
 
@@ -349,7 +350,10 @@ int finish_request(kds_server* s, Request* r, cudaStream_t stream, const float* 
 
 // ---------------------------------------------------------------------------
 // Build thread (served mode)
-void build_loop(kds_server* s) {
+// role 0: request trees on stream sB; role 1: map rebuilds on stream sM.  The two run
+// concurrently, so a completed window's map rebuild never waits behind request trees.
+void build_loop(kds_server* s, int role) {
+  const cudaStream_t bst = role == 1 ? s->sM : s->sB;
   cudaSetDevice(s->device);
   std::vector<Request*> batch;
   std::vector<MapTask> maps;
@@ -362,8 +366,8 @@ void build_loop(kds_server* s) {
       for (;;) {
         if (s->stopping) return;
         const double now = seconds_since(s->t0);
-        // map rebuilds first: they unblock whole windows; they are not held under the cap
-        while (!s->map_tasks.empty() && (int)maps.size() < s->P.max_build_trees) {
+        // map rebuilds (role 1) are not held under the cap
+        while (role == 1 && !s->map_tasks.empty() && (int)maps.size() < s->P.max_build_trees) {
           maps.push_back(s->map_tasks.front());
           s->map_tasks.pop_front();
         }
@@ -371,7 +375,7 @@ void build_loop(kds_server* s) {
         for (auto& m : maps) pts += m.points;
         int64_t rpts = 0;  // request points of the pass
         double next_arrival = -1.0;
-        while (!s->pending.empty() && (int)(batch.size() + maps.size()) < s->P.max_build_trees) {
+        while (role == 0 && !s->pending.empty() && (int)(batch.size() + maps.size()) < s->P.max_build_trees) {
           Request* r = s->pending.front();
           if (r->in.arrival > now) {
             next_arrival = r->in.arrival;
@@ -431,7 +435,7 @@ void build_loop(kds_server* s) {
     B->bytes = 12 * N + 8 * N + 512;
     int rc = KDS_OK;
     if (N > 0) {
-      cudaError_t e = cudaMallocAsync(&B->block, (size_t)B->bytes, s->sB);
+      cudaError_t e = cudaMallocAsync(&B->block, (size_t)B->bytes, bst);
       if (e != cudaSuccess) {
         cudaGetLastError();
         set_error("served build: cudaMallocAsync of %lld bytes failed", (long long)B->bytes);
@@ -446,33 +450,33 @@ void build_loop(kds_server* s) {
     for (int i = 0; rc == KDS_OK && i < (int)maps.size(); ++i) {
       const MapTask& m = maps[i];
       const float* win = s->streams[m.stream].win[(m.version - 1) % 2];
-      cudaError_t e = cudaStreamWaitEvent(s->sB, m.ready, 0);
+      cudaError_t e = cudaStreamWaitEvent(bst, m.ready, 0);
       int64_t o = off[i];
       for (size_t g = 0; e == cudaSuccess && g < m.ranges.size(); ++g) {
         e = cudaMemcpyAsync(bx + 3 * o, win + 3 * m.ranges[g].first, 12 * m.ranges[g].second,
-                            cudaMemcpyDeviceToDevice, s->sB);
+                            cudaMemcpyDeviceToDevice, bst);
         o += m.ranges[g].second;
       }
-      if (e == cudaSuccess && m.points > 0) e = cudaMemsetAsync(bs + off[i], 0, 8 * m.points, s->sB);
+      if (e == cudaSuccess && m.points > 0) e = cudaMemsetAsync(bs + off[i], 0, 8 * m.points, bst);
       if (e != cudaSuccess) rc = cuda_status(e, "served build: map copy", __FILE__, __LINE__);
     }
     int64_t h2d = 0;
     for (int i = 0; rc == KDS_OK && i < (int)batch.size(); ++i) {
       Request* r = batch[i];
       const int64_t o = off[maps.size() + i];
-      cudaError_t e = cudaMemcpyAsync(bx + 3 * o, r->in.xyz, 12 * r->in.n, cudaMemcpyDefault, s->sB);
+      cudaError_t e = cudaMemcpyAsync(bx + 3 * o, r->in.xyz, 12 * r->in.n, cudaMemcpyDefault, bst);
       if (e == cudaSuccess)
-        e = r->in.stamps ? cudaMemcpyAsync(bs + o, r->in.stamps, 8 * r->in.n, cudaMemcpyDefault, s->sB)
-                         : cudaMemsetAsync(bs + o, 0, 8 * r->in.n, s->sB);
+        e = r->in.stamps ? cudaMemcpyAsync(bs + o, r->in.stamps, 8 * r->in.n, cudaMemcpyDefault, bst)
+                         : cudaMemsetAsync(bs + o, 0, 8 * r->in.n, bst);
       if (e != cudaSuccess) rc = cuda_status(e, "served build: point copy", __FILE__, __LINE__);
       if (r->host_input) h2d += (r->in.stamps ? 20 : 12) * r->in.n;
     }
     std::vector<kds_tree*> trees(R, nullptr);
     std::vector<int32_t> status(R, KDS_ERR_TREE_REJECTED);
     if (rc == KDS_OK && N > 0)
-      rc = tree_build_forest(bx, bs, off.data(), R, KDS_MEM_DEVICE, &s->P.tree, s->sB, trees.data(), status.data());
+      rc = tree_build_forest(bx, bs, off.data(), R, KDS_MEM_DEVICE, &s->P.tree, bst, trees.data(), status.data());
     if (rc == KDS_OK) {
-      cudaError_t e = cudaStreamSynchronize(s->sB);
+      cudaError_t e = cudaStreamSynchronize(bst);
       if (e != cudaSuccess) rc = cuda_status(e, "served build", __FILE__, __LINE__);
     }
     if (rc != KDS_OK) {
@@ -525,7 +529,7 @@ void build_loop(kds_server* s) {
         s->ready.push_back(r);
       }
       if (B->refs == 0 && B->block) {
-        cudaFreeAsync(B->block, s->sB);
+        cudaFreeAsync(B->block, bst);
         B->block = nullptr;
       }
       s->cv_gn.notify_all();
@@ -722,10 +726,13 @@ void gn_loop(kds_server* s) {
       }
       if (!rc && !active_cur.empty()) {
         if (s->P.profile) cudaEventRecord(s->ev_lin[buf][0], A);
-        rc = launch_linearize(0, hw0, s->d_jobs, s->d_states, s->d_outs, s->d_lins, s->d_tiles[0], s->d_partials[0], A);
-        if (!rc)
-          rc = launch_linearize(1, hw1, s->d_jobs, s->d_states, s->d_outs, s->d_lins, s->d_tiles[1],
-                                s->d_partials[1], A);
+        for (int it = 0; it < s->P.iters_per_tick && !rc; ++it) {
+          rc = launch_linearize(0, hw0, s->d_jobs, s->d_states, s->d_outs, s->d_lins, s->d_tiles[0],
+                                s->d_partials[0], A);
+          if (!rc)
+            rc = launch_linearize(1, hw1, s->d_jobs, s->d_states, s->d_outs, s->d_lins, s->d_tiles[1],
+                                  s->d_partials[1], A);
+        }
         if (s->P.profile) cudaEventRecord(s->ev_lin[buf][1], A);
         int nslots = 0;
         for (Request* r : active_cur) nslots = std::max(nslots, r->slot + 1);
@@ -951,6 +958,7 @@ void kds_server_params_default(kds_server_params* p) {
   p->hbm_cap = 0;
   p->max_build_points = 16 << 20;
   p->max_tiles = 32768;
+  p->iters_per_tick = 3;
   kds_tree_params_default(&p->tree);
   kds_aligner_params_default(&p->icp);
   kds_aligner_params_default(&p->ct);
@@ -958,7 +966,7 @@ void kds_server_params_default(kds_server_params* p) {
 
 int kds_server_create(const kds_server_params* params, kds_server** out) {
   if (!params || !out || params->max_slots <= 0 || params->map_every <= 0 || params->max_build_trees <= 0 ||
-      params->max_tiles <= 0) {
+      params->max_tiles <= 0 || params->iters_per_tick <= 0) {
     set_error("kds_server_create: bad parameters");
     return KDS_ERR_INVALID_ARG;
   }
@@ -972,6 +980,7 @@ int kds_server_create(const kds_server_params* params, kds_server** out) {
   KDS_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
   KDS_CK(cudaStreamCreateWithPriority(&s->sA, cudaStreamNonBlocking, hi));
   KDS_CK(cudaStreamCreateWithPriority(&s->sB, cudaStreamNonBlocking, lo));
+  KDS_CK(cudaStreamCreateWithPriority(&s->sM, cudaStreamNonBlocking, (lo + hi) / 2));
   size_t fr = 0, tot = 0;
   KDS_CK(cudaMemGetInfo(&fr, &tot));
   const int64_t avail = (int64_t)(fr * 0.9);
@@ -1130,7 +1139,8 @@ int kds_server_start(kds_server* s) {
   if (s->P.serial) {
     s->th_build = std::thread(serial_loop, s);
   } else {
-    s->th_build = std::thread(build_loop, s);
+    s->th_build = std::thread(build_loop, s, 0);
+    s->th_map = std::thread(build_loop, s, 1);
     s->th_gn = std::thread(gn_loop, s);
   }
   return KDS_OK;
@@ -1216,9 +1226,11 @@ void kds_server_free(kds_server* s) {
     s->cv_done.notify_all();
   }
   if (s->th_build.joinable()) s->th_build.join();
+  if (s->th_map.joinable()) s->th_map.join();
   if (s->th_gn.joinable()) s->th_gn.join();
   cudaStreamSynchronize(s->sA);
   cudaStreamSynchronize(s->sB);
+  cudaStreamSynchronize(s->sM);
   for (auto& r : s->reqs) {
     if (r->tree) kds_tree_free(r->tree);
     if (r->batch && r->batch->block) {
@@ -1253,6 +1265,7 @@ void kds_server_free(kds_server* s) {
   }
   cudaStreamDestroy(s->sA);
   cudaStreamDestroy(s->sB);
+  cudaStreamDestroy(s->sM);
   cudaGetLastError();
   delete s;
 }

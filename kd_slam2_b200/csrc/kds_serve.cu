@@ -214,9 +214,8 @@ struct kds_server {
   std::chrono::steady_clock::time_point t0;
   bool started = false, stopping = false;
   int device = 0;
-  // Gauss-Newton (highest priority), map rebuilds (middle), request trees (lowest)
-  cudaStream_t sA = nullptr, sB = nullptr, sM = nullptr;
-  std::thread th_build, th_map, th_gn;
+  cudaStream_t sA = nullptr, sB = nullptr;  // Gauss-Newton (high priority), builds
+  std::thread th_build, th_gn;
   int thread_error = KDS_OK;
   char thread_error_text[256] = {0};
 
@@ -350,10 +349,11 @@ int finish_request(kds_server* s, Request* r, cudaStream_t stream, const float* 
 
 // ---------------------------------------------------------------------------
 // Build thread (served mode)
-// role 0: request trees on stream sB; role 1: map rebuilds on stream sM.  The two run
-// concurrently, so a completed window's map rebuild never waits behind request trees.
-void build_loop(kds_server* s, int role) {
-  const cudaStream_t bst = role == 1 ? s->sM : s->sB;
+// One build thread: each pass takes the pending map rebuilds first (they unblock whole
+// windows), then admits arrived requests.  (Two build passes running concurrently on
+// separate streams each take the whole GPU and slowed each other down.)
+void build_loop(kds_server* s) {
+  const cudaStream_t bst = s->sB;
   cudaSetDevice(s->device);
   std::vector<Request*> batch;
   std::vector<MapTask> maps;
@@ -366,8 +366,8 @@ void build_loop(kds_server* s, int role) {
       for (;;) {
         if (s->stopping) return;
         const double now = seconds_since(s->t0);
-        // map rebuilds (role 1) are not held under the cap
-        while (role == 1 && !s->map_tasks.empty() && (int)maps.size() < s->P.max_build_trees) {
+        // map rebuilds first; they are not held under the cap
+        while (!s->map_tasks.empty() && (int)maps.size() < s->P.max_build_trees) {
           maps.push_back(s->map_tasks.front());
           s->map_tasks.pop_front();
         }
@@ -375,7 +375,7 @@ void build_loop(kds_server* s, int role) {
         for (auto& m : maps) pts += m.points;
         int64_t rpts = 0;  // request points of the pass
         double next_arrival = -1.0;
-        while (role == 0 && !s->pending.empty() && (int)(batch.size() + maps.size()) < s->P.max_build_trees) {
+        while (!s->pending.empty() && (int)(batch.size() + maps.size()) < s->P.max_build_trees) {
           Request* r = s->pending.front();
           if (r->in.arrival > now) {
             next_arrival = r->in.arrival;
@@ -980,7 +980,6 @@ int kds_server_create(const kds_server_params* params, kds_server** out) {
   KDS_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
   KDS_CK(cudaStreamCreateWithPriority(&s->sA, cudaStreamNonBlocking, hi));
   KDS_CK(cudaStreamCreateWithPriority(&s->sB, cudaStreamNonBlocking, lo));
-  KDS_CK(cudaStreamCreateWithPriority(&s->sM, cudaStreamNonBlocking, (lo + hi) / 2));
   size_t fr = 0, tot = 0;
   KDS_CK(cudaMemGetInfo(&fr, &tot));
   const int64_t avail = (int64_t)(fr * 0.9);
@@ -1139,8 +1138,7 @@ int kds_server_start(kds_server* s) {
   if (s->P.serial) {
     s->th_build = std::thread(serial_loop, s);
   } else {
-    s->th_build = std::thread(build_loop, s, 0);
-    s->th_map = std::thread(build_loop, s, 1);
+    s->th_build = std::thread(build_loop, s);
     s->th_gn = std::thread(gn_loop, s);
   }
   return KDS_OK;
@@ -1226,11 +1224,9 @@ void kds_server_free(kds_server* s) {
     s->cv_done.notify_all();
   }
   if (s->th_build.joinable()) s->th_build.join();
-  if (s->th_map.joinable()) s->th_map.join();
   if (s->th_gn.joinable()) s->th_gn.join();
   cudaStreamSynchronize(s->sA);
   cudaStreamSynchronize(s->sB);
-  cudaStreamSynchronize(s->sM);
   for (auto& r : s->reqs) {
     if (r->tree) kds_tree_free(r->tree);
     if (r->batch && r->batch->block) {
@@ -1265,7 +1261,6 @@ void kds_server_free(kds_server* s) {
   }
   cudaStreamDestroy(s->sA);
   cudaStreamDestroy(s->sB);
-  cudaStreamDestroy(s->sM);
   cudaGetLastError();
   delete s;
 }

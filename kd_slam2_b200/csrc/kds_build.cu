@@ -35,7 +35,7 @@ constexpr int kBig = 1024;
 constexpr int kChunk = 1024;
 constexpr int kThreads = 256;
 constexpr int kGridBlocks = 148 * 4;
-constexpr int kLevelBlocks = 64;
+constexpr int kLevelBlocks = 296;
 constexpr int kLevelsPerSync = 4;
 constexpr int kMaxDepth = 64;
 constexpr int kUnroll = 4;  // loads in flight per lane in the warp-per-node phases
@@ -536,17 +536,18 @@ struct PointBufs {
 // Warp-cooperative exact sums of points [b, e) of one point buffer.
 __device__ __forceinline__ void warp_moments(const float4* p, const double* st, int b, int e, double t0, int lane,
                                              Moments& M) {
+  constexpr int U = 2;  // loads in flight per lane (the 11 sums already hold 44 registers)
   for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
-  for (int k0 = b; k0 < e; k0 += 32 * kUnroll) {
-    float4 pv[kUnroll];
-    double sv[kUnroll];
+  for (int k0 = b; k0 < e; k0 += 32 * U) {
+    float4 pv[U];
+    double sv[U];
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int i = k0 + u * 32 + lane;
       if (i < e) { pv[u] = p[i]; sv[u] = st[i]; }
     }
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int i = k0 + u * 32 + lane;
       if (i < e) moments_add_point(M, pv[u], sv[u], t0);
     }

@@ -528,10 +528,10 @@ struct PointBufs {
 };
 
 // Every node's 11 exact moment sums are kept in mom[node].  The roots' sums are
-// computed from their points; a split node hands its children their sums: the left
-// child's from one pass over its points after the partition, the right child's as the
-// parent's minus the left's (exact integer arithmetic).  So below the roots each point
-// is summed once per level only on the left side of its parent.
+// computed from their points; a split node hands its children their sums: the smaller
+// child's from one pass over its points after the partition, the other's as the
+// parent's minus the smaller's (exact integer arithmetic).  So below the roots each point
+// is summed once per level only when it lands in the smaller child of its parent.
 
 // Warp-cooperative exact sums of points [b, e) of one point buffer.
 __device__ __forceinline__ void warp_moments(const float4* p, const double* st, int b, int e, double t0, int lane,
@@ -659,18 +659,20 @@ __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelS
       }
     }
     const int mid = s + nl;
-    __syncwarp();  // the left points written by the warp are read back below
-    Moments ML;
-    warp_moments(pout, sout, s, mid, ts0[nodes[ni].tree], lane, ML);
+    __syncwarp();  // the points written by the warp are read back below
+    // sum the smaller child from its points; the other is the parent minus it
+    const bool small_left = mid - s <= e - mid;
+    Moments MS;
+    warp_moments(pout, sout, small_left ? s : mid, small_left ? mid : e, ts0[nodes[ni].tree], lane, MS);
     const int li = nodes[ni].left, ri = nodes[ni].right;
     if (lane < 11) {
-      U128 q = ML.s[0];
+      U128 q = MS.s[0];
 #pragma unroll
       for (int k = 1; k < 11; ++k)
-        if (lane == k) q = ML.s[k];
-      const U128 m = mom[(size_t)ni * 11 + lane];
-      mom[(size_t)li * 11 + lane] = q;
-      mom[(size_t)ri * 11 + lane] = u128_sub(m, q);
+        if (lane == k) q = MS.s[k];
+      const U128 other = u128_sub(mom[(size_t)ni * 11 + lane], q);
+      mom[(size_t)li * 11 + lane] = small_left ? q : other;
+      mom[(size_t)ri * 11 + lane] = small_left ? other : q;
     }
     if (lane == 0) {
       nodes[ni].mid = mid;
@@ -903,8 +905,8 @@ __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, c
   }
 }
 
-// Sums of the left children of the level's large split nodes: the part of each chunk
-// that lies in [start, mid) of its node, read from the partitioned buffer.
+// Sums of the smaller child of each of the level's large split nodes: the part of each
+// chunk that lies in that child's range of the partitioned buffer.
 __global__ void __launch_bounds__(kThreads) k_big_leftmom(const Chunk* chunks, const LevelState* ls,
                                                           const PointBufs B, const double* ts0, const BNode* nodes,
                                                           U128* accl) {
@@ -916,12 +918,15 @@ __global__ void __launch_bounds__(kThreads) k_big_leftmom(const Chunk* chunks, c
     const Chunk c = chunks[ci];
     const BNode& nd = nodes[c.node];
     if (!nd.split) continue;  // uniform per block
-    const int e = min(c.end, nd.mid);
-    if (c.begin >= e) continue;
+    // the smaller child's range of the partitioned buffer
+    const bool small_left = nd.mid - nd.start <= nd.end - nd.mid;
+    const int b = max(c.begin, small_left ? nd.start : nd.mid);
+    const int e = min(c.end, small_left ? nd.mid : nd.end);
+    if (b >= e) continue;
     const double t0 = ts0[nd.tree];
     Moments M;
     for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
-    for (int i = c.begin + threadIdx.x; i < e; i += blockDim.x) moments_add_point(M, pts[i], st[i], t0);
+    for (int i = b + threadIdx.x; i < e; i += blockDim.x) moments_add_point(M, pts[i], st[i], t0);
     for (int off = 16; off > 0; off >>= 1)
       for (int k = 0; k < 11; ++k) M.s[k] = u128_add(M.s[k], shfl_xor_u128(M.s[k], off));
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -937,7 +942,7 @@ __global__ void __launch_bounds__(kThreads) k_big_leftmom(const Chunk* chunks, c
   }
 }
 
-// Children's sums of the large split nodes: left from accl, right = parent - left.
+// Children's sums of the large split nodes: the smaller from accl, the other = parent - it.
 __global__ void k_big_childmom(const BNode* nodes, const LevelState* ls, const int32_t* big_list, const U128* accl,
                                U128* mom) {
   const int nb = ls->num_big;
@@ -945,9 +950,11 @@ __global__ void k_big_childmom(const BNode* nodes, const LevelState* ls, const i
     const int b = t / 11, k = t % 11;
     const int i = big_list[b];
     if (!nodes[i].split) continue;
-    const U128 l = accl[t];
-    mom[(size_t)nodes[i].left * 11 + k] = l;
-    mom[(size_t)nodes[i].right * 11 + k] = u128_sub(mom[(size_t)i * 11 + k], l);
+    const U128 q = accl[t];  // the smaller child's sums
+    const U128 other = u128_sub(mom[(size_t)i * 11 + k], q);
+    const bool small_left = nodes[i].mid - nodes[i].start <= nodes[i].end - nodes[i].mid;
+    mom[(size_t)nodes[i].left * 11 + k] = small_left ? q : other;
+    mom[(size_t)nodes[i].right * 11 + k] = small_left ? other : q;
   }
 }
 

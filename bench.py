@@ -418,16 +418,26 @@ def main():
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = pst["alg_bytes"] / (pst["lin_ms"] * 1e-3) / 1e9 if pst["lin_ms"] > 0 else None
-    roofline = {"bound": "hbm", "kernel": "k_linearize<0>/<1> (fused ICP / CT-ICP linearization + GN step), "
-                                          "one launch per kind per tick",
-                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
-                "traffic": None, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                "alg_bytes_per_launch": pst["alg_bytes"] / max(1, 2 * pst["lin_ticks"]),
-                "launch_ms": pst["lin_ms"] / max(1, 2 * pst["lin_ticks"]),
-                "model": "per registration iteration: 32 B x moving surfels + 32 B x distinct fixed nodes "
-                         "touched + (M+7) doubles x 2 per tile partial; summed over the run / summed device "
-                         "time of the linearization launches",
-                "ticks": pst["lin_ticks"], "mean_registrations_per_tick": pst["mean_active"]}
+    # the dominant kernels of the step are the tree-build passes; the linearization launches second
+    build_alg = 48.0 * pst["build_point_levels"]
+    build_ach = build_alg / (pst["build_ms"] * 1e-3) / 1e9 if pst["build_ms"] > 0 else None
+    roofline = {"bound": "hbm", "kernel": "tree-build passes (k_small_part, k_decide, k_big_*, level kernels): "
+                                          "forest builds of request and map trees",
+                "achieved": build_ach, "peak": peak, "unit": "GB/s",
+                "frac": build_ach / peak if build_ach else None, "traffic": None,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "alg_bytes_per_step": build_alg, "build_ms_per_step": pst["build_ms"],
+                "model": "48 B per point per level (a 16 B point record read twice and written once); "
+                         "points x levels summed over the step's build passes / their wall time"}
+    ticks = max(1, pst["lin_ticks"])
+    roofline_lin = {"bound": "hbm", "kernel": "k_linearize<0>/<1> (fused ICP / CT-ICP linearization + GN step)",
+                    "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak if achieved else None, "traffic": None,
+                    "alg_bytes_per_tick": pst["alg_bytes"] / ticks, "lin_ms_per_tick": pst["lin_ms"] / ticks,
+                    "model": "per registration iteration: 32 B x moving surfels + 32 B x distinct fixed nodes "
+                             "touched + (M+7) doubles x 2 per tile partial; summed over the run / summed device "
+                             "time of the linearization launches",
+                    "ticks": pst["lin_ticks"], "mean_registrations_per_tick": pst["mean_active"]}
 
     # ---- latency under Poisson arrivals (10 Hz per stream)
     lat_srv, _, _ = streams.serve(poi, tree=TREE, icp=ICP, ct=CT, map_every=MAP_EVERY, timeout=600.0)
@@ -468,6 +478,7 @@ def main():
                    "build_points": st0["build_points"], "peak_reserved_bytes": st0["peak_reserved"],
                    "hbm_cap_bytes": st0["hbm_cap"]},
         "roofline": roofline,
+        "roofline_linearize": roofline_lin,
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_ba:

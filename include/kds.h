@@ -335,6 +335,7 @@ typedef struct {
   int64_t d2h_bytes;       /* results read back to the host */
   double build_ms;         /* wall time of the tree-build passes (requests and map rebuilds) */
   int64_t build_points;    /* points those passes built */
+  double build_point_levels; /* sum over the passes of points x levels */
 } kds_server_stats;
 
 void kds_server_params_default(kds_server_params* p);

@@ -183,6 +183,7 @@ class ServerStats(C.Structure):
         ("d2h_bytes", C.c_int64),
         ("build_ms", C.c_double),
         ("build_points", C.c_int64),
+        ("build_point_levels", C.c_double),
     ]
 
     def as_dict(self) -> dict:

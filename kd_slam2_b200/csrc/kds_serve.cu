@@ -263,6 +263,7 @@ struct kds_server {
   double tick_t0[2] = {0.0, 0.0};
   int tick_n[2] = {0, 0};
   int64_t build_points = 0;   // points built (requests and maps)
+  double build_point_levels = 0.0;  // sum over passes of points x levels
 };
 
 namespace {
@@ -490,6 +491,12 @@ void build_loop(kds_server* s) {
       ++s->build_passes;
       s->build_ms += 1e3 * seconds_since(pass_t0);
       s->build_points += N;
+      {
+        int depth = 0;  // levels of the pass (the same for every tree it built)
+        for (auto* t : trees)
+          if (t) depth = std::max(depth, (int)t->d.depth);
+        s->build_point_levels += (double)N * depth;
+      }
       {
         const double t1 = seconds_since(s->t0);
         s->trace.push_back({0.0, (double)N, t1 - seconds_since(pass_t0), t1});
@@ -1211,6 +1218,7 @@ int kds_server_get_stats(kds_server* s, kds_server_stats* st) {
   st->d2h_bytes = s->d2h_bytes;
   st->build_ms = s->build_ms;
   st->build_points = s->build_points;
+  st->build_point_levels = s->build_point_levels;
   return KDS_OK;
 }
 

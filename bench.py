@@ -116,6 +116,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks_of(x: float, dist, device: str) -> float:
+    """The largest of the ranks' values (every rank gets it); x itself without a process group."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, units_per_rank: float, max_seconds: float) -> float:
+    """Whole-job throughput of independent replicas: every rank's units over the slowest rank's time."""
+    return world * units_per_rank / max_seconds
+
+
 def make_traces():
     """(saturated trace, Poisson trace): the same scans, guesses and request types."""
     from kd_slam2_b200 import streams
@@ -376,11 +391,7 @@ def main():
         return ms, res, stats
 
     def max_over_ranks(x: float) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(x, dist, "cuda")
 
     # warm-up
     for _ in range(args.warmup):
@@ -397,7 +408,7 @@ def main():
     launches = (kds.lib().kds_launch_count() - launches0) // max(1, args.steps)
     n_req = len(sat.requests)
     total_s = max_over_ranks(float(np.sum(times)) / 1e3)
-    value = world * n_req * args.steps / total_s
+    value = replica_throughput(world, n_req * args.steps, total_s)
     ms_step = float(np.mean(times))
 
     # ---- e2e: page-locked host inputs copied inside the step
@@ -406,7 +417,7 @@ def main():
         ms, served_h, e2e_stats = serve_step(host_inputs)
         e2e_times.append(ms)
     e2e_total = max_over_ranks(float(np.sum(e2e_times)) / 1e3)
-    e2e_value = world * n_req * args.steps / e2e_total
+    e2e_value = replica_throughput(world, n_req * args.steps, e2e_total)
     same_host_dev = all(np.array_equal(a["X"], b["X"]) for a, b in zip(served, served_h))
 
     # ---- profile pass (untimed): device time and algorithmic bytes of the linearizations

@@ -258,8 +258,8 @@ typedef struct {
 
 typedef struct kds_batch kds_batch;
 int kds_batch_create(kds_batch** out);
-/* Runs all jobs; with use_graph != 0 the launches are captured once into a CUDA
- * graph and replayed while the job set keeps its shape. */
+/* Runs all jobs; with use_graph != 0, a job-set shape that runs a second time in a
+ * row is captured into a CUDA graph, which is replayed while the shape stays. */
 int kds_batch_run(kds_batch* b, kds_job* jobs, int32_t num_jobs, int32_t use_graph, void* stream);
 /* Launch-shape autotuner for a job set (no reference counterpart): times the batched
  * launches for each candidate configuration -- tree-top nodes staged in shared memory

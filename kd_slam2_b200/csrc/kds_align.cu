@@ -1072,6 +1072,12 @@ int Runner::run(cudaStream_t s, bool use_graph, int32_t* dbg_match, int32_t* dbg
   key.push_back(stage_nodes);
   key.push_back(order_by_size);
   if (key != graph_key) {
+    // capture only a shape that repeats: a one-off shape (every call of a stream of
+    // different scans) costs less launched directly than captured and instantiated
+    if (key != last_key) {
+      last_key = key;
+      return enqueue(s, nullptr, nullptr);
+    }
     drop_graph();
     cudaStream_t cs;
     KDS_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));

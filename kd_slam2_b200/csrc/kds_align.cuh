@@ -112,6 +112,7 @@ struct Runner {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   std::vector<int64_t> graph_key;
+  std::vector<int64_t> last_key;  // shape of the previous run
   // number of top fixed-tree nodes each block stages in shared memory (32 B each)
   int stage_nodes = 2047;
   // tiles of larger jobs first (1) or in job order (0); tuned by kds_batch_autotune

@@ -685,7 +685,7 @@ int kds_batch_autotune(kds_batch* B, kds_job* jobs, int32_t num_jobs, void* stre
     B->runner.stage_nodes = kTuneStage[c % 3];
     B->runner.order_by_size = c / 3;
     double sum = 0.0;
-    for (int rep = 0; rep < 4 && rc == KDS_OK; ++rep) {  // one warm-up (graph capture), three timed
+    for (int rep = 0; rep < 5 && rc == KDS_OK; ++rep) {  // two warm-ups (direct, graph capture), three timed
       rc = B->runner.setup(J, lins, s);
       if (rc) break;
       if (cudaEventRecord(e0, s) != cudaSuccess) { rc = cuda_status(cudaGetLastError(), "autotune", __FILE__, __LINE__); break; }
@@ -696,7 +696,7 @@ int kds_batch_autotune(kds_batch* B, kds_job* jobs, int32_t num_jobs, void* stre
       if (e != cudaSuccess) { rc = cuda_status(e, "autotune", __FILE__, __LINE__); break; }
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
-      if (rep > 0) sum += ms;
+      if (rep > 1) sum += ms;
     }
     if (rc) break;
     const double mean = sum / 3.0;

@@ -1028,7 +1028,7 @@ int Runner::enqueue(cudaStream_t s, int32_t* dbg_match, int32_t* dbg_status) {
   int ev = 0;
   const int stage = stage_nodes;
   const size_t stage_bytes = (size_t)stage * sizeof(DNode);
-  if (stage_bytes > 48 * 1024 && !smem_attr_set) {
+  if (stage_bytes > 0 && !smem_attr_set) {  // static + dynamic shared memory can pass 48 KB
     for (int k = 0; k < 3; ++k) {
       const void* f = k == 0 ? (const void*)k_linearize<0> : (k == 1 ? (const void*)k_linearize<1> : (const void*)k_linearize<2>);
       KDS_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));

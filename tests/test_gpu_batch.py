@@ -67,3 +67,25 @@ def test_autotune_keeps_results(workload):
     assert 0 <= chosen < 6 and np.all(ms > 0)
     same(ref, outputs(b.run(jobs)))
     same(ref, outputs(b.run(jobs)))  # graph replay
+
+
+def test_autotune_as_first_use_of_the_library(tmp_path):
+    """In a fresh process, the autotuner's staged configurations opt the kernels into their
+    shared memory themselves (no earlier launch did it)."""
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+    code = (
+        "import sys; sys.path.insert(0, %r)\n"
+        "import kd_slam2_b200 as kds\n"
+        "from kd_slam2_b200 import ba\n"
+        "wl = ba.make_workload(seed=3, num_keyframes=4, min_pts=8000, max_pts=20000, beams=64, cols=1024)\n"
+        "trees = ba.build_trees(wl, dict(leaf_max_points=16))\n"
+        "jobs = ba.jobs(wl, trees, dict(max_iterations=5), dict(max_iterations=5))\n"
+        "b = kds.Batch()\n"
+        "c, ms = b.autotune(jobs)\n"
+        "print('chosen', c)\n" % ROOT)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "chosen" in r.stdout

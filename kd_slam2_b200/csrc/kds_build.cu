@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <vector>
 
@@ -35,10 +36,10 @@ constexpr int kBig = 1024;
 constexpr int kChunk = 1024;
 constexpr int kThreads = 256;
 constexpr int kGridBlocks = 148 * 4;
-constexpr int kLevelBlocks = 296;
+constexpr int kLevelBlocks = 148 * 3;  // k_decide: 3 blocks per SM at its register count
 constexpr int kLevelsPerSync = 4;
 constexpr int kMaxDepth = 64;
-constexpr int kUnroll = 4;  // loads in flight per lane in the warp-per-node phases
+constexpr int kUnroll = 2;  // rounds of 32 points in flight per lane in the warp-per-node partition
 constexpr int kSmallBlocks = 148 * 8;  // short-lived blocks: other streams' kernels interleave
 
 // ---------------------------------------------------------------------------
@@ -534,9 +535,29 @@ struct PointBufs {
 // is summed once per level only when it lands in the smaller child of its parent.
 
 // Warp-cooperative exact sums of points [b, e) of one point buffer.
-__device__ __forceinline__ void warp_moments(const float4* p, const double* st, int b, int e, double t0, int lane,
-                                             Moments& M) {
+// Warp total of the 11 sums in reduce-scatter form: the 16 slots (11 used) are halved
+// over lane bits 4..1 (8 + 4 + 2 + 1 exchanges instead of 5 x 11), then added with
+// lane ^ 1.  Lanes 2k and 2k + 1 return the total of sum k (k < 11; slots 11-15 are 0).
+__device__ __forceinline__ U128 warp_sum_moments(const Moments& M, int lane) {
+  U128 v[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = k < 11 ? M.s[k] : u128_zero();
+  U128 w8[8], w4[4], w2[2];
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) w8[j] = u128_add(b4 ? v[8 + j] : v[j], shfl_xor_u128(b4 ? v[j] : v[8 + j], 16));
+#pragma unroll
+  for (int j = 0; j < 4; ++j) w4[j] = u128_add(b3 ? w8[4 + j] : w8[j], shfl_xor_u128(b3 ? w8[j] : w8[4 + j], 8));
+#pragma unroll
+  for (int j = 0; j < 2; ++j) w2[j] = u128_add(b2 ? w4[2 + j] : w4[j], shfl_xor_u128(b2 ? w4[j] : w4[2 + j], 4));
+  U128 w1 = u128_add(b1 ? w2[1] : w2[0], shfl_xor_u128(b1 ? w2[0] : w2[1], 2));
+  return u128_add(w1, shfl_xor_u128(w1, 1));
+}
+
+// Sums of the points [b, e) by one warp; returns warp_sum_moments of them.
+__device__ __forceinline__ U128 warp_moments(const float4* p, const double* st, int b, int e, double t0, int lane) {
   constexpr int U = 2;  // loads in flight per lane (the 11 sums already hold 44 registers)
+  Moments M;
   for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
   for (int k0 = b; k0 < e; k0 += 32 * U) {
     float4 pv[U];
@@ -552,8 +573,7 @@ __device__ __forceinline__ void warp_moments(const float4* p, const double* st, 
       if (i < e) moments_add_point(M, pv[u], sv[u], t0);
     }
   }
-  for (int off = 16; off > 0; off >>= 1)
-    for (int k = 0; k < 11; ++k) M.s[k] = u128_add(M.s[k], shfl_xor_u128(M.s[k], off));
+  return warp_sum_moments(M, lane);
 }
 
 // Level 0: warp per root of at most kBig points.
@@ -564,32 +584,56 @@ __global__ void __launch_bounds__(kThreads) k_root_moments(const BNode* nodes, i
   for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < R; r += nw) {
     const int s = nodes[r].start, e = nodes[r].end;
     if (e - s > kBig) continue;
-    Moments M;
-    warp_moments(B.p[0], B.s[0], s, e, ts0[nodes[r].tree], lane, M);
-    if (lane < 11) {
-      U128 q = M.s[0];
-#pragma unroll
-      for (int k = 1; k < 11; ++k)
-        if (lane == k) q = M.s[k];
-      mom[(size_t)r * 11 + lane] = q;
-    }
+    const U128 q = warp_moments(B.p[0], B.s[0], s, e, ts0[nodes[r].tree], lane);
+    if (!(lane & 1) && lane < 22) mom[(size_t)r * 11 + (lane >> 1)] = q;
   }
 }
 
-// Thread per node of the level: the leaf/split decision from its sums.
-__global__ void k_decide(BNode* nodes, const LevelState* ls, const U128* mom, BuildParams P) {
-  const int lb = ls->lb, le = ls->le;
-  for (int i = lb + blockIdx.x * blockDim.x + threadIdx.x; i < le; i += gridDim.x * blockDim.x) {
+// Thread per node of the level: the leaf/split decision from its sums.  Block b takes
+// the b-th contiguous range of the level's nodes and writes its count of split nodes
+// (the children's numbering scans these counts).
+__global__ void k_decide(BNode* nodes, const LevelState* ls, const U128* mom, BuildParams P, int32_t* bsum,
+                         int32_t* bbig) {
+  __shared__ int sm[32];
+  int b, e;
+  level_range(ls, b, e);
+  int v = 0, nc = 0, nb = 0;
+  for (int i = b + threadIdx.x; i < e; i += blockDim.x) {
     BNode nd = nodes[i];
+    const int n = nd.end - nd.start;
     double Sd[11];
     for (int k = 0; k < 11; ++k) Sd[k] = fx_to_d(mom[(size_t)i * 11 + k]);
-    decide(Sd, nd.end - nd.start, nd, P);
+    decide(Sd, n, nd, P);
     nodes[i] = nd;
+    v += nd.split ? 1 : 0;
+    if (n > kBig) {
+      nc += (n + kChunk - 1) / kChunk;
+      nb += 1;
+    }
+  }
+  int total, tc, tb;
+  block_scan(v, sm, &total);
+  block_scan(nc, sm, &tc);
+  block_scan(nb, sm, &tb);
+  if (threadIdx.x == 0) {
+    bsum[blockIdx.x] = total;
+    bbig[2 * blockIdx.x] = tc;  // as k_big_sums
+    bbig[2 * blockIdx.x + 1] = tb;
   }
 }
+
+// The first 18 words of a BNode (start .. dir): one coalesced load by lanes 0-17.
+constexpr int kNodeHeadWords = 18;
+static_assert(offsetof(BNode, dir) + 3 * sizeof(float) == kNodeHeadWords * 4, "BNode head layout");
+static_assert(offsetof(BNode, start) == 0 && offsetof(BNode, end) == 4 && offsetof(BNode, tree) == 12 &&
+                  offsetof(BNode, split) == 16 && offsetof(BNode, left) == 24 && offsetof(BNode, right) == 28 &&
+                  offsetof(BNode, mean) == 48,
+              "BNode head layout");
 
 // Warp per node of at most kBig points, after its children are numbered: stable
 // partition by whichSide (or leaf point order), the children's ranges and sums.
+// Latency-bound at deep levels (many small nodes per warp), so each node's record
+// and sums are fetched in one round of loads, one node ahead.
 __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelState* ls, PointBufs B,
                                                          const double* ts0, U128* mom) {
   const int lb = ls->lb, le = ls->le, cur = ls->cur;
@@ -602,25 +646,49 @@ __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelS
   const int lane = threadIdx.x & 31;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int wslot = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // consecutive nodes on different SMs
+  const bool sum_lane = !(lane & 1) && lane < 22;                  // holds sum lane / 2
   int maxc = 0;
+  int word = 0;
+  U128 pm = u128_zero();
+  auto fetch = [&](int ni) {
+    if (ni < le) {
+      if (lane < kNodeHeadWords) word = reinterpret_cast<const int*>(nodes + ni)[lane];
+      if (sum_lane) pm = mom[(size_t)ni * 11 + (lane >> 1)];
+    }
+  };
+  fetch(lb + wslot);
   for (int ni = lb + wslot; ni < le; ni += nwarps) {
-    const int s = nodes[ni].start, e = nodes[ni].end;
+    const int s = __shfl_sync(0xffffffffu, word, 0), e = __shfl_sync(0xffffffffu, word, 1);
+    const int tree = __shfl_sync(0xffffffffu, word, 3), split = __shfl_sync(0xffffffffu, word, 4);
+    const int li = __shfl_sync(0xffffffffu, word, 6), ri = __shfl_sync(0xffffffffu, word, 7);
+    float mean[3], dir[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      mean[k] = __int_as_float(__shfl_sync(0xffffffffu, word, 12 + k));
+      dir[k] = __int_as_float(__shfl_sync(0xffffffffu, word, 15 + k));
+    }
+    const U128 psum = pm;
+    fetch(ni + nwarps);  // the next node's record and sums are in flight meanwhile
     if (e - s > kBig) continue;
-    if (!nodes[ni].split) {
+    if (!split) {
       for (int i = s + lane; i < e; i += 32) B.perm[i] = iin[i];
       if (lane == 0) nodes[ni].mid = e;
       continue;
     }
-    const float mean[3] = {nodes[ni].mean[0], nodes[ni].mean[1], nodes[ni].mean[2]};
-    const float dir[3] = {nodes[ni].dir[0], nodes[ni].dir[1], nodes[ni].dir[2]};
     const int K = (e - s + 31) >> 5;
+    const bool one = K <= kUnroll;  // the whole node fits one round of loads: keep it
     unsigned bits = 0u;
+    float4 pv[kUnroll];
+    double sv[kUnroll];
+    int iv[kUnroll];
     for (int k0 = 0; k0 < K; k0 += kUnroll) {
-      float4 pv[kUnroll];
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) {
         int i = s + ((k0 + u) << 5) + lane;
-        if (i < e) pv[u] = pin[i];
+        if (i < e) {
+          pv[u] = pin[i];
+          if (one) { sv[u] = sin_[i]; iv[u] = iin[i]; }
+        }
       }
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) {
@@ -630,16 +698,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelS
     }
     int nl = __popc(bits);
     for (int off = 16; off > 0; off >>= 1) nl += __shfl_xor_sync(0xffffffffu, nl, off);
+    const int mid = s + nl;
+    // the smaller child is summed while its points move; the other is the parent minus it
+    const bool small_left = mid - s <= e - mid;
+    const double t0 = ts0[tree];
+    Moments MS;
+    for (int k = 0; k < 11; ++k) MS.s[k] = u128_zero();
     const unsigned lt = (1u << lane) - 1u;
     int cl = 0, cr = 0;
     for (int k0 = 0; k0 < K; k0 += kUnroll) {
-      float4 pv[kUnroll];
-      double sv[kUnroll];
-      int iv[kUnroll];
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) {
         int i = s + ((k0 + u) << 5) + lane;
-        if (i < e) { pv[u] = pin[i]; sv[u] = sin_[i]; iv[u] = iin[i]; }
+        if (i < e && !one) {
+          pv[u] = pin[i];
+          sv[u] = sin_[i];
+          iv[u] = iin[i];
+        }
       }
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) {
@@ -653,26 +728,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelS
           pout[dst] = pv[u];
           sout[dst] = sv[u];
           iout[dst] = iv[u];
+          if (left == small_left) moments_add_point(MS, pv[u], sv[u], t0);
         }
         cl += __popc(bl);
         cr += __popc(br);
       }
     }
-    const int mid = s + nl;
-    __syncwarp();  // the points written by the warp are read back below
-    // sum the smaller child from its points; the other is the parent minus it
-    const bool small_left = mid - s <= e - mid;
-    Moments MS;
-    warp_moments(pout, sout, small_left ? s : mid, small_left ? mid : e, ts0[nodes[ni].tree], lane, MS);
-    const int li = nodes[ni].left, ri = nodes[ni].right;
-    if (lane < 11) {
-      U128 q = MS.s[0];
-#pragma unroll
-      for (int k = 1; k < 11; ++k)
-        if (lane == k) q = MS.s[k];
-      const U128 other = u128_sub(mom[(size_t)ni * 11 + lane], q);
-      mom[(size_t)li * 11 + lane] = small_left ? q : other;
-      mom[(size_t)ri * 11 + lane] = small_left ? other : q;
+    const U128 q = warp_sum_moments(MS, lane);
+    if (sum_lane) {
+      const int k = lane >> 1;
+      const U128 other = u128_sub(psum, q);
+      mom[(size_t)li * 11 + k] = small_left ? q : other;
+      mom[(size_t)ri * 11 + k] = small_left ? other : q;
     }
     if (lane == 0) {
       nodes[ni].mid = mid;
@@ -731,14 +798,21 @@ __global__ void k_big_plan(const BNode* nodes, LevelState* ls, const int32_t* bb
   }
   int b, e;
   level_range(ls, b, e);
-  int carry_c = 0, carry_b = 0, all_c = 0, all_b = 0;
-  for (int k = 0; k < (int)gridDim.x; ++k) {
-    if (k < (int)blockIdx.x) {
-      carry_c += bbig[2 * k];
-      carry_b += bbig[2 * k + 1];
+  int carry_c, carry_b, all_c, all_b;  // chunks / large nodes of the blocks before this one, of all
+  {
+    int vc = 0, vb = 0, ac = 0, ab = 0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+      if (k < (int)blockIdx.x) {
+        vc += bbig[2 * k];
+        vb += bbig[2 * k + 1];
+      }
+      ac += bbig[2 * k];
+      ab += bbig[2 * k + 1];
     }
-    all_c += bbig[2 * k];
-    all_b += bbig[2 * k + 1];
+    block_scan(vc, sm, &carry_c);
+    block_scan(vb, sm, &carry_b);
+    block_scan(ac, sm, &all_c);
+    block_scan(ab, sm, &all_b);
   }
   for (int base = b; base < e; base += blockDim.x) {
     int i = base + threadIdx.x;
@@ -777,6 +851,20 @@ __global__ void k_big_plan(const BNode* nodes, LevelState* ls, const int32_t* bb
   }
 }
 
+// Block sum of per-thread sums into one 128-bit accumulator set (any order: exact).
+__device__ __forceinline__ void block_add_moments(const Moments& M, U128 (*sm)[11], U128* dst) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const U128 q = warp_sum_moments(M, lane);
+  if (!(lane & 1) && lane < 22) sm[w][lane >> 1] = q;
+  __syncthreads();
+  if (threadIdx.x < 11) {
+    U128 t = u128_zero();
+    for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) t = u128_add(t, sm[ww][threadIdx.x]);
+    atomic_add_u128(&dst[threadIdx.x], t);
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(kThreads) k_big_moments(const Chunk* chunks, const LevelState* ls,
                                                           const PointBufs B, const double* ts0, const BNode* nodes,
                                                           U128* acc) {
@@ -790,18 +878,7 @@ __global__ void __launch_bounds__(kThreads) k_big_moments(const Chunk* chunks, c
     Moments M;
     for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
     for (int i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) moments_add_point(M, pts[i], st[i], t0);
-    for (int off = 16; off > 0; off >>= 1)
-      for (int k = 0; k < 11; ++k) M.s[k] = u128_add(M.s[k], shfl_xor_u128(M.s[k], off));
-    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0)
-      for (int k = 0; k < 11; ++k) sm[w][k] = M.s[k];
-    __syncthreads();
-    if (threadIdx.x < 11) {
-      U128 t = u128_zero();
-      for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) t = u128_add(t, sm[ww][threadIdx.x]);
-      atomic_add_u128(&acc[(size_t)c.big * 11 + threadIdx.x], t);
-    }
-    __syncthreads();
+    block_add_moments(M, sm, acc + (size_t)c.big * 11);
   }
 }
 
@@ -854,11 +931,18 @@ __global__ void k_big_offsets(BNode* nodes, LevelState* ls, const int32_t* big_l
   }
 }
 
-// stable scatter of one chunk: each thread owns a contiguous run of points
+// Stable scatter of one chunk by warp ballots: warp w of the block moves points
+// [begin + 128 w, begin + 128 (w + 1)) in four rounds of 32, so left and right runs are
+// written contiguously.  The points that go to the node's smaller child are summed on
+// the way (the sums of the large node's smaller child).
 __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, const LevelState* ls,
                                                           const BNode* nodes, PointBufs B,
-                                                          const int32_t* chunk_loff) {
-  __shared__ int sc[kThreads];
+                                                          const int32_t* chunk_loff, const double* ts0, U128* accl) {
+  constexpr int kPer = kChunk / kThreads;  // rounds of 32 points per warp
+  constexpr int kWarpsB = kThreads / 32;
+  static_assert(kPer * kThreads == kChunk, "chunk = block x rounds");
+  __shared__ int swl[kWarpsB];
+  __shared__ U128 sm[kWarpsB][11];
   const int nc = ls->num_chunks, cur = ls->cur;
   const float4* pin = B.p[cur];
   const double* sin_ = B.s[cur];
@@ -866,79 +950,62 @@ __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, c
   float4* pout = B.p[cur ^ 1];
   double* sout = B.s[cur ^ 1];
   int32_t* iout = B.id[cur ^ 1];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
   for (int ci = blockIdx.x; ci < nc; ci += gridDim.x) {
-    Chunk c = chunks[ci];
+    const Chunk c = chunks[ci];
     const BNode& nd = nodes[c.node];
-    int len = c.end - c.begin;
     if (!nd.split) {
       for (int i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) B.perm[i] = iin[i];
       continue;  // uniform per block
     }
-    int per = (len + blockDim.x - 1) / blockDim.x;
-    int b0 = c.begin + threadIdx.x * per;
-    int b1 = min(b0 + per, c.end);
-    int mine = 0;
-    for (int i = b0; i < b1; ++i) mine += which_side_f(nd.mean, nd.dir, pin[i]) ? 1 : 0;
-    __syncthreads();
-    sc[threadIdx.x] = mine;
-    __syncthreads();
-    for (int off = 1; off < (int)blockDim.x; off <<= 1) {
-      int v = (threadIdx.x >= (unsigned)off) ? sc[threadIdx.x - off] : 0;
-      __syncthreads();
-      sc[threadIdx.x] += v;
-      __syncthreads();
+    const float mean[3] = {nd.mean[0], nd.mean[1], nd.mean[2]};
+    const float dir[3] = {nd.dir[0], nd.dir[1], nd.dir[2]};
+    const int wb = c.begin + w * 32 * kPer;  // this warp's first point
+    float4 pv[kPer];
+    double sv[kPer];
+    int iv[kPer];
+    unsigned bl[kPer], bv[kPer];
+    int nl = 0;
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int i = wb + u * 32 + lane;
+      if (i < c.end) { pv[u] = pin[i]; sv[u] = sin_[i]; iv[u] = iin[i]; }
     }
-    int lbefore = sc[threadIdx.x] - mine;
-    int loff = chunk_loff[ci] + lbefore;
-    int pbefore = (c.begin - nd.start) + (b0 - c.begin);
-    int roff = pbefore - loff;
-    int nl_total = nd.mid - nd.start;
-    for (int i = b0; i < b1; ++i) {
-      float4 p = pin[i];
-      int dst;
-      if (which_side_f(nd.mean, nd.dir, p)) dst = nd.start + loff++;
-      else dst = nd.start + nl_total + roff++;
-      pout[dst] = p;
-      sout[dst] = sin_[i];
-      iout[dst] = iin[i];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int i = wb + u * 32 + lane;
+      bv[u] = __ballot_sync(0xffffffffu, i < c.end);
+      bl[u] = __ballot_sync(0xffffffffu, i < c.end && which_side_f(mean, dir, pv[u]));
+      nl += __popc(bl[u]);
     }
-  }
-}
-
-// Sums of the smaller child of each of the level's large split nodes: the part of each
-// chunk that lies in that child's range of the partitioned buffer.
-__global__ void __launch_bounds__(kThreads) k_big_leftmom(const Chunk* chunks, const LevelState* ls,
-                                                          const PointBufs B, const double* ts0, const BNode* nodes,
-                                                          U128* accl) {
-  __shared__ U128 sm[kThreads / 32][11];
-  const int nc = ls->num_chunks, nxt = ls->cur ^ 1;
-  const float4* pts = B.p[nxt];
-  const double* st = B.s[nxt];
-  for (int ci = blockIdx.x; ci < nc; ci += gridDim.x) {
-    const Chunk c = chunks[ci];
-    const BNode& nd = nodes[c.node];
-    if (!nd.split) continue;  // uniform per block
-    // the smaller child's range of the partitioned buffer
-    const bool small_left = nd.mid - nd.start <= nd.end - nd.mid;
-    const int b = max(c.begin, small_left ? nd.start : nd.mid);
-    const int e = min(c.end, small_left ? nd.mid : nd.end);
-    if (b >= e) continue;
+    if (lane == 0) swl[w] = nl;
+    __syncthreads();
+    int lpre = 0;  // left points of the chunk's earlier warps
+    for (int k = 0; k < w; ++k) lpre += swl[k];
+    const int nl_total = nd.mid - nd.start;
+    const int before = min(wb, c.end) - nd.start;  // the node's points before this warp's
+    int lo = nd.start + chunk_loff[ci] + lpre;
+    int ro = nd.mid + before - (chunk_loff[ci] + lpre);
+    const bool small_left = nl_total <= nd.end - nd.mid;
     const double t0 = ts0[nd.tree];
     Moments M;
     for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
-    for (int i = b + threadIdx.x; i < e; i += blockDim.x) moments_add_point(M, pts[i], st[i], t0);
-    for (int off = 16; off > 0; off >>= 1)
-      for (int k = 0; k < 11; ++k) M.s[k] = u128_add(M.s[k], shfl_xor_u128(M.s[k], off));
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0)
-      for (int k = 0; k < 11; ++k) sm[w][k] = M.s[k];
-    __syncthreads();
-    if (threadIdx.x < 11) {
-      U128 t = u128_zero();
-      for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) t = u128_add(t, sm[ww][threadIdx.x]);
-      atomic_add_u128(&accl[(size_t)c.big * 11 + threadIdx.x], t);
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const unsigned br = bv[u] & ~bl[u];
+      if ((bv[u] >> lane) & 1u) {
+        const bool left = (bl[u] >> lane) & 1u;
+        const int dst = left ? lo + __popc(bl[u] & lt) : ro + __popc(br & lt);
+        pout[dst] = pv[u];
+        sout[dst] = sv[u];
+        iout[dst] = iv[u];
+        if (left == small_left) moments_add_point(M, pv[u], sv[u], t0);
+      }
+      lo += __popc(bl[u]);
+      ro += __popc(br);
     }
-    __syncthreads();
+    block_add_moments(M, sm, accl + (size_t)c.big * 11);  // also orders swl's reuse
   }
 }
 
@@ -960,24 +1027,17 @@ __global__ void k_big_childmom(const BNode* nodes, const LevelState* ls, const i
 
 // ---- children ------------------------------------------------------------------------
 
-__global__ void k_level_sums(const BNode* nodes, const LevelState* ls, int32_t* bsum) {
-  __shared__ int sm[32];
-  int b, e;
-  level_range(ls, b, e);
-  int v = 0;
-  for (int i = b + threadIdx.x; i < e; i += blockDim.x) v += nodes[i].split ? 1 : 0;
-  int total;
-  block_scan(v, sm, &total);
-  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
-}
-
 __global__ void k_level_children(BNode* nodes, LevelState* ls, const int32_t* bsum, int32_t cap) {
   __shared__ int sm[32];
   int b, e;
   level_range(ls, b, e);
   const int le = ls->le;
-  int pre = 0;
-  for (int k = 0; k < (int)blockIdx.x; ++k) pre += bsum[k];
+  int pre;  // split nodes of the blocks before this one
+  {
+    int v = 0;
+    for (int k = threadIdx.x; k < (int)blockIdx.x; k += blockDim.x) v += bsum[k];
+    block_scan(v, sm, &pre);
+  }
   int carry = 0;
   for (int base = b; base < e; base += blockDim.x) {
     int i = base + threadIdx.x;
@@ -1016,10 +1076,14 @@ __global__ void k_level_children(BNode* nodes, LevelState* ls, const int32_t* bs
   }
 }
 
+// One block: the level's split count from the per-block counts, then the next level.
 __global__ void k_level_advance(LevelState* ls, const int32_t* bsum, int nblocks, int32_t* level_begin) {
-  if (ls->lb >= ls->le) return;
-  int total = 0;
-  for (int k = 0; k < nblocks; ++k) total += bsum[k];
+  __shared__ int sm[32];
+  int v = 0;
+  for (int k = threadIdx.x; k < nblocks; k += blockDim.x) v += bsum[k];
+  int total;
+  block_scan(v, sm, &total);
+  if (threadIdx.x != 0 || ls->lb >= ls->le) return;
   ls->lb = ls->le;
   ls->le = ls->le + 2 * total;
   ls->cur ^= 1;
@@ -1363,27 +1427,23 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
           for (int c = 0; c < 4; ++c) count_launch();
         }
       }
-      k_decide<<<kGridBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.mom, P);
-      k_level_sums<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum);
+      k_decide<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.mom, P, w.bsum, w.bbig);
       k_level_children<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum, (int32_t)w.cap_nodes);
       k_small_part<<<kSmallBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.B, w.ts0, w.mom);
-      for (int c = 0; c < 4; ++c) count_launch();
+      for (int c = 0; c < 3; ++c) count_launch();
       if (host_max > kBig) {
-        if (!level0) {
-          k_big_sums<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig);
+        if (!level0) {  // k_decide counted the large nodes per block
           k_big_plan<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig, w.chunks, w.chunk_cap, w.big_list,
                                                        w.node_chunk0, w.acc, w.accl);
-          count_launch();
           count_launch();
         }
         k_big_count<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_nl);
         k_big_offsets<<<64, 128, 0, s>>>(w.nodes, w.ls, w.big_list, w.node_chunk0, w.chunk_nl, w.chunk_loff);
-        k_big_scatter<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_loff);
-        k_big_leftmom<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.B, w.ts0, w.nodes, w.accl);
+        k_big_scatter<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_loff, w.ts0, w.accl);
         k_big_childmom<<<64, 256, 0, s>>>(w.nodes, w.ls, w.big_list, w.accl, w.mom);
         for (int c = 0; c < 5; ++c) count_launch();
       }
-      k_level_advance<<<1, 1, 0, s>>>(w.ls, w.bsum, kLevelBlocks, w.level_begin);
+      k_level_advance<<<1, kThreads, 0, s>>>(w.ls, w.bsum, kLevelBlocks, w.level_begin);
       count_launch();
     }
     KDS_CK(cudaGetLastError());

@@ -114,6 +114,86 @@ int kds_tree_import(const float* mean, const float* dir, const double* dts_mean,
 
 int kds_tree_get_info(const kds_tree* t, kds_tree_info* info);
 
+/* Tree_::root_mean / root_eigenvalues / root_eigenvectors (kd/tree/tree_.h:35-37) as
+ * TreeCPU_'s constructor sets them (kd/tree/tree_cpu_.h:72-86): the root's mean, its
+ * covariance eigenvalues ascending and eigenvectors column-major (columns 0 and 2
+ * reoriented towards the origin, column 0 negated if the determinant is negative).
+ * Built trees carry their own; trees from kds_tree_from_msg carry the message's; trees
+ * from kds_tree_import carry zeros.  Any pointer may be NULL. */
+int kds_tree_get_root(const kds_tree* t, float mean[3], float eigenvalues[3], float eigenvectors[9]);
+
+/* ------------------------------------------------------------------------------
+ * Scan input: toPointsVector + Voxelizer_::voxelize, on the device
+ * ------------------------------------------------------------------------------ */
+
+/* Voxelizer_ PARAMs (kd/utils/voxelizer_.h:37-41), same names and defaults. */
+typedef struct {
+  float range_min;      /* 0: min lidar range [m] */
+  float range_max;      /* 100: max lidar range [m] */
+  float space_res;      /* 0: spatial voxel resolution [m]; 0 = no voxel grid */
+  float time_res;       /* 0: temporal voxel resolution [s]; 0 = disabled */
+  int32_t use_boundary; /* 0: conservative boundary clipping */
+} kds_voxel_params;
+
+void kds_voxel_params_default(kds_voxel_params* p);
+
+/* Replaces toPointsVector (lib/kd_io/scan_utils_impl_.h:9-33) followed by
+ * Voxelizer_::voxelize (kd/utils/voxelizer_impl_.h:111-145): stamps are the per-point
+ * stamps when given, else msg_t + (atan2(y, x) + pi) / (2 pi) * scan_duration when
+ * scan_duration > 0, else msg_t.  Without a voxel grid the points within
+ * [range_min, range_max] are kept in input order; with one, each occupied voxel gives
+ * the mean of its points (float sums in input order, stamps in double, as the
+ * reference's Accumulator) if that mean is within range -- voxels in ascending order of
+ * their integer index (x, y, z, t) where the reference emits its hash map's order.
+ * Inputs and outputs are in the memory that mem names; out_xyz (3n floats) and
+ * out_stamps (n doubles, may be NULL) have room for n points; *out_n receives the
+ * count.  The output feeds kds_tree_build directly. */
+int kds_points_voxelize(const float* xyz, const double* stamps, int64_t n, int32_t mem, double msg_t,
+                        double scan_duration, const kds_voxel_params* p, void* stream, float* out_xyz,
+                        double* out_stamps, int64_t* out_n);
+
+/* ------------------------------------------------------------------------------
+ * Tree wire format: kd_slam2_msgs/msg/KDTree3f with KDNode3f nodes (no points)
+ * ------------------------------------------------------------------------------ */
+
+/* kd_slam2_msgs/msg/KDNode3f (kd_slam2_msgs/msg/KDNode3f.msg), field for field, in the
+ * layout of its generated C++ struct (56 bytes). */
+typedef struct {
+  float mean[3];
+  float direction[3];
+  uint32_t idx_start;
+  uint32_t idx_end;
+  int32_t idx_left;
+  int32_t idx_right;
+  double dts_mean;
+  double dts_covariance;
+} kds_kdnode3f;
+
+/* The tree fields of kd_slam2_msgs/msg/KDTree3f (kd_slam2_msgs/msg/KDTree3f.msg; the
+ * header and src_topic stay with the caller).  nodes: host memory, num_nodes records. */
+typedef struct {
+  double ts_start;
+  float root_mean[3];
+  float root_eigenvalues[3];
+  float root_eigenvectors[9]; /* column-major, as in the message */
+  int64_t num_nodes;
+  kds_kdnode3f* nodes;
+} kds_kdtree3f;
+
+/* Replaces TreeLoader_::fromTreeMsg (lib/kd_io/tree_loader_impl_.h:59-70) with the
+ * bag reader's KDTree3f -> Tree_ conversion (lib/kd_io/rosbag2_message_reader.cpp:159-191):
+ * uploads the node records (one copy of the raw records, unpacked on the device) as a
+ * device tree without points.  The nodes must be BFS numbered (children after their
+ * parent), as the reference's pruned trees are; otherwise KDS_ERR_BAD_TREE. */
+int kds_tree_from_msg(const kds_kdtree3f* msg, kds_tree** out);
+
+/* Replaces toMessage / makeKDTreeMessage (lib/kd_io/slam_messages.h:47-80) and the bag
+ * writer's Tree_ -> KDTree3f conversion (lib/kd_io/rosbag2_message_writer.cpp:258-290):
+ * fills the tree fields of msg.  On entry msg->num_nodes is the capacity of msg->nodes
+ * (may be 0 with nodes NULL to query the count); on return it is the tree's node count,
+ * and KDS_ERR_CAPACITY is returned if the records did not fit. */
+int kds_tree_to_msg(const kds_tree* t, kds_kdtree3f* msg);
+
 /* Device-to-host copy of the tree (any pointer may be NULL).  leaves: num_leaves node
  * indices (Tree_::_leaves_indices_ptr); perm: num_points input indices in final order. */
 int kds_tree_export(const kds_tree* t, float* mean, float* dir, double* dts_mean, double* dts_cov, int64_t* idx_start,
@@ -270,6 +350,30 @@ int kds_batch_run(kds_batch* b, kds_job* jobs, int32_t num_jobs, int32_t use_gra
  * depend on the configuration. */
 int kds_batch_autotune(kds_batch* b, kds_job* jobs, int32_t num_jobs, void* stream, int32_t* chosen,
                        double* ms_out);
+
+/* One multi-view bundle-adjustment factor over a job of the last kds_batch_run.
+ * ICP (a KDS_ICP job): var[0] = fixed pose, var[1] = moving pose (MultiViewICPFactor_).
+ * CT-ICP (a KDS_CTICP job run as KDS_JOB_LINEARIZE_DUAL): var = pose_A, vel_A, pose_B,
+ * vel_B (MultiViewCTICPFactor_).  Variables are 6-dimensional, numbered by the caller. */
+typedef struct {
+  int32_t job;
+  int32_t var[4];
+} kds_factor;
+
+/* Replaces the block updates of MultiViewICPFactor_::compute and
+ * MultiViewCTICPFactor_::compute (kd/map/multiview_icp_factor_impl_.h:30-62,
+ * kd/map/multiview_cticp_factor_impl_.h:33-83) for all factors at once, on the device,
+ * from the H, b of the last kds_batch_run: a factor counts when
+ * inlierRatio() > disable_inlier_ratio (enabled[f], may be NULL); the sum of the counted
+ * factors' blocks is returned as the upper block triangle (row variable <= column
+ * variable): block k is variables (block_rc[2k], block_rc[2k+1]), 36 doubles row-major
+ * in H_blocks, sorted by (row, column); b: 6 doubles per variable (may be NULL).
+ * Contributions are summed in FP64 in factor order.  On entry *num_blocks is the
+ * capacity (0 with NULL block_rc / H_blocks queries the count); on return the count,
+ * with KDS_ERR_CAPACITY if the blocks did not fit. */
+int kds_batch_assemble(kds_batch* b, const kds_factor* factors, int32_t num_factors, int32_t num_vars,
+                       float disable_inlier_ratio, void* stream, int32_t* num_blocks, int32_t* block_rc,
+                       double* H_blocks, double* b_vec, int32_t* enabled);
 void kds_batch_free(kds_batch* b);
 
 /* ------------------------------------------------------------------------------

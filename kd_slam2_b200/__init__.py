@@ -116,6 +116,40 @@ class Tree:
         out["ts_start"] = inf.ts_start
         return out
 
+    def root(self) -> dict:
+        """Tree_::root_mean / root_eigenvalues / root_eigenvectors (3x3, columns = vectors)."""
+        m, ev, V = np.zeros(3, np.float32), np.zeros(3, np.float32), np.zeros(9, np.float32)
+        _check(_lib.kds_tree_get_root(self._h, m.ctypes.data, ev.ctypes.data, V.ctypes.data), "kds_tree_get_root")
+        return {"root_mean": m, "root_eigenvalues": ev, "root_eigenvectors": V.reshape(3, 3).T.copy()}
+
+    def to_msg(self) -> dict:
+        """toMessage (lib/kd_io/slam_messages.h:47-80): the tree fields of a KDTree3f message;
+        nodes as a KDNODE3F_DTYPE array, root_eigenvectors column-major (9 floats)."""
+        m = L.KDTree3f()
+        _check(_lib.kds_tree_to_msg(self._h, C.byref(m)), "kds_tree_to_msg")  # count query
+        nodes = np.zeros(m.num_nodes, L.KDNODE3F_DTYPE)
+        m.nodes = nodes.ctypes.data
+        _check(_lib.kds_tree_to_msg(self._h, C.byref(m)), "kds_tree_to_msg")
+        return {"ts_start": m.ts_start, "root_mean": np.array(m.root_mean, np.float32),
+                "root_eigenvalues": np.array(m.root_eigenvalues, np.float32),
+                "root_eigenvectors": np.array(m.root_eigenvectors, np.float32), "nodes": nodes}
+
+    @staticmethod
+    def from_msg(msg: dict) -> "Tree":
+        """TreeLoader_::fromTreeMsg (lib/kd_io/tree_loader_impl_.h:59-70): a device tree (no
+        points) from the tree fields of a KDTree3f message (the dict of Tree.to_msg)."""
+        nodes = np.ascontiguousarray(msg["nodes"], L.KDNODE3F_DTYPE)
+        m = L.KDTree3f()
+        m.ts_start = float(msg.get("ts_start", 0.0))
+        for k in ("root_mean", "root_eigenvalues", "root_eigenvectors"):
+            if k in msg:
+                getattr(m, k)[:] = [float(x) for x in np.asarray(msg[k], np.float32).reshape(-1)]
+        m.num_nodes = len(nodes)
+        m.nodes = nodes.ctypes.data
+        h = C.c_void_p()
+        _check(_lib.kds_tree_from_msg(C.byref(m), C.byref(h)), "kds_tree_from_msg")
+        return Tree(h.value)
+
     @staticmethod
     def import_nodes(mean, dir, left, right, dts_mean=None, dts_cov=None, start=None, end=None,
                      ts_start: float = 0.0) -> "Tree":
@@ -420,6 +454,26 @@ class Batch:
         _check(_lib.kds_batch_run(self._h, arr, len(jobs), 1 if use_graph else 0, stream), "kds_batch_run")
         return arr
 
+    def assemble(self, factors, num_vars: int, disable_inlier_ratio: float = 1.0, stream=None):
+        """MultiViewICPFactor_ / MultiViewCTICPFactor_ block updates of the last run, on the
+        device (kds_batch_assemble).  factors: (job, [vars]) pairs.  Returns (block_rc (K,2),
+        H_blocks (K,6,6), b (num_vars,6), enabled (num_factors,))."""
+        fa = (L.Factor * len(factors))()
+        for f, (job, vs) in enumerate(factors):
+            fa[f].job = job
+            fa[f].var[:] = list(vs) + [-1] * (4 - len(vs))
+        nb = C.c_int32(0)
+        _check(_lib.kds_batch_assemble(self._h, fa, len(factors), num_vars, disable_inlier_ratio, stream,
+                                       C.byref(nb), None, None, None, None), "kds_batch_assemble")
+        rc = np.zeros((nb.value, 2), np.int32)
+        H = np.zeros((nb.value, 6, 6))
+        b = np.zeros((num_vars, 6))
+        en = np.zeros(len(factors), np.int32)
+        _check(_lib.kds_batch_assemble(self._h, fa, len(factors), num_vars, disable_inlier_ratio, stream,
+                                       C.byref(nb), rc.ctypes.data, H.ctypes.data, b.ctypes.data, en.ctypes.data),
+               "kds_batch_assemble")
+        return rc, H, b, en.astype(bool)
+
 
 # ---------------------------------------------------------------------------- serving
 class Server:
@@ -537,6 +591,41 @@ def aligner_params(**kw) -> L.AlignerParams:
     for k, v in kw.items():
         setattr(p, k, v)
     return p
+
+
+def voxel_params(**kw) -> L.VoxelParams:
+    p = L.VoxelParams()
+    _lib.kds_voxel_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def voxelize(xyz, stamps=None, msg_t: float = 0.0, scan_duration: float = 0.0, stream=None, **params):
+    """toPointsVector + Voxelizer_::voxelize (kds_points_voxelize).  xyz (n, 3) float32 and
+    stamps (n,) float64 (or None) as numpy arrays (host) or CUDA tensors (device); params
+    are Voxelizer_'s (range_min, range_max, space_res, time_res, use_boundary).  Returns
+    (xyz, stamps) of the kept points or voxel means, of the same kind as the inputs."""
+    prm = voxel_params(**params)
+    n = C.c_int64(0)
+    if hasattr(xyz, "is_cuda") and xyz.is_cuda:
+        import torch
+        x = xyz.contiguous().to(torch.float32)
+        st = None if stamps is None else stamps.contiguous().to(torch.float64)
+        ox = torch.empty_like(x)
+        ost = torch.empty(len(x), dtype=torch.float64, device=x.device)
+        _check(_lib.kds_points_voxelize(x.data_ptr(), None if st is None else st.data_ptr(), len(x),
+                                        L.KDS_MEM_DEVICE, msg_t, scan_duration, C.byref(prm), stream, ox.data_ptr(),
+                                        ost.data_ptr(), C.byref(n)), "kds_points_voxelize")
+        return ox[:n.value], ost[:n.value]
+    x = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    st = None if stamps is None else np.ascontiguousarray(stamps, np.float64)
+    ox = np.zeros_like(x)
+    ost = np.zeros(len(x))
+    _check(_lib.kds_points_voxelize(x.ctypes.data, _ptr(st), len(x), L.KDS_MEM_HOST, msg_t, scan_duration,
+                                    C.byref(prm), stream, ox.ctypes.data, ost.ctypes.data, C.byref(n)),
+           "kds_points_voxelize")
+    return ox[:n.value].copy(), ost[:n.value].copy()
 
 
 def tree_params(**kw) -> L.TreeParams:

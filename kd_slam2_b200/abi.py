@@ -9,6 +9,8 @@ from __future__ import annotations
 import ctypes as C
 import os
 
+import numpy as np
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libkds.so")
 
@@ -58,6 +60,57 @@ class TreeInfo(C.Structure):
         ("ts_start", C.c_double),
         ("accepted", C.c_int32),
         ("depth", C.c_int32),
+    ]
+
+
+class KDNode3f(C.Structure):
+    """kd_slam2_msgs/msg/KDNode3f (kds_kdnode3f, 56 bytes)."""
+    _fields_ = [
+        ("mean", C.c_float * 3),
+        ("direction", C.c_float * 3),
+        ("idx_start", C.c_uint32),
+        ("idx_end", C.c_uint32),
+        ("idx_left", C.c_int32),
+        ("idx_right", C.c_int32),
+        ("dts_mean", C.c_double),
+        ("dts_covariance", C.c_double),
+    ]
+
+
+# the same record as a numpy dtype (arrays of KDNode3f without per-record ctypes objects)
+KDNODE3F_DTYPE = np.dtype({
+    "names": ["mean", "direction", "idx_start", "idx_end", "idx_left", "idx_right", "dts_mean", "dts_covariance"],
+    "formats": [("<f4", (3,)), ("<f4", (3,)), "<u4", "<u4", "<i4", "<i4", "<f8", "<f8"],
+    "offsets": [0, 12, 24, 28, 32, 36, 40, 48],
+    "itemsize": 56,
+})
+
+
+class KDTree3f(C.Structure):
+    """The tree fields of kd_slam2_msgs/msg/KDTree3f (kds_kdtree3f)."""
+    _fields_ = [
+        ("ts_start", C.c_double),
+        ("root_mean", C.c_float * 3),
+        ("root_eigenvalues", C.c_float * 3),
+        ("root_eigenvectors", C.c_float * 9),
+        ("num_nodes", C.c_int64),
+        ("nodes", C.c_void_p),
+    ]
+
+
+class Factor(C.Structure):
+    """kds_factor: a multi-view BA factor over a batch job."""
+    _fields_ = [("job", C.c_int32), ("var", C.c_int32 * 4)]
+
+
+class VoxelParams(C.Structure):
+    """kds_voxel_params: Voxelizer_ PARAMs."""
+    _fields_ = [
+        ("range_min", C.c_float),
+        ("range_max", C.c_float),
+        ("space_res", C.c_float),
+        ("time_res", C.c_float),
+        ("use_boundary", C.c_int32),
     ]
 
 
@@ -204,6 +257,12 @@ SIGNATURES = {
                                        C.POINTER(_I32)]),
     "kds_tree_import": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _I64, C.c_double, C.POINTER(_P)]),
     "kds_tree_get_info": (C.c_int, [_P, C.POINTER(TreeInfo)]),
+    "kds_tree_get_root": (C.c_int, [_P, _P, _P, _P]),
+    "kds_voxel_params_default": (None, [C.POINTER(VoxelParams)]),
+    "kds_points_voxelize": (C.c_int, [_P, _P, _I64, _I32, C.c_double, C.c_double, C.POINTER(VoxelParams), _P, _P,
+                                      _P, C.POINTER(_I64)]),
+    "kds_tree_from_msg": (C.c_int, [C.POINTER(KDTree3f), C.POINTER(_P)]),
+    "kds_tree_to_msg": (C.c_int, [_P, C.POINTER(KDTree3f)]),
     "kds_tree_export": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "kds_tree_apply_velocities": (C.c_int, [_P, _P, _I32, _P]),
     "kds_tree_apply_isometry": (C.c_int, [_P, _P, _P]),
@@ -243,6 +302,8 @@ SIGNATURES = {
     "kds_batch_create": (C.c_int, [C.POINTER(_P)]),
     "kds_batch_run": (C.c_int, [_P, C.POINTER(Job), _I32, _I32, _P]),
     "kds_batch_autotune": (C.c_int, [_P, C.POINTER(Job), _I32, _P, C.POINTER(_I32), _P]),
+    "kds_batch_assemble": (C.c_int, [_P, C.POINTER(Factor), _I32, _I32, C.c_float, _P, C.POINTER(_I32), _P, _P,
+                                     _P, _P]),
     "kds_batch_free": (None, [_P]),
     "kds_server_params_default": (None, [C.POINTER(ServerParams)]),
     "kds_server_create": (C.c_int, [C.POINTER(ServerParams), C.POINTER(_P)]),

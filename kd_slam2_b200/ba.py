@@ -142,3 +142,28 @@ def jobs(wl: Workload, trees, icp_params: dict, ct_params: dict):
         else:
             out.append(make_job(KDS_CTICP, trees[p.i], trees[p.j], pc, X=p.X0, v=kf_j.vel, fixed_v=kf_i.vel))
     return out
+
+
+def factor_jobs(wl: Workload, trees, icp_params: dict, ct_params: dict, X=None, v=None):
+    """The linearizations of one bundle-adjustment step: per pair, the rigid factor
+    (MultiViewICPFactor_: buildQuadraticForm at the two keyframes' world poses) and the
+    continuous-time factor (MultiViewCTICPFactor_: buildQuadraticFormDual at the poses
+    and velocities).  X, v: per-keyframe estimates (default: the keyframes' own).
+    Variables: pose of keyframe k = 2k, its velocity = 2k + 1.
+    Returns (jobs, factors as (job, vars), number of variables)."""
+    from . import aligner_params, make_job
+    from .abi import KDS_CTICP, KDS_ICP, KDS_JOB_LINEARIZE, KDS_JOB_LINEARIZE_DUAL
+    X = [kf.X for kf in wl.keyframes] if X is None else X
+    v = [kf.vel for kf in wl.keyframes] if v is None else v
+    pi, pc = aligner_params(**icp_params), aligner_params(**ct_params)
+    jobs, factors = [], []
+    for p in wl.pairs:
+        i, j = p.i, p.j
+        if p.kind == 0:
+            jobs.append(make_job(KDS_ICP, trees[i], trees[j], pi, X=X[j], fixed_X=X[i], mode=KDS_JOB_LINEARIZE))
+            factors.append((len(jobs) - 1, [2 * i, 2 * j]))
+        else:
+            jobs.append(make_job(KDS_CTICP, trees[i], trees[j], pc, X=X[j], fixed_X=X[i], v=v[j], fixed_v=v[i],
+                                 mode=KDS_JOB_LINEARIZE_DUAL))
+            factors.append((len(jobs) - 1, [2 * i, 2 * i + 1, 2 * j, 2 * j + 1]))
+    return jobs, factors, 2 * len(wl.keyframes)

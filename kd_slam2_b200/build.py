@@ -29,6 +29,8 @@ UNITS = [
     ("kds_align.cu", []),
     ("kds_api.cu", []),
     ("kds_serve.cu", ["-fmad=false"]),
+    ("kds_factor.cu", []),
+    ("kds_voxel.cu", []),
 ]
 
 

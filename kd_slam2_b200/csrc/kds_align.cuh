@@ -171,4 +171,8 @@ int linearize_static(const TreeDev& fixed, const TreeDev& moving, int32_t type, 
                      const double* X, const double* Xf, const double* v, const double* fv, int32_t stats_mode,
                      cudaStream_t s, double* H, double* b, kds_stats* stats);
 
+// Device assembly of multi-view factor blocks from a runner's last outputs (kds_factor.cu).
+int batch_assemble(Runner& R, const kds_factor* F, int32_t nf, int32_t nvars, float ratio, cudaStream_t s,
+                   int32_t* num_blocks, int32_t* block_rc, double* H_out, double* b_out, int32_t* enabled_out);
+
 }  // namespace kds

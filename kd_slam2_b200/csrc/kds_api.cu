@@ -190,6 +190,75 @@ int kds_tree_get_info(const kds_tree* t, kds_tree_info* info) {
   return KDS_OK;
 }
 
+void kds_voxel_params_default(kds_voxel_params* p) {
+  if (!p) return;
+  p->range_min = 0.f;
+  p->range_max = 100.f;
+  p->space_res = 0.f;
+  p->time_res = 0.f;
+  p->use_boundary = 0;
+}
+
+int kds_points_voxelize(const float* xyz, const double* stamps, int64_t n, int32_t mem, double msg_t,
+                        double scan_duration, const kds_voxel_params* p, void* stream, float* out_xyz,
+                        double* out_stamps, int64_t* out_n) {
+  KDS_INIT();
+  return points_voxelize(xyz, stamps, n, mem, msg_t, scan_duration, p, as_stream(stream), out_xyz, out_stamps,
+                         out_n);
+}
+
+int kds_tree_get_root(const kds_tree* t, float mean[3], float eigenvalues[3], float eigenvectors[9]) {
+  if (!t) { set_error("kds_tree_get_root: NULL tree"); return KDS_ERR_INVALID_ARG; }
+  if (mean) memcpy(mean, t->root_mean, sizeof(t->root_mean));
+  if (eigenvalues) memcpy(eigenvalues, t->root_eigenvalues, sizeof(t->root_eigenvalues));
+  if (eigenvectors) memcpy(eigenvectors, t->root_eigenvectors, sizeof(t->root_eigenvectors));
+  return KDS_OK;
+}
+
+int kds_tree_from_msg(const kds_kdtree3f* msg, kds_tree** out) {
+  if (!out || !msg) { set_error("kds_tree_from_msg: NULL argument"); return KDS_ERR_INVALID_ARG; }
+  *out = nullptr;
+  KDS_INIT();
+  return tree_from_msg(msg, out);
+}
+
+int kds_tree_to_msg(const kds_tree* t, kds_kdtree3f* msg) {
+  if (!t || !msg || msg->num_nodes < 0) { set_error("kds_tree_to_msg: bad argument"); return KDS_ERR_INVALID_ARG; }
+  const int64_t n = t->d.num_nodes, cap = msg->num_nodes;
+  msg->ts_start = t->d.ts_start;
+  memcpy(msg->root_mean, t->root_mean, sizeof(t->root_mean));
+  memcpy(msg->root_eigenvalues, t->root_eigenvalues, sizeof(t->root_eigenvalues));
+  memcpy(msg->root_eigenvectors, t->root_eigenvectors, sizeof(t->root_eigenvectors));
+  msg->num_nodes = n;
+  if (cap < n || (n > 0 && !msg->nodes)) {
+    if (cap == 0 && !msg->nodes) return KDS_OK;  // count query
+    set_error("kds_tree_to_msg: %lld node records do not fit in %lld", (long long)n, (long long)cap);
+    return KDS_ERR_CAPACITY;
+  }
+  if (n == 0) return KDS_OK;
+  std::vector<float> mean(3 * n), dir(3 * n);
+  std::vector<double> dm(n), dc(n);
+  std::vector<int64_t> s0(n), e0(n);
+  std::vector<int32_t> l(n), r(n);
+  int rc = tree_export(t, mean.data(), dir.data(), dm.data(), dc.data(), s0.data(), e0.data(), l.data(), r.data(),
+                       nullptr, nullptr, nullptr);
+  if (rc) return rc;
+  for (int64_t i = 0; i < n; ++i) {
+    kds_kdnode3f& k = msg->nodes[i];
+    for (int d = 0; d < 3; ++d) {
+      k.mean[d] = mean[3 * i + d];
+      k.direction[d] = dir[3 * i + d];
+    }
+    k.idx_start = (uint32_t)s0[i];
+    k.idx_end = (uint32_t)e0[i];
+    k.idx_left = l[i];
+    k.idx_right = r[i];
+    k.dts_mean = dm[i];
+    k.dts_covariance = dc[i];
+  }
+  return KDS_OK;
+}
+
 int kds_tree_export(const kds_tree* t, float* mean, float* dir, double* dts_mean, double* dts_cov, int64_t* idx_start,
                     int64_t* idx_end, int32_t* left, int32_t* right, int32_t* level, int64_t* leaves, int64_t* perm) {
   if (!t) { set_error("kds_tree_export: NULL tree"); return KDS_ERR_INVALID_ARG; }
@@ -710,6 +779,14 @@ int kds_batch_autotune(kds_batch* B, kds_job* jobs, int32_t num_jobs, void* stre
   B->runner.order_by_size = best / 3;
   if (chosen) *chosen = best;
   return KDS_OK;
+}
+
+int kds_batch_assemble(kds_batch* B, const kds_factor* factors, int32_t num_factors, int32_t num_vars,
+                       float disable_inlier_ratio, void* stream, int32_t* num_blocks, int32_t* block_rc,
+                       double* H_blocks, double* b_vec, int32_t* enabled) {
+  if (!B) { set_error("kds_batch_assemble: NULL batch"); return KDS_ERR_INVALID_ARG; }
+  return batch_assemble(B->runner, factors, num_factors, num_vars, disable_inlier_ratio, as_stream(stream),
+                        num_blocks, block_rc, H_blocks, b_vec, enabled);
 }
 
 int kds_batch_run(kds_batch* B, kds_job* jobs, int32_t num_jobs, int32_t use_graph, void* stream) {

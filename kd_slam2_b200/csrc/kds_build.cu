@@ -33,6 +33,7 @@ namespace kds {
 namespace {
 
 constexpr int kBig = 1024;
+constexpr int kRootFrame = 15;  // doubles per root: eigenvalues, eigenvectors, mean (decide)
 constexpr int kChunk = 1024;
 constexpr int kThreads = 256;
 constexpr int kGridBlocks = 148 * 4;
@@ -311,7 +312,11 @@ __device__ void jacobi3(const double Ain[3][3], double ev[3], double V[3][3]) {
 // (kd/tree/flat_leaf_policy_.h:52-108, count_leaf_policy_.h:27-43,
 // label_policy_base_impl_.h:12-97) on FP64 statistics.
 // Sd: the node's 11 moment sums converted to double (fx_to_d of the exact sums).
-__device__ __noinline__ void decide(const double* Sd, int64_t n, BNode& nd, const BuildParams& P) {
+// root (nullable): for a root node, its frame as TreeCPU_'s constructor stores it
+// (kd/tree/tree_cpu_.h:72-86): [0..2] eigenvalues ascending, [3..11] eigenvectors
+// column-major (columns 0 and 2 reoriented as in fillMetadata, then column 0 negated if
+// the determinant is negative), [12..14] mean; zero where the node has < 3 points.
+__device__ __noinline__ void decide(const double* Sd, int64_t n, BNode& nd, const BuildParams& P, double* root) {
   for (int i = 0; i < 3; ++i) { nd.mean[i] = 0.f; nd.dir[i] = 0.f; }
   nd.dts_mean = 0.0;
   nd.dts_cov = 0.0;
@@ -342,7 +347,27 @@ __device__ __noinline__ void decide(const double* Sd, int64_t n, BNode& nd, cons
       if (ddot3(mean_d, e0) > 0.0) for (int i = 0; i < 3; ++i) e0[i] = -e0[i];
       if (ddot3(mean_d, e2) > 0.0) for (int i = 0; i < 3; ++i) e2[i] = -e2[i];
       is_bad = false;
+      if (root) {
+        const double e1[3] = {V[0][1], V[1][1], V[2][1]};
+        // det [e0 e1 e2] = e0 . (e1 x e2)
+        const double cx = e1[1] * e2[2] - e1[2] * e2[1];
+        const double cy = e1[2] * e2[0] - e1[0] * e2[2];
+        const double cz = e1[0] * e2[1] - e1[1] * e2[0];
+        const double det = e0[0] * cx + (e0[1] * cy + e0[2] * cz);
+        const double sg = det < 0.0 ? -1.0 : 1.0;
+        for (int i = 0; i < 3; ++i) {
+          root[i] = lam[i];
+          root[3 + i] = sg * e0[i];
+          root[6 + i] = e1[i];
+          root[9 + i] = e2[i];
+        }
+      }
     }
+  }
+  if (root) {
+    if (is_bad)
+      for (int i = 0; i < 12; ++i) root[i] = 0.0;
+    for (int i = 0; i < 3; ++i) root[12 + i] = mean_d[i];
   }
   bool is_node = false, is_leaf = false;
   if (is_bad) {
@@ -593,7 +618,7 @@ __global__ void __launch_bounds__(kThreads) k_root_moments(const BNode* nodes, i
 // the b-th contiguous range of the level's nodes and writes its count of split nodes
 // (the children's numbering scans these counts).
 __global__ void k_decide(BNode* nodes, const LevelState* ls, const U128* mom, BuildParams P, int32_t* bsum,
-                         int32_t* bbig) {
+                         int32_t* bbig, double* root_frame) {
   __shared__ int sm[32];
   int b, e;
   level_range(ls, b, e);
@@ -603,7 +628,7 @@ __global__ void k_decide(BNode* nodes, const LevelState* ls, const U128* mom, Bu
     const int n = nd.end - nd.start;
     double Sd[11];
     for (int k = 0; k < 11; ++k) Sd[k] = fx_to_d(mom[(size_t)i * 11 + k]);
-    decide(Sd, n, nd, P);
+    decide(Sd, n, nd, P, nd.level == 0 ? root_frame + (size_t)nd.tree * kRootFrame : nullptr);
     nodes[i] = nd;
     v += nd.split ? 1 : 0;
     if (n > kBig) {
@@ -1249,6 +1274,7 @@ struct BuildWs {
   U128* accl;  // left-child sums of the level's large nodes
   U128* mom;   // exact sums of every node (11 per node)
   double* ts0;
+  double* root_frame;  // kRootFrame per cloud (k_decide at level 0)
   unsigned long long* tsmin;
   int64_t* off;
   LevelState* ls;
@@ -1270,7 +1296,8 @@ size_t ws_bytes(int64_t n, int R) {
   return 2 * carve_size<float4>(n) + 2 * carve_size<double>(n) + 3 * carve_size<int32_t>(n) +
          carve_size<BNode>(cn) + 4 * carve_size<int32_t>(cn) + carve_size<int32_t>(ntiles) +
          carve_size<Chunk>(chunk_cap) + 4 * carve_size<int32_t>(chunk_cap) +
-         2 * carve_size<U128>((size_t)11 * (n / kBig + 2)) + carve_size<U128>((size_t)11 * cn) + 2 * carve_size<double>(R) + carve_size<int64_t>(R + 1) +
+         2 * carve_size<U128>((size_t)11 * (n / kBig + 2)) + carve_size<U128>((size_t)11 * cn) + 2 * carve_size<double>(R) +
+         carve_size<double>((size_t)kRootFrame * R) + carve_size<int64_t>(R + 1) +
          carve_size<LevelState>(1) + carve_size<int32_t>(kMaxDepth + 2) + carve_size<int32_t>(kLevelBlocks) +
          carve_size<int32_t>(2 * kLevelBlocks) +
          7 * carve_size<int32_t>(G) + 3 * carve_size<int32_t>(R) + carve_size<int32_t>(8) + carve_size<TreeDev>(R) +
@@ -1314,6 +1341,7 @@ int ws_alloc(BuildWs& w, int64_t n, int R, cudaStream_t s) {
   w.accl = carve<U128>(p, (size_t)11 * (n / kBig + 2));
   w.mom = carve<U128>(p, (size_t)11 * cn);
   w.ts0 = carve<double>(p, R);
+  w.root_frame = carve<double>(p, (size_t)kRootFrame * R);
   w.tsmin = carve<unsigned long long>(p, R);
   w.off = carve<int64_t>(p, R + 1);
   w.ls = carve<LevelState>(p, 1);
@@ -1427,7 +1455,7 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
           for (int c = 0; c < 4; ++c) count_launch();
         }
       }
-      k_decide<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.mom, P, w.bsum, w.bbig);
+      k_decide<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.mom, P, w.bsum, w.bbig, w.root_frame);
       k_level_children<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum, (int32_t)w.cap_nodes);
       k_small_part<<<kSmallBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.B, w.ts0, w.mom);
       for (int c = 0; c < 3; ++c) count_launch();
@@ -1483,11 +1511,12 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   k_group_tables<<<1, 1024, 0, s>>>(depth, R, w.cnt, w.lcnt, w.gp, w.lgp, w.to, w.lto, w.tot_nodes, w.tot_leaves);
   count_launch();
   std::vector<int32_t> tn(R), tl(R), tu(R);
-  std::vector<double> ts0(R);
+  std::vector<double> ts0(R), rf((size_t)kRootFrame * R);
   KDS_CK(cudaMemcpyAsync(tn.data(), w.tot_nodes, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, s));
   KDS_CK(cudaMemcpyAsync(tl.data(), w.tot_leaves, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, s));
   KDS_CK(cudaMemcpyAsync(tu.data(), w.ucnt, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, s));
   KDS_CK(cudaMemcpyAsync(ts0.data(), w.ts0, sizeof(double) * R, cudaMemcpyDeviceToHost, s));
+  KDS_CK(cudaMemcpyAsync(rf.data(), w.root_frame, sizeof(double) * kRootFrame * R, cudaMemcpyDeviceToHost, s));
   KDS_CK(cudaStreamSynchronize(s));
   std::vector<TreeDev> td(R);
   std::vector<kds_tree*> made(R, nullptr);
@@ -1505,6 +1534,12 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
     t->d.num_unpruned = tu[r];
     t->d.ts_start = ts0[r];
     t->d.depth = depth;
+    const double* f = &rf[(size_t)kRootFrame * r];
+    for (int i = 0; i < 3; ++i) {
+      t->root_eigenvalues[i] = (float)f[i];
+      t->root_mean[i] = (float)f[12 + i];
+    }
+    for (int i = 0; i < 9; ++i) t->root_eigenvectors[i] = (float)f[3 + i];
     made[r] = t;
     td[r] = t->d;
   }

@@ -70,6 +70,11 @@ int tree_gather_leaves(TreeDev& t, cudaStream_t s);
 
 struct kds_tree {
   kds::TreeDev d;
+  // Tree_::root_mean / root_eigenvalues / root_eigenvectors (column-major), host copies:
+  // from the build's root decision, or carried by a tree message
+  float root_mean[3] = {0.f, 0.f, 0.f};
+  float root_eigenvalues[3] = {0.f, 0.f, 0.f};
+  float root_eigenvectors[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 };
 
 // ---------------------------------------------------------------------------
@@ -220,6 +225,10 @@ int tree_import(const float* mean, const float* dir, const double* dts_mean, con
 int tree_apply_velocities(kds_tree* t, const float* v, int skip_leaves, cudaStream_t s);
 int tree_apply_isometry(kds_tree* t, const float* X, cudaStream_t s);
 int tree_extract_leaves(const kds_tree* t, const float* v6, float* out_host, cudaStream_t s);
+int tree_from_msg(const kds_kdtree3f* msg, kds_tree** out);
+int points_voxelize(const float* xyz, const double* stamps, int64_t n, int32_t mem, double msg_t,
+                    double scan_duration, const kds_voxel_params* prm, cudaStream_t s, float* out_xyz,
+                    double* out_stamps, int64_t* out_n);
 int tree_export(const kds_tree* t, float* mean, float* dir, double* dts_mean, double* dts_cov, int64_t* s0,
                 int64_t* e0, int32_t* left, int32_t* right, int32_t* level, int64_t* leaves, int64_t* perm);
 }  // namespace kds

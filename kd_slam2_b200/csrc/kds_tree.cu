@@ -3,6 +3,8 @@
 // -fmad=false so the morph and transform kernels round like the CPU oracle.
 #include <cuda_runtime.h>
 
+#include <cstddef>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -154,6 +156,30 @@ __global__ void k_import(TreeDev t, const float* mean, const float* dir, const d
   t.level[i] = 0;
 }
 
+static_assert(sizeof(kds_kdnode3f) == 56 && offsetof(kds_kdnode3f, idx_start) == 24 &&
+                  offsetof(kds_kdnode3f, dts_mean) == 40 && offsetof(kds_kdnode3f, dts_covariance) == 48,
+              "KDNode3f record layout");
+
+// kd_slam2_msgs/msg/KDNode3f records -> device node arrays (the bag reader's per-node
+// copy, lib/kd_io/rosbag2_message_reader.cpp:180-188), with the same checks as k_import.
+__global__ void k_import_msg(TreeDev t, const kds_kdnode3f* rec, int32_t* bad) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= t.num_nodes) return;
+  const kds_kdnode3f k = rec[i];
+  const int l = k.idx_left, r = k.idx_right;
+  if (l >= t.num_nodes || r >= t.num_nodes || (l >= 0 && l <= i) || (r >= 0 && r <= i)) *bad = 1;
+  DNode d;
+  d.a = make_float4(k.mean[0], k.mean[1], k.mean[2], k.direction[0]);
+  d.b = make_float4(k.direction[1], k.direction[2], __int_as_float(l), __int_as_float(r));
+  t.nodes[i] = d;
+  t.dts_mean[i] = k.dts_mean;
+  t.dts_f[i] = (float)k.dts_mean;
+  t.dts_cov[i] = k.dts_covariance;
+  t.range[2 * i] = (int64_t)k.idx_start;
+  t.range[2 * i + 1] = (int64_t)k.idx_end;
+  t.level[i] = 0;
+}
+
 __global__ void k_leaf_flags_plain(const DNode* nodes, int32_t n, int32_t* flag) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -239,6 +265,9 @@ int tree_gather_leaves(TreeDev& t, cudaStream_t s) {
   return KDS_OK;
 }
 
+static int import_finish(kds_tree* t, int32_t* flag, int32_t* rank, int32_t* tiles, int32_t* dbad, void* stg,
+                         cudaStream_t s, const char* who, kds_tree** out);
+
 int tree_import(const float* mean, const float* dir, const double* dts_mean, const double* dts_cov,
                 const int64_t* s0, const int64_t* e0, const int32_t* left, const int32_t* right, int64_t num_nodes,
                 double ts_start, kds_tree** out) {
@@ -287,7 +316,15 @@ int tree_import(const float* mean, const float* dir, const double* dts_mean, con
   // leaf list by scan over leaf flags, reusing the staging arrays (dl as flag, dr as rank)
   int32_t* flag = (int32_t*)ds;  // ds/de no longer needed after k_import on this stream
   int32_t* rank = (int32_t*)de;
-  int32_t* tiles = dl;
+  return import_finish(t, flag, rank, dl, dbad, stg, s, "kds_tree_import", out);
+}
+
+// Leaf list of an imported tree (scan over leaf flags), the leaf arrays, and the result
+// of the node checks; frees the staging block and hands the tree out (or releases it).
+// flag, rank, tiles: num_nodes int32 scratch each; dbad[0] the check flag, dbad[1] scratch.
+static int import_finish(kds_tree* t, int32_t* flag, int32_t* rank, int32_t* tiles, int32_t* dbad, void* stg,
+                         cudaStream_t s, const char* who, kds_tree** out) {
+  const int64_t num_nodes = t->d.num_nodes;
   int32_t* total = dbad + 1;
   k_leaf_flags_plain<<<nblk(num_nodes, 256), 256, 0, s>>>(t->d.nodes, (int32_t)num_nodes, flag); ::kds::count_launch();
   int rc2 = scan_exclusive(flag, rank, (int32_t)num_nodes, tiles, total, s);
@@ -295,7 +332,7 @@ int tree_import(const float* mean, const float* dir, const double* dts_mean, con
   tree_gather_leaves(t->d, s);
   int32_t bad = 0;
   cudaMemcpyAsync(&bad, dbad, 4, cudaMemcpyDeviceToHost, s);
-  ce = cudaStreamSynchronize(s);
+  cudaError_t ce = cudaStreamSynchronize(s);
   cudaFree(stg);
   if (ce != cudaSuccess || rc2) {
     tree_release(t->d);
@@ -305,11 +342,54 @@ int tree_import(const float* mean, const float* dir, const double* dts_mean, con
   if (bad) {
     tree_release(t->d);
     delete t;
-    set_error("kds_tree_import: child index out of range or not after its parent (BFS order required)");
+    set_error("%s: child index out of range or not after its parent (BFS order required)", who);
     return KDS_ERR_BAD_TREE;
   }
   *out = t;
   return KDS_OK;
+}
+
+int tree_from_msg(const kds_kdtree3f* msg, kds_tree** out) {
+  *out = nullptr;
+  const int64_t n = msg->num_nodes;
+  if (n <= 0 || n > ((int64_t)1 << 30) || !msg->nodes) {
+    set_error("kds_tree_from_msg: bad node array");
+    return KDS_ERR_INVALID_ARG;
+  }
+  int64_t nleaves = 0;
+  for (int64_t i = 0; i < n; ++i)
+    if (msg->nodes[i].idx_left < 0 && msg->nodes[i].idx_right < 0) ++nleaves;
+  kds_tree* t = new kds_tree();
+  cudaStream_t s = cudaStreamPerThread;
+  int rc = tree_alloc(t->d, n, nleaves, 0, s);
+  if (rc) { delete t; return rc; }
+  t->d.ts_start = msg->ts_start;
+  t->d.num_unpruned = n;
+  for (int i = 0; i < 3; ++i) {
+    t->root_mean[i] = msg->root_mean[i];
+    t->root_eigenvalues[i] = msg->root_eigenvalues[i];
+  }
+  for (int i = 0; i < 9; ++i) t->root_eigenvectors[i] = msg->root_eigenvectors[i];
+  // staging: the raw records, then three int32 arrays and two flags
+  void* stg = nullptr;
+  const size_t rec_bytes = (((size_t)n * sizeof(kds_kdnode3f)) + 255) & ~(size_t)255;
+  cudaError_t ce = cudaMalloc(&stg, rec_bytes + (size_t)n * 12 + 64);
+  if (ce != cudaSuccess) {
+    cudaGetLastError();
+    tree_release(t->d);
+    delete t;
+    set_error("kds_tree_from_msg: staging OOM");
+    return KDS_ERR_OOM;
+  }
+  kds_kdnode3f* drec = (kds_kdnode3f*)stg;
+  int32_t* flag = (int32_t*)((char*)stg + rec_bytes);
+  int32_t* rank = flag + n;
+  int32_t* tiles = rank + n;
+  int32_t* dbad = tiles + n;
+  cudaMemcpyAsync(drec, msg->nodes, (size_t)n * sizeof(kds_kdnode3f), cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(dbad, 0, 4, s);
+  k_import_msg<<<nblk(n, 256), 256, 0, s>>>(t->d, drec, dbad); ::kds::count_launch();
+  return import_finish(t, flag, rank, tiles, dbad, stg, s, "kds_tree_from_msg", out);
 }
 
 int tree_apply_velocities(kds_tree* t, const float* v, int skip_leaves, cudaStream_t s) {

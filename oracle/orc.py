@@ -87,6 +87,7 @@ def load() -> C.CDLL:
         "orc_tree_accepted": (C.c_int32, [P]),
         "orc_tree_ts_start": (C.c_double, [P]),
         "orc_tree_export": (None, [P] * 12),
+        "orc_tree_root": (None, [P, P, P, P]),
         "orc_tree_free": (None, [P]),
         "orc_align": (C.c_int32, [C.c_int32, C.c_int32, P, P, C.c_int32, P, C.POINTER(AlignParams),
                                   C.POINTER(OPrior), P, P, P, C.c_int32, C.c_int32, C.POINTER(OResult)]),
@@ -167,7 +168,14 @@ class OTree:
         out["ts_start"] = lib.orc_tree_ts_start(self.h)
         out["num_unpruned"] = lib.orc_tree_num_unpruned(self.h)
         out["accepted"] = self.accepted
+        out.update(self.root())
         return out
+
+    def root(self) -> dict:
+        """Tree_::root_mean / root_eigenvalues / root_eigenvectors (3x3, columns = vectors)."""
+        m, ev, V = np.zeros(3, np.float32), np.zeros(3, np.float32), np.zeros(9, np.float32)
+        load().orc_tree_root(self.h, m.ctypes.data, ev.ctypes.data, V.ctypes.data)
+        return {"root_mean": m, "root_eigenvalues": ev, "root_eigenvectors": V.reshape(3, 3).T.copy()}
 
 
 def align(kind: int, mode: int, fixed, moving: OTree, params: AlignParams, X0, v0=None, fixed_X=None,

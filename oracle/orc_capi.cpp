@@ -63,6 +63,13 @@ void orc_tree_export(void* h, float* mean, float* dir, double* dts_mean, double*
     for (size_t i = 0; i < t->perm.size(); ++i) perm[i] = t->perm[i];
 }
 
+void orc_tree_root(void* h, float* mean, float* eigenvalues, float* eigenvectors) {
+  const Tree* t = (const Tree*)h;
+  std::memcpy(mean, t->root_mean, sizeof(t->root_mean));
+  std::memcpy(eigenvalues, t->root_eigenvalues, sizeof(t->root_eigenvalues));
+  std::memcpy(eigenvectors, t->root_eigenvectors, sizeof(t->root_eigenvectors));
+}
+
 void orc_tree_free(void* h) { delete (Tree*)h; }
 
 int32_t orc_align(int32_t kind, int32_t mode, void* const* fixed, const double* fixed_X, int32_t num_fixed,

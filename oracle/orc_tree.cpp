@@ -164,9 +164,12 @@ struct Meta {
 };
 
 // fillMetadata of FlatLeafPolicy_ (with CountLeafPolicy_ and LabelPolicyBase_ below it).
+// root (nullable): the root's frame, [0..2] eigenvalues, [3..11] eigenvectors column-major
+// (fillMetadata's reorientation of columns 0 and 2, label_policy_base_impl_.h:89-95, then
+// column 0 negated for a negative determinant, tree_cpu_.h:79-82), [12..14] mean.
 static void fill_metadata(const Moments& M, int64_t n, bool has_parent, bool parent_has_prop,
                           const double* parent_prop, int level, const TreeParams& P, Node& node,
-                          Meta& meta) {
+                          Meta& meta, double* root) {
   meta = Meta();
   for (int i = 0; i < 3; ++i) { node.mean[i] = 0.f; node.dir[i] = 0.f; }
   node.dts_mean = 0.0;
@@ -200,7 +203,26 @@ static void fill_metadata(const Moments& M, int64_t n, bool has_parent, bool par
       if (ddot3(mean_d, e0) > 0.0) for (int i = 0; i < 3; ++i) e0[i] = -e0[i];
       if (ddot3(mean_d, e2) > 0.0) for (int i = 0; i < 3; ++i) e2[i] = -e2[i];
       is_bad = false;
+      if (root) {
+        const double e1[3] = {V[0][1], V[1][1], V[2][1]};
+        const double cx = e1[1] * e2[2] - e1[2] * e2[1];
+        const double cy = e1[2] * e2[0] - e1[0] * e2[2];
+        const double cz = e1[0] * e2[1] - e1[1] * e2[0];
+        const double det = e0[0] * cx + (e0[1] * cy + e0[2] * cz);
+        const double sg = det < 0.0 ? -1.0 : 1.0;
+        for (int i = 0; i < 3; ++i) {
+          root[i] = lam[i];
+          root[3 + i] = sg * e0[i];
+          root[6 + i] = e1[i];
+          root[9 + i] = e2[i];
+        }
+      }
     }
+  }
+  if (root) {
+    if (is_bad)
+      for (int i = 0; i < 12; ++i) root[i] = 0.0;
+    for (int i = 0; i < 3; ++i) root[12 + i] = mean_d[i];
   }
   // CountLeafPolicy_
   bool is_node = false, is_leaf = false;
@@ -330,7 +352,16 @@ Tree build_tree(const float* xyz, const double* st, int64_t n, const TreeParams&
       moments_of(xyz, st, T.perm.data(), s, e, T.ts_start, M);
       Meta meta;
       Node nd = nodes[i];
-      fill_metadata(M, e - s, has_parent[i], par_has[i], &par_prop[3 * i], levels[i], P, nd, meta);
+      double root[15];
+      fill_metadata(M, e - s, has_parent[i], par_has[i], &par_prop[3 * i], levels[i], P, nd, meta,
+                    i == 0 ? root : nullptr);
+      if (i == 0) {
+        for (int k = 0; k < 3; ++k) {
+          T.root_eigenvalues[k] = (float)root[k];
+          T.root_mean[k] = (float)root[12 + k];
+        }
+        for (int k = 0; k < 9; ++k) T.root_eigenvectors[k] = (float)root[3 + k];
+      }
       nd.left = nd.right = -1;
       if (meta.is_node) {
         // stable partition of perm[s..e)

@@ -36,6 +36,11 @@ struct Tree {
   std::vector<int64_t> leaves;   // leaf node indices, BFS order
   std::vector<int64_t> perm;     // final point order: perm[i] = input index at position i
   double ts_start = 0.0;
+  // Tree_::root_mean / root_eigenvalues / root_eigenvectors (column-major) as TreeCPU_'s
+  // constructor sets them (kd/tree/tree_cpu_.h:72-86), from the root's FP64 decision
+  float root_mean[3] = {0.f, 0.f, 0.f};
+  float root_eigenvalues[3] = {0.f, 0.f, 0.f};
+  float root_eigenvectors[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   int64_t num_points = 0;
   int64_t num_unpruned = 0;
   bool accepted = false;

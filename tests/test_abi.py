@@ -40,6 +40,16 @@ def test_struct_layouts():
     assert L.Job.X.offset == 4 * 4 + 2 * 8 + 40
     assert L.Job.result.offset == L.Job.X.offset + 36 * 8
     assert L.Job.H.offset % 8 == 0
+    # kds_kdnode3f / kds_kdtree3f: kd_slam2_msgs/msg/KDNode3f.msg and KDTree3f.msg, field for
+    # field in message order (the generated C++ struct layout: 56-byte nodes)
+    node_fields = [("mean", C.c_float * 3), ("direction", C.c_float * 3), ("idx_start", C.c_uint32),
+                   ("idx_end", C.c_uint32), ("idx_left", C.c_int32), ("idx_right", C.c_int32),
+                   ("dts_mean", C.c_double), ("dts_covariance", C.c_double)]
+    assert [(n, C.sizeof(t)) for n, t in L.KDNode3f._fields_] == [(n, C.sizeof(t)) for n, t in node_fields]
+    assert C.sizeof(L.KDNode3f) == 56 and L.KDNode3f.dts_mean.offset == 40
+    assert L.KDNODE3F_DTYPE.itemsize == 56
+    assert all(L.KDNODE3F_DTYPE.fields[n][1] == getattr(L.KDNode3f, n).offset for n, _ in node_fields)
+    assert C.sizeof(L.KDTree3f) == 88 and L.KDTree3f.num_nodes.offset == 72
 
 
 def test_defaults_match_reference_params():

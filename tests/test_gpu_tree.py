@@ -26,6 +26,9 @@ def assert_same_tree(O, G):
         assert np.array_equal(eo[k].view(np.uint64), eg[k].view(np.uint64)), k
     assert eo["ts_start"] == eg["ts_start"]
     assert G.info.num_unpruned == eo["num_unpruned"]
+    ro, rg = O.root(), G.root()  # Tree_::root_* as TreeCPU_'s constructor sets them
+    for k in ("root_mean", "root_eigenvalues", "root_eigenvectors"):
+        assert np.array_equal(ro[k].view(np.uint32), rg[k].view(np.uint32)), k
 
 
 @pytest.mark.parametrize("seed,beams,params", [

@@ -210,3 +210,16 @@ def test_fixed_point_floor_is_exact():
     for v in vals:
         want = math.floor(Fraction(v) * (1 << 64))
         assert orc.fx_floor(v) == want, v
+
+
+def test_voxel_restatement_known_answer():
+    """Two points in one 1 m voxel and one alone; the mean is the float sum times the
+    float reciprocal of the count; a voxel whose mean falls inside range_min is dropped."""
+    from oracle import voxel as OV
+    xyz = np.array([[2.25, 0.5, 0.0], [2.75, 0.25, 0.0], [5.5, 5.5, 1.0], [0.1, 0.1, 0.0]], np.float32)
+    st = np.array([1.0, 2.0, 3.0, 4.0])
+    p, t = OV.voxelize(xyz, st, range_min=0.5, range_max=20.0, space_res=1.0)
+    assert p.tolist() == [[2.5, 0.375, 0.0], [5.5, 5.5, 1.0]]
+    assert t.tolist() == [1.5, 3.0]
+    p, t = OV.voxelize(xyz, st, range_min=0.5, range_max=20.0)  # no grid: range filter only
+    assert len(p) == 3 and t.tolist() == [1.0, 2.0, 3.0]

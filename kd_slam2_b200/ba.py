@@ -122,11 +122,35 @@ def make_workload(seed: int = 4, num_keyframes: int = 200, radius: float = 30.0,
     return wl
 
 
-def build_trees(wl: Workload, tree_params: dict, stream=None):
-    """All keyframe trees in one batched build pass (stamps kept: CT pairs deskew)."""
-    from . import TreeGeneratorB2003D
-    gen = TreeGeneratorB2003D(**tree_params)
-    return gen.make_trees([(kf.xyz, kf.stamps) for kf in wl.keyframes], stream=stream)
+def build_trees(wl: Workload, tree_params: dict, stream=None, inputs=None):
+    """All keyframe trees in one batched build pass (stamps kept: CT pairs deskew).
+    inputs: the keyframes already on the device, as returned by device_inputs (the pass
+    then reads device memory); otherwise the host arrays are gathered and copied."""
+    import ctypes as C
+
+    from . import Tree, TreeGeneratorB2003D, _check, lib, tree_params as tp
+    from .abi import KDS_MEM_DEVICE, KDS_OK
+    if inputs is None:
+        gen = TreeGeneratorB2003D(**tree_params)
+        return gen.make_trees([(kf.xyz, kf.stamps) for kf in wl.keyframes], stream=stream)
+    xyz, st, off = inputs
+    R = len(off) - 1
+    hs = (C.c_void_p * R)()
+    status = (C.c_int32 * R)()
+    prm = tp(**tree_params)
+    _check(lib().kds_tree_build_batch(xyz.data_ptr(), st.data_ptr(), off.ctypes.data, R, KDS_MEM_DEVICE,
+                                      C.byref(prm), stream, hs, status), "kds_tree_build_batch")
+    return [Tree(hs[i]) if status[i] == KDS_OK else None for i in range(R)]
+
+
+def device_inputs(wl: Workload):
+    """The keyframes' points and stamps back to back in device memory, with their offsets."""
+    import torch
+    xyz = torch.from_numpy(np.ascontiguousarray(np.concatenate([kf.xyz for kf in wl.keyframes]))).cuda()
+    st = torch.from_numpy(np.ascontiguousarray(np.concatenate([kf.stamps for kf in wl.keyframes]))).cuda()
+    off = np.zeros(len(wl.keyframes) + 1, np.int64)
+    off[1:] = np.cumsum([len(kf.xyz) for kf in wl.keyframes])
+    return xyz, st, off
 
 
 def jobs(wl: Workload, trees, icp_params: dict, ct_params: dict):

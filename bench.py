@@ -295,21 +295,22 @@ def batched_ba(steps: int):
     sample = list(range(0, len(jobs), max(1, len(jobs) // 200)))
     aligners = {0: kds.ICPB2003D(**ICP), 1: kds.CTICPB2003D(**CT)}
     same = True
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for k in sample:
-        p = wl.pairs[k]
-        a = aligners[p.kind]
-        a.set_fixed(trees[p.i])
-        a.set_moving(trees[p.j])
-        a.set_x(p.X0)
-        if p.kind == 1:
-            a.set_fixed_velocities(wl.keyframes[p.i].vel)
-            a.set_velocities(wl.keyframes[p.j].vel)
-        r = a.compute()
-        same = same and r == res[k].result and np.array_equal(np.asarray(a.get_x()).reshape(12),
-                                                              np.array(res[k].X[:]))
-    plain_s = (time.perf_counter() - t0) / len(sample)
+    for rep in range(2):  # the first pass grows the aligners' workspaces; the second is timed
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in sample:
+            p = wl.pairs[k]
+            a = aligners[p.kind]
+            a.set_fixed(trees[p.i])
+            a.set_moving(trees[p.j])
+            a.set_x(p.X0)
+            if p.kind == 1:
+                a.set_fixed_velocities(wl.keyframes[p.i].vel)
+                a.set_velocities(wl.keyframes[p.j].vel)
+            r = a.compute()
+            same = same and r == res[k].result and np.array_equal(np.asarray(a.get_x()).reshape(12),
+                                                                  np.array(res[k].X[:]))
+        plain_s = (time.perf_counter() - t0) / len(sample)
     n = [len(k.xyz) for k in wl.keyframes]
     errs = np.array([pose_err(np.array(res[k].X[:]), wl.pairs[k].X_true) for k in range(len(jobs))])
     return {

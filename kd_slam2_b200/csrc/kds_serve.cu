@@ -215,7 +215,6 @@ struct kds_server {
   bool started = false, stopping = false;
   int device = 0;
   cudaStream_t sA = nullptr, sB = nullptr;  // Gauss-Newton (high priority), builds
-  cudaStream_t sC = nullptr;                // copies of the next build pass's points
   std::thread th_build, th_gn;
   int thread_error = KDS_OK;
   char thread_error_text[256] = {0};
@@ -354,273 +353,193 @@ int finish_request(kds_server* s, Request* r, cudaStream_t stream, const float* 
 // One build thread: each pass takes the pending map rebuilds first (they unblock whole
 // windows), then admits arrived requests.  (Two build passes running concurrently on
 // separate streams each take the whole GPU and slowed each other down.)
-// One build pass: the map rebuilds and requests it takes, and its device copy of their points.
-struct Pass {
+void build_loop(kds_server* s) {
+  const cudaStream_t bst = s->sB;
+  cudaSetDevice(s->device);
   std::vector<Request*> batch;
   std::vector<MapTask> maps;
-  int64_t transient = 0;  // workspace bytes reserved for the pass
-  std::vector<int64_t> off;
-  std::shared_ptr<Batch> B;
-  int64_t h2d = 0;
-  cudaEvent_t staged = nullptr;  // the pass's copies are done
-};
-
-// Takes the next pass under the lock: pending map rebuilds first (not held under the cap),
-// then arrived requests in arrival order while their device bytes fit under the cap.
-// wait: block until there is work; otherwise return false at once when there is none.
-// requests: take requests at all (false: a pass of map rebuilds only).
-// Returns false when there is no pass (or the server stops).
-bool admit_pass(kds_server* s, Pass& P, bool wait, bool requests) {
-  std::vector<Request*>& batch = P.batch;
-  std::vector<MapTask>& maps = P.maps;
-  std::unique_lock<std::mutex> lk(s->mu);
   for (;;) {
-    if (s->stopping) return false;
-    const double now = seconds_since(s->t0);
-    while (!s->map_tasks.empty() && (int)maps.size() < s->P.max_build_trees) {
-      maps.push_back(s->map_tasks.front());
-      s->map_tasks.pop_front();
-    }
-    int64_t pts = 0;  // points of the pass; the maps' share is not held under the cap
-    for (auto& m : maps) pts += m.points;
-    int64_t rpts = 0;  // request points of the pass
-    double next_arrival = -1.0;
-    while (requests && !s->pending.empty() && (int)(batch.size() + maps.size()) < s->P.max_build_trees) {
-      Request* r = s->pending.front();
-      if (r->in.arrival > now) {
-        next_arrival = r->in.arrival;
-        break;
-      }
-      if (!batch.empty() && pts + r->in.n > s->P.max_build_points) break;
-      const int64_t need = request_persistent_bytes(r->in);
-      const int64_t ws = (int64_t)forest_workspace_bytes(rpts + r->in.n, (int)batch.size() + 1);
-      if (s->reserved + need + ws > s->cap) {
-        if (s->reserved == 0 && batch.empty()) {
-          // can never fit: refused at admission, finishes with its initial guess
-          s->pending.pop_front();
-          r->res.status = KDS_ERR_ADMISSION;
-          memcpy(r->res.X, r->in.X0, sizeof(r->res.X));
-          memcpy(r->res.v, r->in.v0, sizeof(r->res.v));
-          if (window_progress(s, r, false)) {
-            lk.unlock();
-            fail_thread(s, KDS_ERR_CUDA);
-            return false;
-          }
-          r->res.t_done = seconds_since(s->t0);
-          r->done = true;
-          ++s->completed;
-          s->cv_done.notify_all();
-          continue;
+    batch.clear();
+    maps.clear();
+    int64_t transient = 0;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      for (;;) {
+        if (s->stopping) return;
+        const double now = seconds_since(s->t0);
+        // map rebuilds first; they are not held under the cap
+        while (!s->map_tasks.empty() && (int)maps.size() < s->P.max_build_trees) {
+          maps.push_back(s->map_tasks.front());
+          s->map_tasks.pop_front();
         }
-        break;
-      }
-      s->pending.pop_front();
-      r->reserved = need;
-      s->reserved += need;
-      r->res.t_admit = now;
-      batch.push_back(r);
-      pts += r->in.n;
-      rpts += r->in.n;
-    }
-    if (!batch.empty() || !maps.empty()) {
-      P.transient = batch.empty() ? 0 : (int64_t)forest_workspace_bytes(rpts, (int)batch.size());
-      s->reserved += P.transient;
-      s->peak_reserved = std::max(s->peak_reserved, s->reserved);
-      return true;
-    }
-    if (!wait) return false;
-    if (next_arrival > 0.0)
-      s->cv_build.wait_for(lk, std::chrono::duration<double>(std::max(0.0, next_arrival - now)));
-    else
-      s->cv_build.wait(lk);
-  }
-}
-
-// Allocates the pass's point block and queues the copies of its points on the copy
-// stream cs: map windows device to device, request points from wherever they live.
-int stage_pass(kds_server* s, Pass& P, cudaStream_t cs) {
-  const int R = (int)(P.maps.size() + P.batch.size());
-  P.off.assign(R + 1, 0);
-  for (int i = 0; i < (int)P.maps.size(); ++i) P.off[i + 1] = P.off[i] + P.maps[i].points;
-  for (int i = 0; i < (int)P.batch.size(); ++i)
-    P.off[P.maps.size() + i + 1] = P.off[P.maps.size() + i] + P.batch[i]->in.n;
-  const int64_t N = P.off[R];
-  P.B = std::make_shared<Batch>();
-  P.B->bytes = 12 * N + 8 * N + 512;
-  if (N > 0) {
-    cudaError_t e = cudaMallocAsync(&P.B->block, (size_t)P.B->bytes, cs);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      set_error("served build: cudaMallocAsync of %lld bytes failed", (long long)P.B->bytes);
-      return KDS_ERR_OOM;
-    }
-  }
-  float* bx = (float*)P.B->block;
-  double* bs = (double*)((char*)P.B->block + ((12 * N + 255) & ~(int64_t)255));
-  P.B->xyz = bx;
-  P.B->stamps = bs;
-  for (int i = 0; i < (int)P.maps.size(); ++i) {
-    const MapTask& m = P.maps[i];
-    const float* win = s->streams[m.stream].win[(m.version - 1) % 2];
-    cudaError_t e = cudaStreamWaitEvent(cs, m.ready, 0);
-    int64_t o = P.off[i];
-    for (size_t g = 0; e == cudaSuccess && g < m.ranges.size(); ++g) {
-      e = cudaMemcpyAsync(bx + 3 * o, win + 3 * m.ranges[g].first, 12 * m.ranges[g].second,
-                          cudaMemcpyDeviceToDevice, cs);
-      o += m.ranges[g].second;
-    }
-    if (e == cudaSuccess && m.points > 0) e = cudaMemsetAsync(bs + P.off[i], 0, 8 * m.points, cs);
-    if (e != cudaSuccess) return cuda_status(e, "served build: map copy", __FILE__, __LINE__);
-  }
-  for (int i = 0; i < (int)P.batch.size(); ++i) {
-    Request* r = P.batch[i];
-    const int64_t o = P.off[P.maps.size() + i];
-    cudaError_t e = cudaMemcpyAsync(bx + 3 * o, r->in.xyz, 12 * r->in.n, cudaMemcpyDefault, cs);
-    if (e == cudaSuccess)
-      e = r->in.stamps ? cudaMemcpyAsync(bs + o, r->in.stamps, 8 * r->in.n, cudaMemcpyDefault, cs)
-                       : cudaMemsetAsync(bs + o, 0, 8 * r->in.n, cs);
-    if (e != cudaSuccess) return cuda_status(e, "served build: point copy", __FILE__, __LINE__);
-    if (r->host_input) P.h2d += (r->in.stamps ? 20 : 12) * r->in.n;
-  }
-  KDS_CK(cudaEventCreateWithFlags(&P.staged, cudaEventDisableTiming));
-  KDS_CK(cudaEventRecord(P.staged, cs));
-  return KDS_OK;
-}
-
-// Builds a staged pass on the build stream and hands its trees out.
-int build_pass(kds_server* s, Pass& P) {
-  const cudaStream_t bst = s->sB;
-  const auto pass_t0 = std::chrono::steady_clock::now();
-  std::vector<Request*>& batch = P.batch;
-  std::vector<MapTask>& maps = P.maps;
-  const int R = (int)(maps.size() + batch.size());
-  const std::vector<int64_t>& off = P.off;
-  const int64_t N = off[R];
-  auto B = P.B;
-  int rc = KDS_OK;
-  {
-    cudaError_t e = cudaStreamWaitEvent(bst, P.staged, 0);
-    cudaEventDestroy(P.staged);
-    P.staged = nullptr;
-    if (e != cudaSuccess) rc = cuda_status(e, "served build: wait for copies", __FILE__, __LINE__);
-  }
-  std::vector<kds_tree*> trees(R, nullptr);
-  std::vector<int32_t> status(R, KDS_ERR_TREE_REJECTED);
-  if (rc == KDS_OK && N > 0)
-    rc = tree_build_forest(B->xyz, B->stamps, off.data(), R, KDS_MEM_DEVICE, &s->P.tree, bst, trees.data(),
-                           status.data());
-  if (rc == KDS_OK) {
-    cudaError_t e = cudaStreamSynchronize(bst);
-    if (e != cudaSuccess) rc = cuda_status(e, "served build", __FILE__, __LINE__);
-  }
-  if (rc != KDS_OK) return rc;
-  std::lock_guard<std::mutex> g(s->mu);
-  s->reserved -= P.transient;
-  s->h2d_bytes += P.h2d;
-  ++s->build_passes;
-  s->build_ms += 1e3 * seconds_since(pass_t0);
-  s->build_points += N;
-  {
-    int depth = 0;  // levels of the pass (the same for every tree it built)
-    for (auto* t : trees)
-      if (t) depth = std::max(depth, (int)t->d.depth);
-    s->build_point_levels += (double)N * depth;
-  }
-  {
-    const double t1 = seconds_since(s->t0);
-    s->trace.push_back({0.0, (double)N, t1 - seconds_since(pass_t0), t1});
-  }
-  s->built_trees += R;
-  for (int i = 0; i < (int)maps.size(); ++i) {
-    cudaEventDestroy(maps[i].ready);
-    ++s->map_builds;
-    // a rejected map keeps the previous version in service
-    if (trees[i]) install_map(s, maps[i].stream, maps[i].version, trees[i]);
-    else {
-      StreamState& st = s->streams[maps[i].stream];
-      auto it = st.maps.find(st.installed);
-      if (it != st.maps.end()) {
-        MapVersion alias = it->second;
-        st.maps.erase(it);
-        st.maps[maps[i].version] = alias;
-        st.installed = maps[i].version;
+        int64_t pts = 0;  // points of the pass; the maps' share is not held under the cap
+        for (auto& m : maps) pts += m.points;
+        int64_t rpts = 0;  // request points of the pass
+        double next_arrival = -1.0;
+        while (!s->pending.empty() && (int)(batch.size() + maps.size()) < s->P.max_build_trees) {
+          Request* r = s->pending.front();
+          if (r->in.arrival > now) {
+            next_arrival = r->in.arrival;
+            break;
+          }
+          if (!batch.empty() && pts + r->in.n > s->P.max_build_points) break;
+          const int64_t need = request_persistent_bytes(r->in);
+          const int64_t ws = (int64_t)forest_workspace_bytes(rpts + r->in.n, (int)batch.size() + 1);
+          if (s->reserved + need + ws > s->cap) {
+            if (s->reserved == 0 && batch.empty()) {
+              // can never fit: refused at admission, finishes with its initial guess
+              s->pending.pop_front();
+              r->res.status = KDS_ERR_ADMISSION;
+              memcpy(r->res.X, r->in.X0, sizeof(r->res.X));
+              memcpy(r->res.v, r->in.v0, sizeof(r->res.v));
+              if (window_progress(s, r, false)) {
+                lk.unlock();
+                fail_thread(s, KDS_ERR_CUDA);
+                return;
+              }
+              r->res.t_done = seconds_since(s->t0);
+              r->done = true;
+              ++s->completed;
+              s->cv_done.notify_all();
+              continue;
+            }
+            break;
+          }
+          s->pending.pop_front();
+          r->reserved = need;
+          s->reserved += need;
+          r->res.t_admit = now;
+          batch.push_back(r);
+          pts += r->in.n;
+          rpts += r->in.n;
+        }
+        if (!batch.empty() || !maps.empty()) {
+          transient = batch.empty() ? 0 : (int64_t)forest_workspace_bytes(rpts, (int)batch.size());
+          s->reserved += transient;
+          s->peak_reserved = std::max(s->peak_reserved, s->reserved);
+          break;
+        }
+        if (next_arrival > 0.0)
+          s->cv_build.wait_for(lk, std::chrono::duration<double>(std::max(0.0, next_arrival - now)));
+        else
+          s->cv_build.wait(lk);
       }
     }
-  }
-  B->refs = (int)batch.size();
-  const double now = seconds_since(s->t0);
-  for (int i = 0; i < (int)batch.size(); ++i) {
-    Request* r = batch[i];
-    r->built = true;
-    r->res.t_built = now;
-    r->batch = B;
-    r->batch_off = off[maps.size() + i];
-    r->build_status = status[maps.size() + i];
-    r->tree = trees[maps.size() + i];
-    if (r->tree) {
-      const int64_t actual = 20 * r->in.n + tree_bytes(r->tree->d);
-      s->reserved += actual - r->reserved;
-      r->reserved = actual;
+    // one forest pass over the maps and the admitted requests
+    const auto pass_t0 = std::chrono::steady_clock::now();
+    const int R = (int)(maps.size() + batch.size());
+    std::vector<int64_t> off(R + 1, 0);
+    for (int i = 0; i < (int)maps.size(); ++i) off[i + 1] = off[i] + maps[i].points;
+    for (int i = 0; i < (int)batch.size(); ++i) off[maps.size() + i + 1] = off[maps.size() + i] + batch[i]->in.n;
+    const int64_t N = off[R];
+    auto B = std::make_shared<Batch>();
+    B->bytes = 12 * N + 8 * N + 512;
+    int rc = KDS_OK;
+    if (N > 0) {
+      cudaError_t e = cudaMallocAsync(&B->block, (size_t)B->bytes, bst);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("served build: cudaMallocAsync of %lld bytes failed", (long long)B->bytes);
+        fail_thread(s, KDS_ERR_OOM);
+        return;
+      }
     }
-    s->ready.push_back(r);
-  }
-  if (B->refs == 0 && B->block) {
-    cudaFreeAsync(B->block, bst);
-    B->block = nullptr;
-  }
-  s->cv_gn.notify_all();
-  return KDS_OK;
-}
-
-// Build thread: one pass ahead.  While a pass builds on the build stream, the next
-// pass of requests is admitted and its points copied on the copy stream, so the copies
-// of host inputs overlap the builds.  Map rebuilds (which the next windows wait for)
-// go before a staged pass of requests.  Each tree is the same whatever pass builds it.
-void build_loop(kds_server* s) {
-  cudaSetDevice(s->device);
-  Pass staged;  // admitted and copied, not built yet
-  bool have = false;
-  int rc = KDS_OK;
-  while (rc == KDS_OK) {
-    Pass cur;
-    bool maps_first = false;
-    if (have) {
+    float* bx = (float*)B->block;
+    double* bs = (double*)((char*)B->block + ((12 * N + 255) & ~(int64_t)255));
+    B->xyz = bx;
+    B->stamps = bs;
+    for (int i = 0; rc == KDS_OK && i < (int)maps.size(); ++i) {
+      const MapTask& m = maps[i];
+      const float* win = s->streams[m.stream].win[(m.version - 1) % 2];
+      cudaError_t e = cudaStreamWaitEvent(bst, m.ready, 0);
+      int64_t o = off[i];
+      for (size_t g = 0; e == cudaSuccess && g < m.ranges.size(); ++g) {
+        e = cudaMemcpyAsync(bx + 3 * o, win + 3 * m.ranges[g].first, 12 * m.ranges[g].second,
+                            cudaMemcpyDeviceToDevice, bst);
+        o += m.ranges[g].second;
+      }
+      if (e == cudaSuccess && m.points > 0) e = cudaMemsetAsync(bs + off[i], 0, 8 * m.points, bst);
+      if (e != cudaSuccess) rc = cuda_status(e, "served build: map copy", __FILE__, __LINE__);
+    }
+    int64_t h2d = 0;
+    for (int i = 0; rc == KDS_OK && i < (int)batch.size(); ++i) {
+      Request* r = batch[i];
+      const int64_t o = off[maps.size() + i];
+      cudaError_t e = cudaMemcpyAsync(bx + 3 * o, r->in.xyz, 12 * r->in.n, cudaMemcpyDefault, bst);
+      if (e == cudaSuccess)
+        e = r->in.stamps ? cudaMemcpyAsync(bs + o, r->in.stamps, 8 * r->in.n, cudaMemcpyDefault, bst)
+                         : cudaMemsetAsync(bs + o, 0, 8 * r->in.n, bst);
+      if (e != cudaSuccess) rc = cuda_status(e, "served build: point copy", __FILE__, __LINE__);
+      if (r->host_input) h2d += (r->in.stamps ? 20 : 12) * r->in.n;
+    }
+    std::vector<kds_tree*> trees(R, nullptr);
+    std::vector<int32_t> status(R, KDS_ERR_TREE_REJECTED);
+    if (rc == KDS_OK && N > 0)
+      rc = tree_build_forest(bx, bs, off.data(), R, KDS_MEM_DEVICE, &s->P.tree, bst, trees.data(), status.data());
+    if (rc == KDS_OK) {
+      cudaError_t e = cudaStreamSynchronize(bst);
+      if (e != cudaSuccess) rc = cuda_status(e, "served build", __FILE__, __LINE__);
+    }
+    if (rc != KDS_OK) {
+      fail_thread(s, rc);
+      return;
+    }
+    {
       std::lock_guard<std::mutex> g(s->mu);
-      maps_first = !s->map_tasks.empty();
-    }
-    if (maps_first) {
-      if (!admit_pass(s, cur, false, false)) break;
-      rc = stage_pass(s, cur, s->sC);
-    } else if (have) {
-      cur = std::move(staged);
-      staged = Pass();
-      have = false;
-    } else {
-      if (!admit_pass(s, cur, true, true)) break;
-      rc = stage_pass(s, cur, s->sC);
-    }
-    if (rc != KDS_OK) break;
-    if (!have) {  // the next pass of requests, staged while this one builds
-      if (admit_pass(s, staged, false, true)) {
-        have = true;
-        rc = stage_pass(s, staged, s->sC);
-        if (rc != KDS_OK) break;
-      } else if (s->stopping) {
-        break;
+      s->reserved -= transient;
+      s->h2d_bytes += h2d;
+      ++s->build_passes;
+      s->build_ms += 1e3 * seconds_since(pass_t0);
+      s->build_points += N;
+      {
+        int depth = 0;  // levels of the pass (the same for every tree it built)
+        for (auto* t : trees)
+          if (t) depth = std::max(depth, (int)t->d.depth);
+        s->build_point_levels += (double)N * depth;
       }
-    }
-    rc = build_pass(s, cur);
-  }
-  if (rc != KDS_OK) fail_thread(s, rc);
-  // a pass admitted but not built when the server stops: its copies may still run
-  if (have) {
-    if (staged.staged) {
-      cudaEventSynchronize(staged.staged);
-      cudaEventDestroy(staged.staged);
-    }
-    if (staged.B && staged.B->block) {
-      cudaFreeAsync(staged.B->block, s->sC);
-      staged.B->block = nullptr;
+      {
+        const double t1 = seconds_since(s->t0);
+        s->trace.push_back({0.0, (double)N, t1 - seconds_since(pass_t0), t1});
+      }
+      s->built_trees += R;
+      for (int i = 0; i < (int)maps.size(); ++i) {
+        cudaEventDestroy(maps[i].ready);
+        ++s->map_builds;
+        // a rejected map keeps the previous version in service
+        if (trees[i]) install_map(s, maps[i].stream, maps[i].version, trees[i]);
+        else {
+          StreamState& st = s->streams[maps[i].stream];
+          auto it = st.maps.find(st.installed);
+          if (it != st.maps.end()) {
+            MapVersion alias = it->second;
+            st.maps.erase(it);
+            st.maps[maps[i].version] = alias;
+            st.installed = maps[i].version;
+          }
+        }
+      }
+      B->refs = (int)batch.size();
+      const double now = seconds_since(s->t0);
+      for (int i = 0; i < (int)batch.size(); ++i) {
+        Request* r = batch[i];
+        r->built = true;
+        r->res.t_built = now;
+        r->batch = B;
+        r->batch_off = off[maps.size() + i];
+        r->build_status = status[maps.size() + i];
+        r->tree = trees[maps.size() + i];
+        if (r->tree) {
+          const int64_t actual = 20 * r->in.n + tree_bytes(r->tree->d);
+          s->reserved += actual - r->reserved;
+          r->reserved = actual;
+        }
+        s->ready.push_back(r);
+      }
+      if (B->refs == 0 && B->block) {
+        cudaFreeAsync(B->block, bst);
+        B->block = nullptr;
+      }
+      s->cv_gn.notify_all();
     }
   }
 }
@@ -1068,7 +987,6 @@ int kds_server_create(const kds_server_params* params, kds_server** out) {
   KDS_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
   KDS_CK(cudaStreamCreateWithPriority(&s->sA, cudaStreamNonBlocking, hi));
   KDS_CK(cudaStreamCreateWithPriority(&s->sB, cudaStreamNonBlocking, lo));
-  KDS_CK(cudaStreamCreateWithPriority(&s->sC, cudaStreamNonBlocking, lo));
   size_t fr = 0, tot = 0;
   KDS_CK(cudaMemGetInfo(&fr, &tot));
   const int64_t avail = (int64_t)(fr * 0.9);
@@ -1317,7 +1235,6 @@ void kds_server_free(kds_server* s) {
   if (s->th_gn.joinable()) s->th_gn.join();
   cudaStreamSynchronize(s->sA);
   cudaStreamSynchronize(s->sB);
-  cudaStreamSynchronize(s->sC);
   for (auto& r : s->reqs) {
     if (r->tree) kds_tree_free(r->tree);
     if (r->batch && r->batch->block) {
@@ -1352,7 +1269,6 @@ void kds_server_free(kds_server* s) {
   }
   cudaStreamDestroy(s->sA);
   cudaStreamDestroy(s->sB);
-  if (s->sC) cudaStreamDestroy(s->sC);
   cudaGetLastError();
   delete s;
 }

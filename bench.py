@@ -470,13 +470,21 @@ def main():
     # ---- the plain drop-in on the same trace
     plain = None
     if not args.no_plain:
-        p_ms, p_res, _ = serve_step(dev_inputs, serial=1)
+        serve_step(dev_inputs, serial=1)  # warm-up: the serial path's aligners grow their workspaces
+        # the serial step's time varies from run to run (210-540 alignments/s seen on one box);
+        # the fastest of three is reported, which keeps served_over_plain conservative
+        p_runs = [serve_step(dev_inputs, serial=1) for _ in range(3)]
+        p_all = [float(r[0]) for r in p_runs]
+        p_ms = min(p_all)
+        p_res = p_runs[-1][1]
         p_val = n_req / (p_ms / 1e3)
         same = all(np.array_equal(a["X"], b["X"]) and a["result"] == b["result"] for a, b in zip(served, p_res))
         lat_p, _, _ = streams.serve(poi, serial=True, tree=TREE, icp=ICP, ct=CT, map_every=MAP_EVERY,
                                     timeout=600.0)
         latp = np.array([1e3 * (q["t_done"] - q["t_arrival"]) for q in lat_p])
-        plain = {"value": p_val, "unit": UNIT, "ms_per_step": p_ms, "served_over_plain": value / world / p_val,
+        plain = {"value": p_val, "unit": UNIT, "ms_per_step": p_ms, "ms_per_step_all": p_all,
+                 "reported": "fastest of %d timed steps after 1 warm-up" % len(p_runs),
+                 "served_over_plain": value / world / p_val,
                  "results_identical_to_served": bool(same),
                  "latency_ms_poisson": {"p50": float(np.percentile(latp, 50)), "p99": float(np.percentile(latp, 99))}}
 

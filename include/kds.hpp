@@ -110,6 +110,22 @@ class Tree {
     check(kds_tree_extract_compressed_leaves(_t, nullptr, out.data(), nullptr), "kds_tree_extract_compressed_leaves");
     return out;
   }
+  // toMessage (lib/kd_io/slam_messages.h:47-80): the tree fields of a KDTree3f message;
+  // the node records are written to `nodes`, which the returned struct points into.
+  kds_kdtree3f toMessage(std::vector<kds_kdnode3f>& nodes) const {
+    kds_kdtree3f m{};
+    check(kds_tree_to_msg(_t, &m), "kds_tree_to_msg");  // node count
+    nodes.resize((size_t)m.num_nodes);
+    m.nodes = nodes.data();
+    check(kds_tree_to_msg(_t, &m), "kds_tree_to_msg");
+    return m;
+  }
+  // TreeLoader_::fromTreeMsg (lib/kd_io/tree_loader_impl_.h:59-70): a device tree without points
+  static std::shared_ptr<Tree> fromTreeMsg(const kds_kdtree3f& m) {
+    kds_tree* t = nullptr;
+    check(kds_tree_from_msg(&m, &t), "kds_tree_from_msg");
+    return std::make_shared<Tree>(t);
+  }
 
  private:
   kds_tree* _t;

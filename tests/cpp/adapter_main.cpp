@@ -69,8 +69,13 @@ static int align_mode(char** argv) {
   read_cloud(argv[3], xf, sf);
   read_cloud(argv[4], xm, sm);
   TreePtr fixed = gen.makeTree(xf.data(), sf.data(), (int64_t)sf.size());
-  TreePtr moving = gen.makeTree(xm.data(), sm.data(), (int64_t)sm.size());
-  if (!fixed || !moving) throw std::runtime_error("tree rejected");
+  TreePtr built = gen.makeTree(xm.data(), sm.data(), (int64_t)sm.size());
+  if (!fixed || !built) throw std::runtime_error("tree rejected");
+  // the moving tree goes through the tree wire format (toMessage / fromTreeMsg): the
+  // alignment must not change
+  std::vector<kds_kdnode3f> records;
+  const kds_kdtree3f msg = built->toMessage(records);
+  TreePtr moving = Tree::fromTreeMsg(msg);
   CTICPB2003D a;
   ConfReader::configure(a, *find_type(objs, "CTICPB2003D"), objs);
   a.setFixed(*fixed);

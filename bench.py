@@ -311,6 +311,24 @@ def batched_ba(steps: int):
             same = same and r == res[k].result and np.array_equal(np.asarray(a.get_x()).reshape(12),
                                                                   np.array(res[k].X[:]))
         plain_s = (time.perf_counter() - t0) / len(sample)
+    # one solver step: every factor linearized at the keyframes' estimates (rigid:
+    # buildQuadraticForm, CT: buildQuadraticFormDual), then the factors' block updates
+    # assembled on the device (disable_inlier_ratio 0.3, the map's default)
+    fjobs, factors, nv = ba.factor_jobs(wl, trees, ICP, CT)
+    fb = kds.Batch()
+    fb.run(fjobs)
+    fb.run(fjobs)  # the second run captures the graph
+    lin_t, asm_t = [], []
+    for _ in range(max(1, steps)):
+        torch.cuda.synchronize()
+        e0.record()
+        fb.run(fjobs)
+        e1.record()
+        e1.synchronize()
+        lin_t.append(e0.elapsed_time(e1))
+        t0 = time.perf_counter()
+        brc, _, _, ben = fb.assemble(factors, nv, disable_inlier_ratio=0.3)
+        asm_t.append(1e3 * (time.perf_counter() - t0))
     n = [len(k.xyz) for k in wl.keyframes]
     errs = np.array([pose_err(np.array(res[k].X[:]), wl.pairs[k].X_true) for k in range(len(jobs))])
     return {
@@ -325,6 +343,63 @@ def batched_ba(steps: int):
         "results_identical_to_plain": bool(same), "autotune_config": int(chosen),
         "autotune_ms": [float(x) for x in tune_ms],
         "median_t_err_vs_truth_m": float(np.median(errs[:, 0])), "median_r_err_vs_truth_rad": float(np.median(errs[:, 1])),
+        "factor_step": {"factors": len(factors), "variables": nv, "blocks": int(len(brc)),
+                        "enabled": int(np.sum(ben)), "linearize_ms": float(np.mean(lin_t)),
+                        "assemble_ms": float(np.mean(asm_t)),
+                        "note": "linearize: one graph-replayed batch with results read back; assemble: "
+                                "kds_batch_assemble wall time (block layout on the host, sums on the "
+                                "device, blocks read back)"},
+    }
+
+
+def scan_input(steps: int):
+    """The scan input stage and the tree wire format on full-size sweeps: toPointsVector +
+    Voxelizer_::voxelize on the device (kds_points_voxelize, device-resident inputs) over
+    eight 128 x 2048 sweeps, and a KDTree3f round trip (kds_tree_to_msg / from_msg) of the
+    tree built from one of them."""
+    import torch
+
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import synth
+    boxes = synth.scene(1003)
+    scans = []
+    for k in range(8):
+        X = synth.pose((-4.0 + k, 0.0, 1.8))
+        xyz, st = synth.scan(boxes, X, beams=128, cols=2048, elev=(-22.5, 22.5), seed=7000 + k, threads=16)
+        scans.append((torch.from_numpy(xyz).cuda(), torch.from_numpy(st).cuda()))
+    prm = dict(range_min=1.0, range_max=100.0, space_res=0.1)
+    for x, s_ in scans[:2]:
+        kds.voxelize(x, s_, **prm)  # warm-up
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times, kept = [], 0
+    for _ in range(max(1, steps)):
+        torch.cuda.synchronize()
+        e0.record()
+        kept = 0
+        for x, s_ in scans:
+            ox, _ = kds.voxelize(x, s_, **prm)
+            kept += len(ox)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    pts = sum(len(x) for x, _ in scans)
+    ms = float(np.mean(times))
+    gx, gs = kds.voxelize(*scans[0], **prm)
+    T = kds.TreeGeneratorB2003D(**TREE).make_tree(gx.cpu().numpy(), gs.cpu().numpy())
+    t0 = time.perf_counter()
+    msg = T.to_msg()
+    t1 = time.perf_counter()
+    U = kds.Tree.from_msg(msg)
+    t2 = time.perf_counter()
+    et, eu = T.export(), U.export()
+    same = all(np.array_equal(et[k], eu[k]) for k in ("mean", "dir", "dts_mean", "dts_cov", "start", "end", "left",
+                                                        "right", "leaves"))
+    return {
+        "voxelize": {"scans": len(scans), "points": int(pts), "kept_voxels": int(kept), "params": prm,
+                     "ms": ms, "points_per_s": pts / (ms / 1e3),
+                     "note": "kds_points_voxelize per sweep, device inputs and outputs, CUDA events around the 8 calls"},
+        "tree_message": {"nodes": int(T.num_nodes), "bytes": int(msg["nodes"].nbytes), "to_msg_ms": 1e3 * (t1 - t0),
+                         "from_msg_ms": 1e3 * (t2 - t1), "round_trip_identical": bool(same)},
     }
 
 
@@ -514,6 +589,7 @@ def main():
     }
     if rank == 0 and not args.no_ba:
         line["batched_ba"] = batched_ba(args.steps)
+        line["scan_input"] = scan_input(args.steps)
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = min(os.cpu_count() or 1, 8)
         line["cpu_baseline"] = cpu_baseline_leg(sat, served, threads)

@@ -53,3 +53,22 @@ def test_assembly_rejects_bad_factors():
         with pytest.raises(KdsError) as e:
             B.assemble(bad, 8)
         assert e.value.code == KDS_ERR_INVALID_ARG
+
+
+def test_assembly_full_ba_step():
+    """The full bundle-adjustment configuration (200 keyframes, 894 pairs, each a rigid and a
+    CT factor = 1,788 factors over 400 variables): device assembly equals the restatement."""
+    from kd_slam2_b200 import ba
+    from oracle import factors as OF
+    wl = ba.make_workload()
+    trees = ba.build_trees(wl, TREE, inputs=ba.device_inputs(wl))
+    jobs, factors, nv = ba.factor_jobs(wl, trees, ICP, CT)
+    B = kds.Batch()
+    res = B.run(jobs)
+    rc, H, b, en = B.assemble(factors, nv, disable_inlier_ratio=0.3)
+    Hr, br, enr = OF.assemble(res, factors, nv, 0.3)
+    assert len(factors) == 1788 and np.array_equal(en, enr)
+    assert [tuple(x) for x in rc] == sorted(Hr)
+    for k, (r, c) in enumerate(rc):
+        assert np.array_equal(H[k], Hr[(r, c)]), (r, c)
+    assert np.array_equal(b, br)

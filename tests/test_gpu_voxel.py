@@ -60,3 +60,16 @@ def test_voxelized_scan_builds_the_oracles_tree(scene):
     for k in ("left", "right", "start", "end", "leaves", "perm"):
         assert np.array_equal(eg[k], eo[k]), k
     assert np.array_equal(eg["mean"], eo["mean"]) and np.array_equal(eg["dir"], eo["dir"])
+
+
+def test_voxelize_full_sweep():
+    """A full 128 x 2048 sweep (about 200k returns) at the grid used by the benchmark."""
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import synth
+    boxes = synth.scene(1003)
+    xyz, st = synth.scan(boxes, synth.pose((0.0, 0.0, 1.8)), beams=128, cols=2048, elev=(-22.5, 22.5), seed=7000,
+                         threads=16)
+    prm = dict(range_min=1.0, range_max=100.0, space_res=0.1)
+    gx, gs = kds.voxelize(xyz, st, **prm)
+    ox, os_ = OV.voxelize(xyz, st, **prm)
+    assert len(xyz) > 150000 and same(gx, ox) and same(gs, os_)

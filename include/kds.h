@@ -391,7 +391,7 @@ typedef struct kds_server kds_server;
 typedef struct {
   int32_t max_slots;        /* registrations on the device at once (512) */
   int32_t map_every;        /* map rebuilt from the last map_every scans of a stream (5) */
-  int32_t max_build_trees;  /* trees per build pass (64) */
+  int32_t max_build_trees;  /* trees per build pass (128) */
   int32_t serial;           /* 1: plain drop-in, one request at a time via the per-call API (0) */
   int32_t profile;          /* 1: time the linearization launches of every tick and count the
                                fixed nodes each registration touches (0; adds work) */

@@ -959,7 +959,7 @@ void kds_server_params_default(kds_server_params* p) {
   memset(p, 0, sizeof(*p));
   p->max_slots = 512;
   p->map_every = 5;
-  p->max_build_trees = 64;
+  p->max_build_trees = 128;
   p->serial = 0;
   p->profile = 0;
   p->hbm_cap = 0;

@@ -41,7 +41,7 @@ constexpr int kLevelBlocks = 148 * 3;  // k_decide: 3 blocks per SM at its regis
 constexpr int kLevelsPerSync = 4;
 constexpr int kMaxDepth = 64;
 constexpr int kUnroll = 2;  // rounds of 32 points in flight per lane in the warp-per-node partition
-constexpr int kSmallBlocks = 148 * 8;  // short-lived blocks: other streams' kernels interleave
+constexpr int kSmallBlocks = 148 * 4;  // two waves: other streams' kernels interleave at block boundaries
 
 // ---------------------------------------------------------------------------
 // 128-bit two's complement fixed point (units of 2^-64)

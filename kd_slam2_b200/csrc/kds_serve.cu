@@ -376,8 +376,9 @@ void build_loop(kds_server* s) {
         for (auto& m : maps) pts += m.points;
         int64_t rpts = 0;  // request points of the pass
         double next_arrival = -1.0;
-        while (!s->pending.empty() && (int)(batch.size() + maps.size()) < s->P.max_build_trees) {
-          Request* r = s->pending.front();
+        auto it = s->pending.begin();
+        while (it != s->pending.end() && (int)(batch.size() + maps.size()) < s->P.max_build_trees) {
+          Request* r = *it;
           if (r->in.arrival > now) {
             next_arrival = r->in.arrival;
             break;
@@ -388,7 +389,7 @@ void build_loop(kds_server* s) {
           if (s->reserved + need + ws > s->cap) {
             if (s->reserved == 0 && batch.empty()) {
               // can never fit: refused at admission, finishes with its initial guess
-              s->pending.pop_front();
+              it = s->pending.erase(it);
               r->res.status = KDS_ERR_ADMISSION;
               memcpy(r->res.X, r->in.X0, sizeof(r->res.X));
               memcpy(r->res.v, r->in.v0, sizeof(r->res.v));
@@ -405,7 +406,7 @@ void build_loop(kds_server* s) {
             }
             break;
           }
-          s->pending.pop_front();
+          it = s->pending.erase(it);
           r->reserved = need;
           s->reserved += need;
           r->res.t_admit = now;
@@ -419,6 +420,9 @@ void build_loop(kds_server* s) {
           s->peak_reserved = std::max(s->peak_reserved, s->reserved);
           break;
         }
+        // a request refused above can complete a window and queue its map rebuild (its
+        // notification came while this thread held the lock): take it before waiting
+        if (!s->map_tasks.empty()) continue;
         if (next_arrival > 0.0)
           s->cv_build.wait_for(lk, std::chrono::duration<double>(std::max(0.0, next_arrival - now)));
         else

@@ -959,15 +959,15 @@ __global__ void k_big_offsets(BNode* nodes, LevelState* ls, const int32_t* big_l
 // Stable scatter of one chunk by warp ballots: warp w of the block moves points
 // [begin + 128 w, begin + 128 (w + 1)) in four rounds of 32, so left and right runs are
 // written contiguously.  The points that go to the node's smaller child are summed on
-// the way (the sums of the large node's smaller child).
+// the way (the sums of the large node's smaller child); each warp adds its sums with
+// 128-bit atomics, so the chunk needs one block barrier (for the warps' left counts).
 __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, const LevelState* ls,
                                                           const BNode* nodes, PointBufs B,
                                                           const int32_t* chunk_loff, const double* ts0, U128* accl) {
   constexpr int kPer = kChunk / kThreads;  // rounds of 32 points per warp
   constexpr int kWarpsB = kThreads / 32;
   static_assert(kPer * kThreads == kChunk, "chunk = block x rounds");
-  __shared__ int swl[kWarpsB];
-  __shared__ U128 sm[kWarpsB][11];
+  __shared__ int swl[2][kWarpsB];  // left counts of the chunk's warps, by chunk parity
   const int nc = ls->num_chunks, cur = ls->cur;
   const float4* pin = B.p[cur];
   const double* sin_ = B.s[cur];
@@ -977,6 +977,7 @@ __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, c
   int32_t* iout = B.id[cur ^ 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
+  int par = 0;
   for (int ci = blockIdx.x; ci < nc; ci += gridDim.x) {
     const Chunk c = chunks[ci];
     const BNode& nd = nodes[c.node];
@@ -1004,10 +1005,10 @@ __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, c
       bl[u] = __ballot_sync(0xffffffffu, i < c.end && which_side_f(mean, dir, pv[u]));
       nl += __popc(bl[u]);
     }
-    if (lane == 0) swl[w] = nl;
+    if (lane == 0) swl[par][w] = nl;
     __syncthreads();
     int lpre = 0;  // left points of the chunk's earlier warps
-    for (int k = 0; k < w; ++k) lpre += swl[k];
+    for (int k = 0; k < w; ++k) lpre += swl[par][k];
     const int nl_total = nd.mid - nd.start;
     const int before = min(wb, c.end) - nd.start;  // the node's points before this warp's
     int lo = nd.start + chunk_loff[ci] + lpre;
@@ -1030,7 +1031,11 @@ __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, c
       lo += __popc(bl[u]);
       ro += __popc(br);
     }
-    block_add_moments(M, sm, accl + (size_t)c.big * 11);  // also orders swl's reuse
+    {  // the warp's sums straight into its node's accumulators (exact integers: any order)
+      const U128 q = warp_sum_moments(M, lane);
+      if (!(lane & 1) && lane < 22) atomic_add_u128(&accl[(size_t)c.big * 11 + (lane >> 1)], q);
+    }
+    par ^= 1;  // the barrier above keeps warps within one split chunk of each other
   }
 }
 

@@ -935,23 +935,34 @@ __global__ void k_big_count(const Chunk* chunks, const LevelState* ls, const BNo
   }
 }
 
+// Block per large node: the exclusive scan of its chunks' left counts (each chunk's left
+// offset inside the node), then the node's split point and its children's ranges.
 __global__ void k_big_offsets(BNode* nodes, LevelState* ls, const int32_t* big_list,
                               const int32_t* node_chunk0, const int32_t* chunk_nl, int32_t* chunk_loff) {
+  __shared__ int sm[32];
   const int nb = ls->num_big, nc = ls->num_chunks;
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
-    int i = big_list[b];
-    int c0 = node_chunk0[b];
-    int c1 = (b + 1 < nb) ? node_chunk0[b + 1] : nc;
-    int acc = 0;
-    for (int c = c0; c < c1; ++c) { chunk_loff[c] = acc; acc += chunk_nl[c]; }
-    BNode& nd = nodes[i];
-    nd.mid = nd.split ? nd.start + acc : nd.end;
-    if (nd.split) {
-      nodes[nd.left].start = nd.start;
-      nodes[nd.left].end = nd.mid;
-      nodes[nd.right].start = nd.mid;
-      nodes[nd.right].end = nd.end;
-      atomicMax(&ls->max_next, max(nd.mid - nd.start, nd.end - nd.mid));
+  for (int b = blockIdx.x; b < nb; b += gridDim.x) {
+    const int c0 = node_chunk0[b];
+    const int c1 = (b + 1 < nb) ? node_chunk0[b + 1] : nc;
+    int carry = 0;
+    for (int base = c0; base < c1; base += blockDim.x) {
+      const int c = base + threadIdx.x;
+      const int v = c < c1 ? chunk_nl[c] : 0;
+      int tot;
+      const int ex = block_scan(v, sm, &tot);
+      if (c < c1) chunk_loff[c] = carry + ex;
+      carry += tot;
+    }
+    if (threadIdx.x == 0) {
+      BNode& nd = nodes[big_list[b]];
+      nd.mid = nd.split ? nd.start + carry : nd.end;
+      if (nd.split) {
+        nodes[nd.left].start = nd.start;
+        nodes[nd.left].end = nd.mid;
+        nodes[nd.right].start = nd.mid;
+        nodes[nd.right].end = nd.end;
+        atomicMax(&ls->max_next, max(nd.mid - nd.start, nd.end - nd.mid));
+      }
     }
   }
 }
@@ -1471,7 +1482,8 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
           count_launch();
         }
         k_big_count<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_nl);
-        k_big_offsets<<<64, 128, 0, s>>>(w.nodes, w.ls, w.big_list, w.node_chunk0, w.chunk_nl, w.chunk_loff);
+        k_big_offsets<<<kGridBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.big_list, w.node_chunk0, w.chunk_nl,
+                                                       w.chunk_loff);
         k_big_scatter<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_loff, w.ts0, w.accl);
         k_big_childmom<<<64, 256, 0, s>>>(w.nodes, w.ls, w.big_list, w.accl, w.mom);
         for (int c = 0; c < 5; ++c) count_launch();

@@ -217,7 +217,7 @@ struct BNode {
   int32_t has_parent;
   int32_t par_has;    // propagated normal received from the parent
   int32_t has_prop;   // propagated normal handed to the children
-  int32_t pad_;
+  int32_t parent;     // parent node, -1 for a root
   float mean[3], dir[3];
   double dts_mean, dts_cov;
   double prop[3];
@@ -533,6 +533,7 @@ __global__ void k_init_roots(BNode* nodes, const int64_t* off, int R, LevelState
     nd.end = (int32_t)off[r + 1];
     nd.tree = r;
     nd.left = nd.right = -1;
+    nd.parent = -1;
     nodes[r] = nd;
     atomicMax(&ls->max_size, nd.end - nd.start);
   }
@@ -1106,6 +1107,7 @@ __global__ void k_level_children(BNode* nodes, LevelState* ls, const int32_t* bs
             c.level = nd.level + 1;
             c.tree = nd.tree;
             c.left = c.right = -1;
+            c.parent = i;
             c.has_parent = 1;
             c.par_has = nd.has_prop;
             for (int j = 0; j < 3; ++j) c.par_prop[j] = nd.prop[j];
@@ -1135,21 +1137,24 @@ __global__ void k_level_advance(LevelState* ls, const int32_t* bsum, int nblocks
 }
 
 // ---- prune and per-tree compaction -----------------------------------------------------
-__global__ void k_alive(const BNode* nodes, int32_t lb, int32_t le, int32_t* alive, float incidence) {
-  int i = lb + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= le) return;
-  const BNode& nd = nodes[i];
-  int a;
-  if (nd.left < 0 && nd.right < 0) {
-    // IsGoodLeafPredicate_ in float (kd/tree/tree_predicates_.h:18-29)
+// Prune in one launch (alive[] zeroed before): a leaf lives if it passes
+// IsGoodLeafPredicate_ (kd/tree/tree_predicates_.h:18-29, in float), an inner node if
+// any child lives, i.e. if a good leaf lies below it (kd/tree/tree_cpu_.h:172-196).  Each
+// good leaf marks its ancestors up to the first one already marked: whoever marks a node
+// first goes on to its parent, so every ancestor ends marked whatever the order.
+__global__ void k_alive(const BNode* nodes, int32_t total, int32_t* alive, float incidence) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const BNode& nd = nodes[i];
+    if (nd.left >= 0 || nd.right >= 0) continue;
     F3 d = f3(nd.dir[0], nd.dir[1], nd.dir[2]);
     F3 m = f3(nd.mean[0], nd.mean[1], nd.mean[2]);
-    bool ok = dot3x(d, d) > 0.0f && fabsf(dot3x(m, d)) > incidence;
-    a = ok ? 1 : 0;
-  } else {
-    a = ((nd.left >= 0 && alive[nd.left]) || (nd.right >= 0 && alive[nd.right])) ? 1 : 0;
+    if (!(dot3x(d, d) > 0.0f && fabsf(dot3x(m, d)) > incidence)) continue;
+    alive[i] = 1;
+    for (int p = nd.parent; p >= 0; p = nodes[p].parent) {
+      if (((volatile int32_t*)alive)[p]) break;
+      alive[p] = 1;
+    }
   }
-  alive[i] = a;
 }
 
 // group = (level, tree); nodes of one group are contiguous in global order
@@ -1453,7 +1458,6 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   KDS_CK(cudaGetLastError());
 
   LevelState hls;
-  std::vector<int32_t> level_begin(kMaxDepth + 2, 0);
   int32_t host_max = max_size;
   const int cb = std::min<int>(w.chunk_cap, kGridBlocks * 2);
   for (int round = 0; round < kMaxDepth; ++round) {
@@ -1502,18 +1506,11 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   if (hls.lb < hls.le) { set_error("kds_tree_build: depth limit"); return KDS_ERR_CAPACITY; }
   const int depth = hls.depth;
   const int32_t total = hls.le;
-  KDS_CK(cudaMemcpyAsync(level_begin.data(), w.level_begin, sizeof(int32_t) * (kMaxDepth + 2),
-                         cudaMemcpyDeviceToHost, s));
-  KDS_CK(cudaStreamSynchronize(s));
-  level_begin[depth] = total;
-  // prune: bottom-up per level
-  for (int l = depth - 1; l >= 0; --l) {
-    int32_t b = level_begin[l], e = level_begin[l + 1];
-    if (e > b) {
-      k_alive<<<nblk(e - b, kThreads), kThreads, 0, s>>>(w.nodes, b, e, w.alive, P.prune_incidence);
-      count_launch();
-    }
-  }
+  // prune
+  KDS_CK(cudaMemsetAsync(w.alive, 0, sizeof(int32_t) * total, s));
+  k_alive<<<(int)std::min<int64_t>(nblk(total, kThreads), kGridBlocks * 4), kThreads, 0, s>>>(w.nodes, total, w.alive,
+                                                                                          P.prune_incidence);
+  count_launch();
   const int64_t G = (int64_t)(kMaxDepth + 2) * R;
   KDS_CK(cudaMemsetAsync(w.cnt, 0, sizeof(int32_t) * G, s));
   KDS_CK(cudaMemsetAsync(w.lcnt, 0, sizeof(int32_t) * G, s));

@@ -493,6 +493,15 @@ def main():
     n_req = len(sat.requests)
     total_s = max_over_ranks(float(np.sum(times)) / 1e3)
     value = replica_throughput(world, n_req * args.steps, total_s)
+    # the other rates of the served step: moving surfels x Gauss-Newton iterations, and
+    # scan points registered, per second (rank 0's step, one replica)
+    surfel_iters = sum((q["stats"]["num_inliers"] + q["stats"]["num_outliers"] + q["stats"]["num_bad"] +
+                        q["stats"]["num_err_normal"] + q["stats"]["num_err_fn"]) * q["iterations"] for q in served)
+    scan_points = int(sum(len(r.xyz) for r in sat.requests))
+    step_s = float(np.mean(times)) / 1e3
+    rates = {"surfel_iterations_per_s": surfel_iters / step_s, "scan_points_per_s": scan_points / step_s,
+             "note": "per replica: surfels = moving leaves of each registration (its last iteration's count) "
+                     "x its iterations; scan points = the requests' points"}
     ms_step = float(np.mean(times))
 
     # ---- e2e: page-locked host inputs copied inside the step
@@ -583,6 +592,7 @@ def main():
                    "map_rebuilds": st0["map_builds"], "build_pass_ms": st0["build_ms"],
                    "build_points": st0["build_points"], "peak_reserved_bytes": st0["peak_reserved"],
                    "hbm_cap_bytes": st0["hbm_cap"]},
+        "rates": rates,
         "roofline": roofline,
         "roofline_linearize": roofline_lin,
         "clocks": clk.summary(),

@@ -1460,29 +1460,38 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   LevelState hls;
   int32_t host_max = max_size;
   const int cb = std::min<int>(w.chunk_cap, kGridBlocks * 2);
+  // Grids of the level kernels sized to the level: a level has at most twice the nodes
+  // of the one before, and the host learns the current level's size at each sync.  The
+  // node-range kernels (k_decide, k_level_children, k_big_plan, k_level_advance) share
+  // one block count per level; every kernel's result is independent of its grid.
+  int64_t level_nodes = R;
   for (int round = 0; round < kMaxDepth; ++round) {
     for (int k = 0; k < kLevelsPerSync; ++k) {
       const bool level0 = round == 0 && k == 0;
+      const int64_t nodes_bound = level_nodes << k;
+      const int lvl_blocks = (int)std::max<int64_t>(1, std::min<int64_t>(kLevelBlocks, (nodes_bound + kThreads - 1) / kThreads));
+      const int small_blocks =
+          (int)std::max<int64_t>(1, std::min<int64_t>(kSmallBlocks, (nodes_bound + kThreads / 32 - 1) / (kThreads / 32)));
       if (level0) {  // the roots' sums
         k_root_moments<<<kGridBlocks, kThreads, 0, s>>>(w.nodes, R, w.B, w.ts0, w.mom);
         count_launch();
         if (host_max > kBig) {
-          k_big_sums<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig);
-          k_big_plan<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig, w.chunks, w.chunk_cap, w.big_list,
-                                                       w.node_chunk0, w.acc, w.accl);
+          k_big_sums<<<lvl_blocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig);
+          k_big_plan<<<lvl_blocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig, w.chunks, w.chunk_cap, w.big_list,
+                                                     w.node_chunk0, w.acc, w.accl);
           k_big_moments<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.B, w.ts0, w.nodes, w.acc);
           k_big_to_mom<<<64, 256, 0, s>>>(w.ls, w.big_list, w.acc, w.mom);
           for (int c = 0; c < 4; ++c) count_launch();
         }
       }
-      k_decide<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.mom, P, w.bsum, w.bbig, w.root_frame);
-      k_level_children<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum, (int32_t)w.cap_nodes);
-      k_small_part<<<kSmallBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.B, w.ts0, w.mom);
+      k_decide<<<lvl_blocks, kThreads, 0, s>>>(w.nodes, w.ls, w.mom, P, w.bsum, w.bbig, w.root_frame);
+      k_level_children<<<lvl_blocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum, (int32_t)w.cap_nodes);
+      k_small_part<<<small_blocks, kThreads, 0, s>>>(w.nodes, w.ls, w.B, w.ts0, w.mom);
       for (int c = 0; c < 3; ++c) count_launch();
       if (host_max > kBig) {
         if (!level0) {  // k_decide counted the large nodes per block
-          k_big_plan<<<kLevelBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig, w.chunks, w.chunk_cap, w.big_list,
-                                                       w.node_chunk0, w.acc, w.accl);
+          k_big_plan<<<lvl_blocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig, w.chunks, w.chunk_cap, w.big_list,
+                                                     w.node_chunk0, w.acc, w.accl);
           count_launch();
         }
         k_big_count<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_nl);
@@ -1492,7 +1501,7 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
         k_big_childmom<<<64, 256, 0, s>>>(w.nodes, w.ls, w.big_list, w.accl, w.mom);
         for (int c = 0; c < 5; ++c) count_launch();
       }
-      k_level_advance<<<1, kThreads, 0, s>>>(w.ls, w.bsum, kLevelBlocks, w.level_begin);
+      k_level_advance<<<1, kThreads, 0, s>>>(w.ls, w.bsum, lvl_blocks, w.level_begin);
       count_launch();
     }
     KDS_CK(cudaGetLastError());
@@ -1502,6 +1511,7 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
     if (hls.error == 1) { set_error("kds_tree_build: node capacity exceeded"); return KDS_ERR_CAPACITY; }
     if (hls.lb >= hls.le) break;
     host_max = hls.max_size;
+    level_nodes = hls.le - hls.lb;
   }
   if (hls.lb < hls.le) { set_error("kds_tree_build: depth limit"); return KDS_ERR_CAPACITY; }
   const int depth = hls.depth;

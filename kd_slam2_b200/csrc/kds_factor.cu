@@ -198,7 +198,7 @@ int batch_assemble(Runner& R, const kds_factor* F, int32_t nf, int32_t nvars, fl
     set_error("kds_batch_assemble: %d blocks do not fit in %d", nb, cap);
     return KDS_ERR_CAPACITY;
   }
-  memcpy(block_rc, rc.data(), sizeof(int32_t) * rc.size());
+  if (!rc.empty()) memcpy(block_rc, rc.data(), sizeof(int32_t) * rc.size());
   // device buffers: one block from the stream-ordered pool
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t sz_fjob = al(sizeof(int32_t) * std::max(nf, 1)), sz_en = sz_fjob;

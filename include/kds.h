@@ -39,7 +39,8 @@ enum {
   KDS_ERR_TIMEOUT = -8,       /* a bounded device-side wait gave up */
   KDS_ERR_ADMISSION = -9,     /* server refused a request (memory budget) */
   KDS_ERR_NO_DEVICE = -10,
-  KDS_ERR_CAPACITY = -11      /* a fixed-size buffer is too small for the request */
+  KDS_ERR_CAPACITY = -11,     /* a fixed-size buffer is too small for the request */
+  KDS_ERR_DIVERGED = -12      /* the tracker's aligned pose is not finite */
 };
 
 enum { KDS_ICP = 0, KDS_CTICP = 1 };
@@ -375,6 +376,71 @@ int kds_batch_assemble(kds_batch* b, const kds_factor* factors, int32_t num_fact
                        float disable_inlier_ratio, void* stream, int32_t* num_blocks, int32_t* block_rc,
                        double* H_blocks, double* b_vec, int32_t* enabled);
 void kds_batch_free(kds_batch* b);
+
+/* ------------------------------------------------------------------------------
+ * Tracker step: the odometry of TrackerProc_::addFrame
+ * (kd/tracker/tracker_proc_frame_impl_.h:33-115) with its motion model
+ * (ZeroVelMotionModel_ / ConstVelMotionModel_, kd/motion_model/zero_vel_motion_model_.h,
+ * kd/motion_model/const_vel_motion_model_.h) and the keyframe switch of
+ * SLAMProc_::addFrame / addKeyframe (kd/slam/slam_proc_frame_impl_.h:8-49, 73-138) with
+ * relocalisation, loop search and the pose graph left out: a frame that fails
+ * shouldSwitchKeyframe (kd/tracker/tracker_proc_frame_impl_.h:118-123) becomes the
+ * keyframe.  Each step morphs the frame tree by the predicted velocity
+ * (Frame::applyVelocity, kd/map/map_.h:103-110), aligns it to the keyframe tree from
+ * pose_in_kf * prediction, updates the motion model with the relative motion and, for
+ * CT-ICP, morphs the tree again by the estimated residual velocities.
+ * ------------------------------------------------------------------------------ */
+typedef struct kds_tracker kds_tracker;
+
+enum { KDS_MOTION_ZERO_VEL = 0, KDS_MOTION_CONST_VEL = 1 };
+/* KDStatus (kd/map/map_common.h:74-83): values the tracker reports. */
+enum { KDS_STATUS_INIT = 0, KDS_STATUS_TRACKING = 1 };
+
+typedef struct {
+  int32_t aligner_type;       /* odom_aligner: KDS_ICP / KDS_CTICP (KDS_CTICP) */
+  kds_aligner_params aligner; /* its PARAMs (kds_aligner_params_default; CT damping 100) */
+  int32_t motion_model;       /* KDS_MOTION_ZERO_VEL (the reference's default) / KDS_MOTION_CONST_VEL */
+  float motion_model_alpha;   /* ConstVelMotionModel_ low-pass factor (0.9) */
+  float min_inlier_frac;      /* TrackerProc_ PARAMs (kd/tracker/tracker_proc_.h:55-57): 0.6 */
+  float max_kf_trans;         /* 3.0 m */
+  float max_kf_rot_deg;       /* 360 deg */
+} kds_tracker_params;
+
+void kds_tracker_params_default(kds_tracker_params* p);
+
+typedef struct {
+  int32_t status;            /* KDS_STATUS_INIT on the first frame, else KDS_STATUS_TRACKING */
+  int32_t result;            /* the aligner's compute() return (-1 on the first frame) */
+  int32_t new_keyframe;      /* 1 when this frame became the keyframe */
+  int32_t frame_idx;         /* _frame_idx before the step */
+  int32_t keyframe_count;    /* keyframes made so far, this one included */
+  int32_t pad_;
+  double frame_duration;     /* ts - previous ts (0 on the first frame) */
+  double pose_in_kf[12];     /* after the step, before a keyframe switch resets it */
+  double pose_in_world[12];  /* the frame's pose_in_world */
+  double velocity[6];        /* velocity applied before the alignment (velocityLog / frame_duration) */
+  double ct_velocity[6];     /* CT-ICP: the residual velocities applied after it (else 0) */
+  kds_stats stats;           /* the aligner's stats (zero on the first frame) */
+} kds_tracker_result;
+
+/* Creates a tracker with its own aligner.  All work runs on `stream` (NULL: the
+ * calling thread's default stream). */
+int kds_tracker_create(const kds_tracker_params* p, void* stream, kds_tracker** out);
+/* One addFrame.  The frame tree is transformed in place, by T_base_lidar first when it
+ * is not NULL (TrackerProc_::makeFrame, tracker_proc_frame_impl_.h:15-16), then by the
+ * velocity morphs, as the reference's frame tree is.  A frame that becomes the
+ * keyframe is copied into the tracker, so the caller keeps ownership of every tree it
+ * passes.  A non-finite aligned pose returns KDS_ERR_DIVERGED and leaves the tracker's
+ * pose and motion model as they were before the step (the reference throws). */
+int kds_tracker_add_frame(kds_tracker* t, kds_tree* frame, double ts, const double T_base_lidar[12],
+                          kds_tracker_result* out);
+/* Pose of the last frame in the world (TrackerProc_::poseGlobal) and relative to its keyframe. */
+int kds_tracker_get_pose(const kds_tracker* t, double pose_global[12], double pose_in_kf[12]);
+/* The keyframe tree the next frame is aligned to (owned by the tracker; NULL before the first frame). */
+int kds_tracker_get_keyframe(const kds_tracker* t, const kds_tree** kf, double pose_in_world[12]);
+/* Motion model reset (ZeroVelMotionModel_::reset / ConstVelMotionModel_::reset), keyframe dropped. */
+int kds_tracker_reset(kds_tracker* t);
+void kds_tracker_free(kds_tracker* t);
 
 /* ------------------------------------------------------------------------------
  * Served registration (no reference counterpart: the reference runs one tracker

@@ -6,6 +6,7 @@ parameter names of the reference types they stand in for:
   TreeGeneratorB2003D  ~ TreeGenerator3D   (kd/tree/tree_generator_.h:10-47)
   ICPB2003D            ~ ICPCUDA3D / ICPCPU3D   (kd/icp/tree_aligner_base_.h:25-161)
   CTICPB2003D          ~ CTICPCUDA3D / CTICPCPU3D (kd/cticp/cticp_.h:20-261)
+  Tracker3D            ~ the odometry of TrackerProc_ / SLAMProc_ (kd/tracker/tracker_proc_.h)
 
 Poses are 3x4 numpy arrays [R | t] (world <- body); velocities are [v; w].
 All compute runs on the GPU; there is no CPU fallback.
@@ -427,6 +428,103 @@ class CTICPB2003D(_AlignerBase):
 
 
 # ---------------------------------------------------------------------------- batches
+class _TreeView(Tree):
+    """A tree handle owned elsewhere (the tracker's keyframe): never freed here."""
+
+    def free(self) -> None:
+        self._h = C.c_void_p(None)
+
+
+class ZeroVelMotionModel3D:
+    """ZeroVelMotionModel_ (kd/motion_model/zero_vel_motion_model_.h): identity prediction."""
+    KIND = L.KDS_MOTION_ZERO_VEL
+
+    def __init__(self):
+        self.motion_model_alpha = 0.9
+
+
+class ConstVelMotionModel3D(ZeroVelMotionModel3D):
+    """ConstVelMotionModel_ (kd/motion_model/const_vel_motion_model_.h): prediction
+    expmap(T_delta_log), updated by T_delta_log <- alpha T_delta_log + (1 - alpha) log(delta)."""
+    KIND = L.KDS_MOTION_CONST_VEL
+
+    def __init__(self, motion_model_alpha: float = 0.9):
+        self.motion_model_alpha = motion_model_alpha
+
+
+class Tracker3D:
+    """Odometry of TrackerProc_::addFrame (kd/tracker/tracker_proc_frame_impl_.h:33-115)
+    with SLAMProc_'s keyframe switch (kd/slam/slam_proc_frame_impl_.h:8-49) and no
+    relocalisation, loop search or pose graph.
+
+    odom_aligner: an ICPB2003D or CTICPB2003D whose parameters the tracker copies (the
+    tracker runs its own aligner); motion_model: ZeroVelMotionModel3D (the reference's
+    default) or ConstVelMotionModel3D.  add_frame transforms the frame tree in place
+    (T_base_lidar, then the velocity morphs) as the reference does; the keyframe is a
+    device copy owned by the tracker.
+    """
+
+    def __init__(self, odom_aligner=None, motion_model=None, min_inlier_frac: float = 0.6,
+                 max_kf_trans: float = 3.0, max_kf_rot_deg: float = 360.0, stream=None):
+        p = L.TrackerParams()
+        _lib.kds_tracker_params_default(C.byref(p))
+        if odom_aligner is not None:
+            p.aligner_type = odom_aligner.TYPE
+            p.aligner = odom_aligner.params
+        mm = motion_model if motion_model is not None else ZeroVelMotionModel3D()
+        p.motion_model = mm.KIND
+        p.motion_model_alpha = mm.motion_model_alpha
+        p.min_inlier_frac = min_inlier_frac
+        p.max_kf_trans = max_kf_trans
+        p.max_kf_rot_deg = max_kf_rot_deg
+        self.params = p
+        h = C.c_void_p()
+        _check(_lib.kds_tracker_create(C.byref(p), stream, C.byref(h)), "kds_tracker_create")
+        self._h = h
+
+    def __del__(self):
+        self.free()
+
+    def free(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.kds_tracker_free(self._h)
+            self._h = C.c_void_p(None)
+
+    def add_frame(self, tree: Tree, ts: float, T_base_lidar=None) -> dict:
+        r = L.TrackerResult()
+        X = None if T_base_lidar is None else _pose12(T_base_lidar)
+        _check(_lib.kds_tracker_add_frame(self._h, tree.handle, float(ts), _ptr(X), C.byref(r)),
+               "kds_tracker_add_frame")
+        return {"status": r.status, "result": r.result, "new_keyframe": bool(r.new_keyframe),
+                "frame_idx": r.frame_idx, "keyframe_count": r.keyframe_count, "frame_duration": r.frame_duration,
+                "pose_in_kf": np.array(r.pose_in_kf[:]).reshape(3, 4),
+                "pose_in_world": np.array(r.pose_in_world[:]).reshape(3, 4),
+                "velocity": np.array(r.velocity[:]), "ct_velocity": np.array(r.ct_velocity[:]),
+                "stats": r.stats.as_dict()}
+
+    def pose_global(self) -> np.ndarray:
+        X = np.zeros(12)
+        _check(_lib.kds_tracker_get_pose(self._h, X.ctypes.data, None), "kds_tracker_get_pose")
+        return X.reshape(3, 4)
+
+    def pose_in_kf(self) -> np.ndarray:
+        X = np.zeros(12)
+        _check(_lib.kds_tracker_get_pose(self._h, None, X.ctypes.data), "kds_tracker_get_pose")
+        return X.reshape(3, 4)
+
+    def keyframe(self) -> tuple[dict | None, np.ndarray]:
+        """The keyframe tree's export (None before the first frame) and its pose_in_world."""
+        h = C.c_void_p()
+        X = np.zeros(12)
+        _check(_lib.kds_tracker_get_keyframe(self._h, C.byref(h), X.ctypes.data), "kds_tracker_get_keyframe")
+        if not h.value:
+            return None, X.reshape(3, 4)
+        return _TreeView(h.value).export(), X.reshape(3, 4)
+
+    def reset(self) -> None:
+        _check(_lib.kds_tracker_reset(self._h), "kds_tracker_reset")
+
+
 class Batch:
     """Many independent alignments / linearizations per launch (kds_batch_run)."""
 

@@ -26,6 +26,7 @@ KDS_ERR_TIMEOUT = -8
 KDS_ERR_ADMISSION = -9
 KDS_ERR_NO_DEVICE = -10
 KDS_ERR_CAPACITY = -11
+KDS_ERR_DIVERGED = -12
 
 KDS_ICP = 0
 KDS_CTICP = 1
@@ -34,6 +35,10 @@ KDS_MEM_DEVICE = 1
 KDS_JOB_COMPUTE = 0
 KDS_JOB_LINEARIZE = 1
 KDS_JOB_LINEARIZE_DUAL = 2
+KDS_MOTION_ZERO_VEL = 0
+KDS_MOTION_CONST_VEL = 1
+KDS_STATUS_INIT = 0
+KDS_STATUS_TRACKING = 1
 
 
 class TreeParams(C.Structure):
@@ -247,6 +252,37 @@ class ServerStats(C.Structure):
 _P = C.c_void_p
 _I32 = C.c_int32
 _I64 = C.c_int64
+
+class TrackerParams(C.Structure):
+    """kds_tracker_params: TrackerProc_ PARAMs, its odometry aligner and motion model."""
+    _fields_ = [
+        ("aligner_type", C.c_int32),
+        ("aligner", AlignerParams),
+        ("motion_model", C.c_int32),
+        ("motion_model_alpha", C.c_float),
+        ("min_inlier_frac", C.c_float),
+        ("max_kf_trans", C.c_float),
+        ("max_kf_rot_deg", C.c_float),
+    ]
+
+
+class TrackerResult(C.Structure):
+    """kds_tracker_result: what one addFrame produced."""
+    _fields_ = [
+        ("status", C.c_int32),
+        ("result", C.c_int32),
+        ("new_keyframe", C.c_int32),
+        ("frame_idx", C.c_int32),
+        ("keyframe_count", C.c_int32),
+        ("pad_", C.c_int32),
+        ("frame_duration", C.c_double),
+        ("pose_in_kf", C.c_double * 12),
+        ("pose_in_world", C.c_double * 12),
+        ("velocity", C.c_double * 6),
+        ("ct_velocity", C.c_double * 6),
+        ("stats", Stats),
+    ]
+
 SIGNATURES = {
     "kds_last_error": (C.c_char_p, []),
     "kds_init": (C.c_int, [_I32, _I32]),
@@ -315,6 +351,13 @@ SIGNATURES = {
     "kds_server_get_stats": (C.c_int, [_P, C.POINTER(ServerStats)]),
     "kds_server_get_trace": (C.c_int, [_P, _P, _I32, C.POINTER(_I32)]),
     "kds_server_free": (None, [_P]),
+    "kds_tracker_params_default": (None, [C.POINTER(TrackerParams)]),
+    "kds_tracker_create": (C.c_int, [C.POINTER(TrackerParams), _P, C.POINTER(_P)]),
+    "kds_tracker_add_frame": (C.c_int, [_P, _P, C.c_double, _P, C.POINTER(TrackerResult)]),
+    "kds_tracker_get_pose": (C.c_int, [_P, _P, _P]),
+    "kds_tracker_get_keyframe": (C.c_int, [_P, C.POINTER(_P), _P]),
+    "kds_tracker_reset": (C.c_int, [_P]),
+    "kds_tracker_free": (None, [_P]),
     "kds_linearize_static": (C.c_int, [_P, _P, _I32, C.POINTER(AlignerParams), _P, _P, _P, _P, _I32, _P, _P, _P,
                                        C.POINTER(Stats)]),
 }

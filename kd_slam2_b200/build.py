@@ -31,6 +31,7 @@ UNITS = [
     ("kds_serve.cu", ["-fmad=false"]),
     ("kds_factor.cu", []),
     ("kds_voxel.cu", []),
+    ("kds_tracker.cu", []),
 ]
 
 

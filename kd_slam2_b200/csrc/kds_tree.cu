@@ -464,3 +464,54 @@ int tree_export(const kds_tree* t, float* mean, float* dir, double* dts_mean, do
 }
 
 }  // namespace kds
+
+namespace kds {
+
+// Device-to-device copy of a whole tree into a new block allocated on stream s: every
+// node and leaf array, the point permutation and the host-side fields.  The arrays are
+// copied one by one because the two blocks may carve at different base alignments.
+int tree_clone(const kds_tree* src, cudaStream_t s, kds_tree** out) {
+  *out = nullptr;
+  const TreeDev& a = src->d;
+  kds_tree* t = new kds_tree();
+  int rc = tree_alloc(t->d, a.num_nodes, a.num_leaves, a.num_points, s);
+  if (rc != KDS_OK) {
+    delete t;
+    return rc;
+  }
+  TreeDev& b = t->d;
+  const int64_t nn = a.num_nodes, nl = a.num_leaves, np = a.num_points;
+  cudaError_t e = cudaSuccess;
+  auto cp = [&](void* dst, const void* from, size_t bytes) {
+    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(dst, from, bytes, cudaMemcpyDeviceToDevice, s);
+  };
+  cp(b.nodes, a.nodes, sizeof(DNode) * nn);
+  cp(b.dts_f, a.dts_f, sizeof(float) * nn);
+  cp(b.dts_mean, a.dts_mean, sizeof(double) * nn);
+  cp(b.dts_cov, a.dts_cov, sizeof(double) * nn);
+  cp(b.range, a.range, sizeof(int64_t) * 2 * nn);
+  cp(b.level, a.level, sizeof(int32_t) * nn);
+  cp(b.leaf_idx, a.leaf_idx, sizeof(int32_t) * nl);
+  cp(b.leaf_md, a.leaf_md, sizeof(float4) * nl);
+  cp(b.leaf_nrm, a.leaf_nrm, sizeof(float4) * nl);
+  if (a.perm && b.perm) cp(b.perm, a.perm, sizeof(int32_t) * np);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    tree_release(t->d);
+    delete t;
+    return cuda_status(e, "tree_clone copies", __FILE__, __LINE__);
+  }
+  b.num_unpruned = a.num_unpruned;
+  b.ts_start = a.ts_start;
+  b.depth = a.depth;
+  b.accepted = a.accepted;
+  for (int i = 0; i < 3; ++i) {
+    t->root_mean[i] = src->root_mean[i];
+    t->root_eigenvalues[i] = src->root_eigenvalues[i];
+  }
+  for (int i = 0; i < 9; ++i) t->root_eigenvectors[i] = src->root_eigenvectors[i];
+  *out = t;
+  return KDS_OK;
+}
+
+}  // namespace kds

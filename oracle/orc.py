@@ -103,6 +103,9 @@ def load() -> C.CDLL:
         "orc_jacobi3": (None, [P, P, P]),
         "orc_fx_floor": (None, [C.c_double, C.POINTER(C.c_int64), C.POINTER(C.c_uint64)]),
         "orc_warp_leaf": (None, [P, C.c_float, P, P, P, P]),
+        "orc_tree_apply_velocities": (None, [P, P]),
+        "orc_tree_apply_isometry": (None, [P, P]),
+        "orc_tree_clone": (P, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -170,6 +173,19 @@ class OTree:
         out["accepted"] = self.accepted
         out.update(self.root())
         return out
+
+    def apply_velocities_in_place(self, v) -> None:
+        """Tree_::applyVelocitiesInPlace: every node warped by v * (float)dts_mean."""
+        vv = np.ascontiguousarray(v, np.float32)
+        load().orc_tree_apply_velocities(self.h, vv.ctypes.data)
+
+    def apply_isometry_in_place(self, X) -> None:
+        """Tree_::applyIsometryInPlace with a 3x4 float isometry."""
+        XX = np.ascontiguousarray(np.asarray(X, np.float32).reshape(12))
+        load().orc_tree_apply_isometry(self.h, XX.ctypes.data)
+
+    def clone(self) -> "OTree":
+        return OTree(load().orc_tree_clone(self.h))
 
     def root(self) -> dict:
         """Tree_::root_mean / root_eigenvalues / root_eigenvectors (3x3, columns = vectors)."""

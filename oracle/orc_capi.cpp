@@ -162,6 +162,36 @@ void orc_warp_leaf(const float* v6, float dt, const float* m, const float* n, fl
   for (int i = 0; i < 3; ++i) { mo[i] = a[i]; no[i] = b[i]; }
 }
 
+// Tree_::applyVelocitiesInPlace over every node (kd/tree/tree_cuda_impl_.h:132-150):
+// the per-node warp of orc_warp_leaf at dt = (float)dts_mean.
+void orc_tree_apply_velocities(void* h, const float* v6) {
+  Tree* t = (Tree*)h;
+  for (Node& n : t->nodes) {
+    float mo[3], no[3];
+    orc_warp_leaf(v6, (float)n.dts_mean, n.mean, n.dir, mo, no);
+    for (int i = 0; i < 3; ++i) { n.mean[i] = mo[i]; n.dir[i] = no[i]; }
+  }
+}
+
+// Tree_::applyIsometryInPlace (kd/tree/tree_cuda_impl_.h:152-173) with applyIsometry_'s
+// row loop ((t + R0 p0) + R1 p1) + R2 p2 (kd/utils/geometry_.h:11-25); directions are
+// rotated by the same loop from 0.  X: 3x4 row-major floats.
+void orc_tree_apply_isometry(void* h, const float* X) {
+  Tree* t = (Tree*)h;
+  for (Node& n : t->nodes) {
+    float m[3], d[3];
+    for (int r = 0; r < 3; ++r) {
+      const float* R = X + 4 * r;
+      m[r] = ((R[3] + R[0] * n.mean[0]) + R[1] * n.mean[1]) + R[2] * n.mean[2];
+      d[r] = ((0.0f + R[0] * n.dir[0]) + R[1] * n.dir[1]) + R[2] * n.dir[2];
+    }
+    for (int i = 0; i < 3; ++i) { n.mean[i] = m[i]; n.dir[i] = d[i]; }
+  }
+}
+
+// Deep copy (a keyframe kept while the caller's tree moves on).
+void* orc_tree_clone(void* h) { return new Tree(*(Tree*)h); }
+
 void orc_jacobi3(const double* A9, double* ev3, double* V9) {
   double A[3][3], V[3][3];
   for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) A[i][j] = A9[i * 3 + j];

@@ -69,6 +69,16 @@ def test_defaults_match_reference_params():
     assert ap.min_normal_cos == pytest.approx(math.cos(25 / 180 * math.pi), rel=1e-7)
     assert (ap.min_good_measurements, ap.max_iterations, ap.term_crit) == (10, 20, 0)
     assert ap.velocity_damping == pytest.approx(100.0)
+    # TrackerProc_ PARAMs (kd/tracker/tracker_proc_.h:55-60): motion_model defaults to
+    # ZeroVelMotionModel_; ConstVelMotionModel_ motion_model_alpha 0.9
+    import ctypes
+    from kd_slam2_b200 import abi as L, lib
+    tr = L.TrackerParams()
+    lib().kds_tracker_params_default(ctypes.byref(tr))
+    assert (tr.aligner_type, tr.motion_model) == (L.KDS_CTICP, L.KDS_MOTION_ZERO_VEL)
+    assert (tr.min_inlier_frac, tr.max_kf_trans, tr.max_kf_rot_deg) == pytest.approx((0.6, 3.0, 360.0))
+    assert tr.motion_model_alpha == pytest.approx(0.9)
+    assert tr.aligner.max_iterations == ap.max_iterations
 
 
 def test_calls_without_a_device_fail_with_a_status_not_a_crash():
@@ -79,4 +89,36 @@ def test_calls_without_a_device_fail_with_a_status_not_a_crash():
     h = C.c_void_p()
     rc = lib().kds_aligner_create(0, None, C.byref(h))
     assert rc == L.KDS_ERR_NO_DEVICE
+    tp = L.TrackerParams()
+    lib().kds_tracker_params_default(C.byref(tp))
+    assert lib().kds_tracker_create(C.byref(tp), None, C.byref(h)) == L.KDS_ERR_NO_DEVICE and not h.value
     assert b"device" in lib().kds_last_error()
+
+
+def test_struct_layouts_match_the_c_header(tmp_path):
+    """The ctypes mirrors against the C compiler's own sizeof/offsetof of include/kds.h."""
+    import shutil
+    import subprocess
+    from kd_slam2_b200 import abi as L
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    checks = [("kds_tracker_params", L.TrackerParams, ["aligner", "motion_model", "max_kf_rot_deg"]),
+              ("kds_tracker_result", L.TrackerResult, ["frame_duration", "pose_in_kf", "velocity", "stats"]),
+              ("kds_aligner_params", L.AlignerParams, ["velocity_damping", "d_score"]),
+              ("kds_stats", L.Stats, ["chi2", "pert_vel_norm"])]
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "kds.h"', "int main(void) {"]
+    for cname, _, fields in checks:
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        lines += [f'  printf("%zu\\n", offsetof({cname}, {f}));' for f in fields]
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                    str(exe)], check=True, capture_output=True, text=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    want = []
+    for _, ct, fields in checks:
+        want.append(C.sizeof(ct))
+        want += [getattr(ct, f).offset for f in fields]
+    assert got == want

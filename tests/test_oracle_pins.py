@@ -223,3 +223,33 @@ def test_voxel_restatement_known_answer():
     assert t.tolist() == [1.5, 3.0]
     p, t = OV.voxelize(xyz, st, range_min=0.5, range_max=20.0)  # no grid: range filter only
     assert len(p) == 3 and t.tolist() == [1.0, 2.0, 3.0]
+
+
+def test_tracker_geometry_restatement():
+    """The tracker oracle's FP64 pose helpers: expmap/logmap invert each other (below
+    pi), the Shepperd-quaternion rotation angle equals acos((tr R - 1) / 2) on both of
+    its branches, and iso_inv is the inverse of iso_mul."""
+    from oracle import tracker as T
+    rng = np.random.default_rng(5)
+    for k in range(200):
+        ang = [0.0, 1e-8, 1e-3, 0.5, 2.0, 3.1][k % 6]
+        a = rng.normal(size=3)
+        a *= ang / np.linalg.norm(a)
+        v = list(rng.normal(size=3)) + list(a)
+        X = T.expmap(v)
+        assert np.allclose(T.logmap(X), v, atol=1e-7 if ang > 1e-7 else 1e-12)
+        R = np.array(X).reshape(3, 4)[:, :3]
+        want = math.acos(max(-1.0, min(1.0, (np.trace(R) - 1) / 2)))
+        assert abs(T.rotation_angle(X) - want) <= 1e-6, (ang, T.rotation_angle(X), want)
+        Y = T.expmap(list(rng.normal(size=6)))
+        I = T.iso_mul(T.iso_inv(Y), Y)
+        assert np.allclose(I, [1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0], atol=1e-12)
+    # ConstVelMotionModel_ arithmetic on a known sequence: two updates by the same
+    # delta from zero give (1 - alpha^2) log(delta) (alpha = (float)0.9)
+    alpha = float(np.float32(0.9))
+    d = T.expmap([0.2, 0.01, 0.0, 0.0, 0.0, 0.01])
+    dv = T.logmap(d)
+    s = [0.0] * 6
+    for _ in range(2):
+        s = [alpha * s[i] + (1.0 - alpha) * dv[i] for i in range(6)]
+    assert np.allclose(s, np.array(dv) * (1 - alpha ** 2), rtol=1e-12)

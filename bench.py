@@ -403,6 +403,67 @@ def scan_input(steps: int):
     }
 
 
+def tracker_step(frames: int = 24, cpu_frames: int = 6, cpu: bool = True):
+    """The tracker step (kds_tracker_add_frame) on a 64 x 1024 sweep sequence at 10 Hz
+    (2 m/s, 0.1 rad/s, in-scan motion): per frame the frame tree is built from host
+    points and added to a CT-ICP + constant-velocity tracker (pre-deskew, alignment to
+    the keyframe, CT morph, keyframe switch at 0.5 m).  Host-timed per frame (the call
+    returns once its results are on the host).  With cpu, beside it the CPU baseline:
+    the oracle's restatement of the first frames (tree build + step, the reference's
+    FP32 aligner semantics) on one host core, and the largest pose difference between
+    the two chains over those frames."""
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import streams, synth
+    boxes = synth.scene(1004)
+    v = np.array([2.0, 0.1, 0.0, 0.0, 0.0, 0.1])
+    P = synth.pose((0.0, 0.0, 1.8))
+    M = streams.motion(v, 0.1)
+    seq = []
+    for k in range(frames + 2):
+        xyz, st = synth.scan(boxes, P, vel=v, beams=64, cols=1024, seed=900 + k, t_start=0.1 * k, threads=16)
+        seq.append((0.1 * k, xyz, st))
+        P = streams.compose(P, M)
+    gen = kds.TreeGeneratorB2003D(**TREE)
+    kw = dict(max_kf_trans=0.5, min_inlier_frac=0.3)
+
+    def gpu_chain(n):
+        trk = kds.Tracker3D(odom_aligner=kds.CTICPB2003D(**CT), motion_model=kds.ConstVelMotionModel3D(), **kw)
+        out, ms = [], []
+        for ts, xyz, st in seq[:n]:
+            t0 = time.perf_counter()
+            r = trk.add_frame(gen.make_tree(xyz, st), ts)
+            ms.append(1e3 * (time.perf_counter() - t0))
+            out.append(r)
+        return out, ms
+
+    gpu_chain(2)  # warm-up
+    res, ms = gpu_chain(frames)
+    steady = ms[1:]
+    line = {"frames": frames, "points_per_frame": int(np.mean([len(x) for _, x, _ in seq[:frames]])),
+            "keyframes": int(res[-1]["keyframe_count"]),
+            "ms_per_frame_p50": float(np.percentile(steady, 50)), "ms_per_frame_max": float(np.max(steady)),
+            "frames_per_s": 1e3 / float(np.mean(steady)),
+            "note": "host-timed tree build + add_frame per frame, first frame (keyframe init) excluded"}
+    if not cpu:
+        return line
+    try:
+        from oracle import orc
+        from oracle.tracker import OTracker
+        otrk = OTracker(orc.KIND_CT, orc.align_params(**CT), const_vel=True, mode=orc.MODE_REF32, **kw)
+        cms, worst = [], 0.0
+        for (ts, xyz, st), rg in zip(seq[:cpu_frames], res):
+            t0 = time.perf_counter()
+            ro = otrk.add_frame(orc.OTree.build(xyz, st, orc.tree_params(**TREE)), ts)
+            cms.append(1e3 * (time.perf_counter() - t0))
+            dt, dr = pose_err(rg["pose_in_world"], np.array(ro["pose_in_world"]).reshape(3, 4))
+            worst = max(worst, dt, dr)
+        line["cpu_baseline"] = {"frames": cpu_frames, "ms_per_frame": float(np.mean(cms[1:])), "cores": 1,
+                                "kind": "port", "max_pose_diff_vs_gpu": worst}
+    except Exception as e:  # the oracle is the checker; its absence leaves the GPU numbers
+        line["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -600,6 +661,7 @@ def main():
     if rank == 0 and not args.no_ba:
         line["batched_ba"] = batched_ba(args.steps)
         line["scan_input"] = scan_input(args.steps)
+        line["tracker_step"] = tracker_step(cpu=world == 1 and not args.no_cpu)
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = min(os.cpu_count() or 1, 8)
         line["cpu_baseline"] = cpu_baseline_leg(sat, served, threads)

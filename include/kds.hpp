@@ -168,6 +168,7 @@ class AlignerB200 {
   }
   kds_aligner* handle() const { return _a; }
   kds_aligner_params& params() { return _p; }
+  const kds_aligner_params& params() const { return _p; }
   int dim() const { return _type == KDS_ICP ? 6 : 12; }
   bool isGPU() const { return true; }
 
@@ -284,6 +285,65 @@ class CTICPB2003D : public AlignerB200 {
   void buildQuadraticFormDual(bool stats_mode = false) {
     check(kds_aligner_build_quadratic_form_dual(_a, stats_mode ? 1 : 0), "kds_aligner_build_quadratic_form_dual");
   }
+};
+
+// ---------------------------------------------------------------------------
+// Tracker step: the odometry of TrackerProc_::addFrame with its motion model and
+// SLAMProc_'s keyframe switch (kd/tracker/tracker_proc_frame_impl_.h:33-123).
+// Takes the aligner's type and PARAMs; the keyframe is a device copy it owns.
+class TrackerB200 {
+ public:
+  using Result = kds_tracker_result;
+  // PARAM names: min_inlier_frac, max_kf_trans, max_kf_rot_deg (kd/tracker/tracker_proc_.h:55-57),
+  // motion_model_alpha (kd/motion_model/const_vel_motion_model_.h:19)
+  static bool setParam(kds_tracker_params& p, const std::string& k, double v) {
+    if (k == "min_inlier_frac") p.min_inlier_frac = (float)v;
+    else if (k == "max_kf_trans") p.max_kf_trans = (float)v;
+    else if (k == "max_kf_rot_deg") p.max_kf_rot_deg = (float)v;
+    else if (k == "motion_model_alpha") p.motion_model_alpha = (float)v;
+    else return false;
+    return true;
+  }
+  TrackerB200(const AlignerB200& odom_aligner, bool const_vel, kds_tracker_params p = defaults(),
+              void* stream = nullptr) {
+    p.aligner_type = odom_aligner.alignerType();
+    p.aligner = odom_aligner.params();
+    p.motion_model = const_vel ? KDS_MOTION_CONST_VEL : KDS_MOTION_ZERO_VEL;
+    check(kds_tracker_create(&p, stream, &_t), "kds_tracker_create");
+  }
+  ~TrackerB200() {
+    if (_t) kds_tracker_free(_t);
+  }
+  TrackerB200(const TrackerB200&) = delete;
+  TrackerB200& operator=(const TrackerB200&) = delete;
+
+  static kds_tracker_params defaults() {
+    kds_tracker_params p;
+    kds_tracker_params_default(&p);
+    return p;
+  }
+  // addFrame: frame is transformed in place (T_base_lidar, then the velocity morphs)
+  Result addFrame(Tree& frame, double ts, const Pose* T_base_lidar = nullptr) {
+    Result r;
+    check(kds_tracker_add_frame(_t, frame.handle(), ts, T_base_lidar ? T_base_lidar->data() : nullptr, &r),
+          "kds_tracker_add_frame");
+    return r;
+  }
+  Pose poseGlobal() const {
+    Pose X;
+    check(kds_tracker_get_pose(_t, X.data(), nullptr), "kds_tracker_get_pose");
+    return X;
+  }
+  Pose poseInKeyframe() const {
+    Pose X;
+    check(kds_tracker_get_pose(_t, nullptr, X.data()), "kds_tracker_get_pose");
+    return X;
+  }
+  void reset() { check(kds_tracker_reset(_t), "kds_tracker_reset"); }
+  kds_tracker* handle() const { return _t; }
+
+ private:
+  kds_tracker* _t = nullptr;
 };
 
 // ---------------------------------------------------------------------------

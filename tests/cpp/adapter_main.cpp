@@ -4,6 +4,10 @@
 //   adapter_main align <file.conf> <fixed.bin> <moving.bin> <x0.bin> <v0.bin> <out.bin>
 //       builds both trees with the conf's TreeGeneratorB2003D, runs the conf's
 //       CTICPB2003D and writes [result, X(12), v(6)] as doubles
+//   adapter_main track <file.conf> <out.bin> <frame0.bin> <frame1.bin> ...
+//       tracks the frames (stamps of frame i start at 0.1 i; ts = 0.1 i) with the
+//       conf's CTICPB2003D and a constant-velocity TrackerB200 (max_kf_trans 0.5,
+//       min_inlier_frac 0.3) and writes [new_keyframe, result, pose_in_world(12)] per frame
 // A cloud file is int64 n, then n*3 float32 xyz, then n float64 stamps.
 #include <cstdio>
 #include <fstream>
@@ -95,11 +99,43 @@ static int align_mode(char** argv) {
   return 0;
 }
 
+static int track_mode(int argc, char** argv) {
+  auto objs = ConfReader::load(argv[2]);
+  TreeGeneratorB2003D gen;
+  ConfReader::configure(gen, *find_type(objs, "TreeGeneratorB2003D"));
+  CTICPB2003D odom;
+  ConfReader::configure(odom, *find_type(objs, "CTICPB2003D"), objs);
+  kds_tracker_params tp = TrackerB200::defaults();
+  TrackerB200::setParam(tp, "max_kf_trans", 0.5);
+  TrackerB200::setParam(tp, "min_inlier_frac", 0.3);
+  TrackerB200 tracker(odom, true, tp);
+  std::vector<double> out;
+  for (int i = 4; i < argc; ++i) {
+    std::vector<float> xyz;
+    std::vector<double> st;
+    read_cloud(argv[i], xyz, st);
+    TreePtr t = gen.makeTree(xyz.data(), st.data(), (int64_t)st.size());
+    if (!t) throw std::runtime_error("tree rejected");
+    TrackerB200::Result r = tracker.addFrame(*t, 0.1 * (i - 4));
+    out.push_back((double)r.new_keyframe);
+    out.push_back((double)r.result);
+    out.insert(out.end(), r.pose_in_world, r.pose_in_world + 12);
+  }
+  std::ofstream f(argv[3], std::ios::binary);
+  f.write(reinterpret_cast<const char*>(out.data()), (std::streamsize)(out.size() * sizeof(double)));
+  const Pose g = tracker.poseGlobal();
+  std::printf("frames %d x %.6f\n", argc - 4, g[3]);
+  return 0;
+}
+
 int main(int argc, char** argv) {
   try {
     if (argc >= 3 && std::string(argv[1]) == "conf") return conf_mode(argv[2]);
     if (argc >= 8 && std::string(argv[1]) == "align") return align_mode(argv);
-    std::fprintf(stderr, "usage: adapter_main conf <file> | align <conf> <fixed> <moving> <x0> <v0> <out>\n");
+    if (argc >= 5 && std::string(argv[1]) == "track") return track_mode(argc, argv);
+    std::fprintf(stderr,
+                 "usage: adapter_main conf <file> | align <conf> <fixed> <moving> <x0> <v0> <out> |"
+                 " track <conf> <out> <frames...>\n");
     return 2;
   } catch (const std::exception& e) {
     std::fprintf(stderr, "error: %s\n", e.what());

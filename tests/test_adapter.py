@@ -108,3 +108,34 @@ def test_cpp_adapter_matches_python_api(adapter_bin, scene, tmp_path):
     assert out[0] == r
     assert np.array_equal(out[1:13], np.asarray(a.get_x(), np.float64).reshape(12))
     assert np.array_equal(out[13:19], a.velocities())
+
+
+@pytest.mark.gpu
+def test_cpp_tracker_adapter_matches_python_api(adapter_bin, scene, tmp_path):
+    """TrackerB200 (include/kds.hpp) over four frames gives what Tracker3D gives: the same
+    library, so keyframe flags, result codes and poses are identical."""
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import streams, synth
+    v = np.array([2.0, 0.1, 0.0, 0.0, 0.0, 0.1])
+    P = synth.pose((0.0, 0.0, 1.8))
+    M = streams.motion(v, 0.1)
+    frames = []
+    for k in range(4):
+        xyz, st = synth.scan(scene, P, vel=v, beams=16, cols=1024, seed=60 + k, t_start=0.1 * k)
+        frames.append((xyz, st))
+        _write_cloud(tmp_path / f"fr{k}.bin", xyz, st)
+        P = streams.compose(P, M)
+    subprocess.run([adapter_bin, "track", FIXTURE, str(tmp_path / "trk.bin")] +
+                   [str(tmp_path / f"fr{k}.bin") for k in range(4)], check=True, capture_output=True, text=True)
+    out = np.fromfile(tmp_path / "trk.bin", np.float64).reshape(4, 14)
+
+    gen = kds.TreeGeneratorB2003D(leaf_max_points=16, tree_min_good_leaves=10, propagate_normal=0)
+    odom = kds.CTICPB2003D(kernel_threshold=np.float32(0.200000003), damping=1.0, max_error=0.5,
+                           min_normal_cos=np.float32(0.699999988), max_iterations=15, velocity_damping=10.0,
+                           term_crit=dict(d_pert=np.float32(0.00200000009), d_score=np.float32(0.000500000024)))
+    trk = kds.Tracker3D(odom_aligner=odom, motion_model=kds.ConstVelMotionModel3D(), max_kf_trans=0.5,
+                        min_inlier_frac=0.3)
+    for k, (xyz, st) in enumerate(frames):
+        r = trk.add_frame(gen.make_tree(xyz, st), 0.1 * k)
+        assert out[k, 0] == float(r["new_keyframe"]) and out[k, 1] == r["result"], k
+        assert np.array_equal(out[k, 2:], r["pose_in_world"].reshape(12)), k

@@ -473,7 +473,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain drop-in comparison")
     ap.add_argument("--no-ba", action="store_true", help="skip the batched bundle-adjustment section")
+    ap.add_argument("--tracker-only", action="store_true",
+                    help="run only the tracker-step leg and print its JSON (for profiling it)")
     args = ap.parse_args()
+    if args.tracker_only:
+        print(json.dumps({"tracker_step": tracker_step(cpu=not args.no_cpu)}), flush=True)
+        return
     if args.warmup < 3:
         args.warmup = 3
 

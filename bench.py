@@ -444,6 +444,7 @@ def tracker_step(frames: int = 24, cpu_frames: int = 6, cpu: bool = True):
             "ms_per_frame_p50": float(np.percentile(steady, 50)), "ms_per_frame_max": float(np.max(steady)),
             "frames_per_s": 1e3 / float(np.mean(steady)),
             "note": "host-timed tree build + add_frame per frame, first frame (keyframe init) excluded"}
+    line["many_streams"] = tracker_streams()
     if not cpu:
         return line
     try:
@@ -462,6 +463,75 @@ def tracker_step(frames: int = 24, cpu_frames: int = 6, cpu: bool = True):
     except Exception as e:  # the oracle is the checker; its absence leaves the GPU numbers
         line["cpu_baseline"] = {"unavailable": str(e)[:200]}
     return line
+
+
+def tracker_streams(num_streams: int = 32, frames: int = 8):
+    """Many sensor streams, each with its own tracker (CT-ICP + ConstVel), one frame per
+    stream per step: the frames' trees built in one forest pass (kds_tree_build_batch)
+    and the steps run as one batched call (kds_tracker_add_frames: one batch of
+    alignments), against the same streams stepped one at a time (kds_tree_build +
+    kds_tracker_add_frame).  64 x 1024 sweeps in page-locked host memory, copied to the
+    device inside each step; host-timed steps after the first (keyframe initialisation);
+    the two runs' poses must be identical."""
+    import torch
+
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import streams, synth
+    boxes = synth.scene(1005)
+    seqs = []
+    for i in range(num_streams):
+        v = np.array([1.0 + 0.1 * (i % 8), 0.05, 0.0, 0.0, 0.0, 0.02 * ((i % 5) - 2)])
+        P = synth.pose((-20.0 + 1.3 * i, -8.0 + 0.5 * (i % 7), 1.8), (0.0, 0.0, 0.2 * i))
+        M = streams.motion(v, 0.1)
+        fr = []
+        for k in range(frames):
+            xyz, st = synth.scan(boxes, P, vel=v, beams=64, cols=1024, seed=5000 + 37 * i + k, t_start=0.1 * k,
+                                 threads=16)
+            # page-locked host buffers, as a sensor driver would fill them
+            fr.append((0.1 * k, torch.from_numpy(xyz).pin_memory().numpy(),
+                       torch.from_numpy(st).pin_memory().numpy()))
+            P = streams.compose(P, M)
+        seqs.append(fr)
+    gen = kds.TreeGeneratorB2003D(**TREE)
+    kw = dict(max_kf_trans=0.5, min_inlier_frac=0.3)
+
+    def trackers():
+        return [kds.Tracker3D(odom_aligner=kds.CTICPB2003D(**CT), motion_model=kds.ConstVelMotionModel3D(), **kw)
+                for _ in range(num_streams)]
+
+    def one_at_a_time():
+        trk, poses, ms = trackers(), [], []
+        for k in range(frames):
+            t0 = time.perf_counter()
+            rs = [trk[i].add_frame(gen.make_tree(seqs[i][k][1], seqs[i][k][2]), seqs[i][k][0])
+                  for i in range(num_streams)]
+            ms.append(1e3 * (time.perf_counter() - t0))
+            poses.append([r["pose_in_world"] for r in rs])
+        return poses, ms
+
+    def batched():
+        trk, batch, poses, ms = trackers(), kds.Batch(), [], []
+        for k in range(frames):
+            t0 = time.perf_counter()
+            trees = gen.make_trees([(seqs[i][k][1], seqs[i][k][2]) for i in range(num_streams)])
+            rs, codes = kds.Tracker3D.add_frames(trk, trees, [seqs[i][k][0] for i in range(num_streams)], batch)
+            ms.append(1e3 * (time.perf_counter() - t0))
+            assert not np.any(codes)
+            poses.append([r["pose_in_world"] for r in rs])
+        return poses, ms
+
+    batched()  # warm-up (graph capture, pools)
+    pb, mb = batched()
+    ps, msq = one_at_a_time()
+    same = all(np.array_equal(a, b) for ra, rb in zip(pb, ps) for a, b in zip(ra, rb))
+    fb = num_streams * (frames - 1) / (sum(mb[1:]) / 1e3)
+    fs = num_streams * (frames - 1) / (sum(msq[1:]) / 1e3)
+    return {"streams": num_streams, "frames": frames,
+            "points_per_step": int(sum(len(seqs[i][1][1]) for i in range(num_streams))),
+            "batched_frames_per_s": fb, "batched_ms_per_step": float(np.mean(mb[1:])),
+            "one_at_a_time_frames_per_s": fs, "one_at_a_time_ms_per_step": float(np.mean(msq[1:])),
+            "speedup": fb / fs, "identical_poses": bool(same),
+            "note": "host-timed steps (one frame of every stream), first step excluded"}
 
 
 def main():

@@ -105,6 +105,12 @@ int kds_tree_build(const float* xyz, const double* stamps, int64_t n, int32_t me
  * KDS_ERR_TREE_REJECTED); the return value reports failures of the whole call. */
 int kds_tree_build_batch(const float* xyz, const double* stamps, const int64_t* offsets, int32_t num_trees,
                          int32_t mem, const kds_tree_params* p, void* stream, kds_tree** out, int32_t* status);
+/* kds_tree_build_batch over clouds in separate host arrays: cloud r is counts[r] points
+ * at xyz[r] (stamps[r], or zeros when stamps or stamps[r] is NULL), copied one by one
+ * into place on the device, so the caller need not pack them into one array first. */
+int kds_tree_build_batch_gather(const float* const* xyz, const double* const* stamps, const int64_t* counts,
+                                int32_t num_trees, const kds_tree_params* p, void* stream, kds_tree** out,
+                                int32_t* status);
 
 /* Replaces Tree_CUDAfromCPU_ (kd/tree/tree_cuda_impl_.h:197-222): uploads a node
  * array in the Node_ field order (kd/tree/node_.h:33-43), BFS numbered, node 0 the
@@ -434,6 +440,16 @@ int kds_tracker_create(const kds_tracker_params* p, void* stream, kds_tracker** 
  * pose and motion model as they were before the step (the reference throws). */
 int kds_tracker_add_frame(kds_tracker* t, kds_tree* frame, double ts, const double T_base_lidar[12],
                           kds_tracker_result* out);
+/* The same step for n independent trackers at once (many sensor streams, no reference
+ * counterpart): every tracker's morphs and keyframe copies run on `stream`, and the n
+ * alignments run as one batch (kds_batch_run, COMPUTE jobs, graph-captured when the job
+ * set's shape repeats) instead of n aligner calls.  Each tracker's result is what
+ * kds_tracker_add_frame gives it.  codes[i] (may be NULL) is KDS_OK or that tracker's
+ * error (KDS_ERR_DIVERGED leaves only that tracker as it was); the return value is
+ * KDS_OK or the first error.  The trackers must be distinct, and their own streams idle. */
+int kds_tracker_add_frames(kds_tracker* const* trackers, kds_tree* const* frames, const double* ts,
+                           const double* T_base_lidar, int32_t n, kds_batch* batch, void* stream,
+                           kds_tracker_result* out, int32_t* codes);
 /* Pose of the last frame in the world (TrackerProc_::poseGlobal) and relative to its keyframe. */
 int kds_tracker_get_pose(const kds_tracker* t, double pose_global[12], double pose_in_kf[12]);
 /* The keyframe tree the next frame is aligned to (owned by the tracker; NULL before the first frame). */

@@ -215,20 +215,18 @@ class TreeGeneratorB2003D:
 
     def make_trees(self, clouds, stream=None) -> list:
         """Builds one tree per (xyz, stamps) cloud in a single batched pass; None entries
-        where makeTree would return nullptr."""
-        xyz = np.ascontiguousarray(np.concatenate([np.asarray(c[0], np.float32).reshape(-1, 3) for c in clouds]))
-        has_st = any(c[1] is not None for c in clouds)
-        st = None
-        if has_st:
-            st = np.ascontiguousarray(np.concatenate(
-                [np.zeros(len(c[0])) if c[1] is None else np.asarray(c[1], np.float64) for c in clouds]))
-        off = np.zeros(len(clouds) + 1, np.int64)
-        off[1:] = np.cumsum([len(c[0]) for c in clouds])
+        where makeTree would return nullptr.  The clouds are copied to the device one by
+        one (kds_tree_build_batch_gather), without packing them on the host first."""
+        xs = [np.ascontiguousarray(np.asarray(c[0], np.float32).reshape(-1, 3)) for c in clouds]
+        ss = [None if c[1] is None else np.ascontiguousarray(c[1], np.float64) for c in clouds]
         R = len(clouds)
+        xp = (C.c_void_p * R)(*[x.ctypes.data for x in xs])
+        sp = (C.c_void_p * R)(*[None if t is None else t.ctypes.data for t in ss])
+        counts = np.array([len(x) for x in xs], np.int64)
         hs = (C.c_void_p * R)()
         status = (C.c_int32 * R)()
-        _check(_lib.kds_tree_build_batch(xyz.ctypes.data, _ptr(st), off.ctypes.data, R, L.KDS_MEM_HOST,
-                                         C.byref(self.params), stream, hs, status), "kds_tree_build_batch")
+        _check(_lib.kds_tree_build_batch_gather(xp, sp, counts.ctypes.data, R, C.byref(self.params), stream, hs,
+                                                status), "kds_tree_build_batch_gather")
         return [Tree(hs[i]) if status[i] == L.KDS_OK else None for i in range(R)]
 
 
@@ -495,12 +493,35 @@ class Tracker3D:
         X = None if T_base_lidar is None else _pose12(T_base_lidar)
         _check(_lib.kds_tracker_add_frame(self._h, tree.handle, float(ts), _ptr(X), C.byref(r)),
                "kds_tracker_add_frame")
+        return self._result(r)
+
+    @staticmethod
+    def _result(r) -> dict:
         return {"status": r.status, "result": r.result, "new_keyframe": bool(r.new_keyframe),
                 "frame_idx": r.frame_idx, "keyframe_count": r.keyframe_count, "frame_duration": r.frame_duration,
                 "pose_in_kf": np.array(r.pose_in_kf[:]).reshape(3, 4),
                 "pose_in_world": np.array(r.pose_in_world[:]).reshape(3, 4),
                 "velocity": np.array(r.velocity[:]), "ct_velocity": np.array(r.ct_velocity[:]),
                 "stats": r.stats.as_dict()}
+
+    @staticmethod
+    def add_frames(trackers, trees, ts, batch: "Batch", T_base_lidar=None, stream=None):
+        """One step of many trackers with their alignments in one batch
+        (kds_tracker_add_frames).  Returns (results, codes); raises on a call error other
+        than a tracker's divergence, which shows as that tracker's code."""
+        n = len(trackers)
+        hs = (C.c_void_p * n)(*[t._h.value for t in trackers])
+        fs = (C.c_void_p * n)(*[t.handle.value for t in trees])
+        tt = np.ascontiguousarray(ts, np.float64)
+        X = None if T_base_lidar is None else np.ascontiguousarray(
+            np.stack([_pose12(x) for x in T_base_lidar]))
+        out = (L.TrackerResult * n)()
+        codes = np.zeros(n, np.int32)
+        rc = _lib.kds_tracker_add_frames(hs, fs, tt.ctypes.data, _ptr(X), n, batch._h, stream, out,
+                                         codes.ctypes.data)
+        if rc not in (L.KDS_OK, L.KDS_ERR_DIVERGED):
+            _check(rc, "kds_tracker_add_frames")
+        return [Tracker3D._result(out[i]) for i in range(n)], codes
 
     def pose_global(self) -> np.ndarray:
         X = np.zeros(12)

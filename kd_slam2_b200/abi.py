@@ -351,9 +351,11 @@ SIGNATURES = {
     "kds_server_get_stats": (C.c_int, [_P, C.POINTER(ServerStats)]),
     "kds_server_get_trace": (C.c_int, [_P, _P, _I32, C.POINTER(_I32)]),
     "kds_server_free": (None, [_P]),
+    "kds_tree_build_batch_gather": (C.c_int, [_P, _P, _P, _I32, C.POINTER(TreeParams), _P, _P, _P]),
     "kds_tracker_params_default": (None, [C.POINTER(TrackerParams)]),
     "kds_tracker_create": (C.c_int, [C.POINTER(TrackerParams), _P, C.POINTER(_P)]),
     "kds_tracker_add_frame": (C.c_int, [_P, _P, C.c_double, _P, C.POINTER(TrackerResult)]),
+    "kds_tracker_add_frames": (C.c_int, [_P, _P, _P, _P, _I32, _P, _P, C.POINTER(TrackerResult), _P]),
     "kds_tracker_get_pose": (C.c_int, [_P, _P, _P]),
     "kds_tracker_get_keyframe": (C.c_int, [_P, C.POINTER(_P), _P]),
     "kds_tracker_reset": (C.c_int, [_P]),

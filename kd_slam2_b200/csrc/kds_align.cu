@@ -886,10 +886,14 @@ int count_touched(Runner& R, int kind, int64_t fixed_nodes, int64_t* out, cudaSt
 // Host runner
 int Runner::reserve(int nj, int nl, int nt) {
   if (nj <= cap_jobs && nl <= cap_lins && nt <= cap_tiles) return KDS_OK;
+  // grow by at least half of the old capacity: callers whose job sets vary from call to
+  // call (a tracker's frames, served ticks) reallocate -- a device-wide synchronisation in
+  // cudaFree -- a logarithmic number of times instead of at every new maximum
+  const int oj = cap_jobs, ol = cap_lins, ot = cap_tiles;
   release();
-  cap_jobs = std::max(nj, 1);
-  cap_lins = std::max(nl, 1);
-  cap_tiles = std::max(nt, 1);
+  cap_jobs = std::max({nj, oj + oj / 2, 1});
+  cap_lins = std::max({nl, ol + ol / 2, 1});
+  cap_tiles = std::max({nt, ot + ot / 2, 1});
   size_t bytes = sizeof(JobIn) * cap_jobs + sizeof(JobState) * cap_jobs + sizeof(JobOut) * cap_jobs +
                  sizeof(kds_stats) * kMaxLog * cap_jobs + sizeof(LinDev) * cap_lins + sizeof(TileDev) * cap_tiles +
                  sizeof(double) * kPStride * cap_tiles + 8 * 256;

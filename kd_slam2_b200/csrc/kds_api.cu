@@ -169,6 +169,49 @@ int kds_tree_build_batch(const float* xyz, const double* stamps, const int64_t* 
   return tree_build_forest(xyz, stamps, offsets, num_trees, mem, p, as_stream(stream), out, status);
 }
 
+int kds_tree_build_batch_gather(const float* const* xyz, const double* const* stamps, const int64_t* counts,
+                                int32_t num_trees, const kds_tree_params* p, void* stream, kds_tree** out,
+                                int32_t* status) {
+  if (!out || !status || !xyz || !counts || num_trees <= 0) {
+    set_error("kds_tree_build_batch_gather: bad arguments");
+    return KDS_ERR_INVALID_ARG;
+  }
+  for (int r = 0; r < num_trees; ++r) out[r] = nullptr;
+  std::vector<int64_t> off((size_t)num_trees + 1, 0);
+  bool any_st = false;
+  for (int r = 0; r < num_trees; ++r) {
+    if (counts[r] < 0 || (counts[r] > 0 && !xyz[r]) || counts[r] > ((int64_t)1 << 30)) {
+      set_error("kds_tree_build_batch_gather: cloud %d has a bad count or a NULL point array", r);
+      return KDS_ERR_INVALID_ARG;
+    }
+    off[r + 1] = off[r] + counts[r];
+    any_st = any_st || (stamps && stamps[r]);
+  }
+  if (off[num_trees] > ((int64_t)1 << 30)) { set_error("kds_tree_build_batch_gather: too many points"); return KDS_ERR_INVALID_ARG; }
+  KDS_INIT();
+  kds_tree_params def;
+  if (!p) { kds_tree_params_default(&def); p = &def; }
+  cudaStream_t s = as_stream(stream);
+  const int64_t N = off[num_trees];
+  float* d_xyz = nullptr;
+  double* d_st = nullptr;
+  cudaError_t e = cudaMallocAsync(&d_xyz, sizeof(float) * 3 * std::max<int64_t>(N, 1), s);
+  if (e == cudaSuccess && any_st) e = cudaMallocAsync(&d_st, sizeof(double) * std::max<int64_t>(N, 1), s);
+  // each cloud straight into its place: no host-side concatenation
+  for (int r = 0; r < num_trees && e == cudaSuccess; ++r) {
+    if (counts[r] == 0) continue;
+    e = cudaMemcpyAsync(d_xyz + 3 * off[r], xyz[r], sizeof(float) * 3 * counts[r], cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && d_st)
+      e = stamps[r] ? cudaMemcpyAsync(d_st + off[r], stamps[r], sizeof(double) * counts[r], cudaMemcpyHostToDevice, s)
+                    : cudaMemsetAsync(d_st + off[r], 0, sizeof(double) * counts[r], s);
+  }
+  int rc = e == cudaSuccess ? tree_build_forest(d_xyz, d_st, off.data(), num_trees, KDS_MEM_DEVICE, p, s, out, status)
+                            : cuda_status(e, "kds_tree_build_batch_gather copies", __FILE__, __LINE__);
+  if (d_xyz) cudaFreeAsync(d_xyz, s);
+  if (d_st) cudaFreeAsync(d_st, s);
+  return rc;
+}
+
 int kds_tree_import(const float* mean, const float* dir, const double* dts_mean, const double* dts_cov,
                     const int64_t* idx_start, const int64_t* idx_end, const int32_t* left, const int32_t* right,
                     int64_t num_nodes, double ts_start, kds_tree** out) {

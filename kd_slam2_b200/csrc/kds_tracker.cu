@@ -15,6 +15,7 @@
 // and pose arithmetic is FP64 on the host, as the aligner's pose math is.
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "kds_internal.cuh"
 
@@ -192,13 +193,13 @@ void motion_update(kds_tracker* t, const Iso& delta) {
 }
 
 // Frame::applyVelocity: morph only when the velocity is not zero
-int apply_velocity(kds_tracker* t, kds_tree* tree, const double* v) {
+int apply_velocity(kds_tree* tree, const double* v, cudaStream_t s) {
   bool zero = true;
   for (int i = 0; i < 6; ++i) zero = zero && v[i] == 0.0;
   if (zero) return KDS_OK;
   float vf[6];
   for (int i = 0; i < 6; ++i) vf[i] = (float)v[i];
-  return tree_apply_velocities(tree, vf, 0, t->stream);
+  return tree_apply_velocities(tree, vf, 0, s);
 }
 
 // TrackerProc_::shouldSwitchKeyframe (tracker_proc_frame_impl_.h:118-123); inlierRatio()
@@ -214,9 +215,9 @@ bool should_switch(const kds_tracker* t, const Iso& X, const kds_stats& st) {
 
 // SLAMProc_::addKeyframe (slam_proc_frame_impl_.h:73-138), tracker part: the frame
 // becomes the keyframe; ZeroVel/ConstVel onKeyframe and onOriginReset are no-ops.
-int make_keyframe(kds_tracker* t, const kds_tree* frame, const Iso& pose_in_world) {
+int make_keyframe(kds_tracker* t, const kds_tree* frame, const Iso& pose_in_world, cudaStream_t s) {
   kds_tree* copy = nullptr;
-  int rc = tree_clone(frame, t->stream, &copy);
+  int rc = tree_clone(frame, s, &copy);
   if (rc != KDS_OK) return rc;
   if (t->keyframe) {
     tree_release(t->keyframe->d);
@@ -229,6 +230,97 @@ int make_keyframe(kds_tracker* t, const kds_tree* frame, const Iso& pose_in_worl
   return KDS_OK;
 }
 
+// What a step must restore when it fails.
+struct Saved {
+  Iso pose_in_kf_prev;
+  double last_ts, frame_duration;
+};
+
+int restore(kds_tracker* t, const Saved& sv, int code) {
+  t->last_ts = sv.last_ts;
+  t->frame_duration = sv.frame_duration;
+  return code;
+}
+
+// The step up to the alignment: makeFrame's T_base_lidar, doPredict, the pre-deskew
+// morph, and the first frame (which becomes the keyframe: *done = true).  Otherwise
+// *X0 = pose_in_kf * prediction for the alignment.
+int pre_step(kds_tracker* t, kds_tree* frame, double ts, const double* T_base_lidar, cudaStream_t s,
+             kds_tracker_result* out, Saved* sv, bool* done, Iso* X0) {
+  *done = false;
+  if (!std::isfinite(ts)) { set_error("kds_tracker_add_frame: timestamp is not finite"); return KDS_ERR_INVALID_ARG; }
+  memset(out, 0, sizeof(*out));
+  out->result = -1;
+  out->frame_idx = t->frame_idx;
+  int rc = KDS_OK;
+  if (T_base_lidar) {
+    float Xf[12];
+    for (int i = 0; i < 12; ++i) Xf[i] = (float)T_base_lidar[i];
+    if ((rc = tree_apply_isometry(frame, Xf, s)) != KDS_OK) return rc;
+  }
+  sv->pose_in_kf_prev = t->pose_in_kf;
+  sv->last_ts = t->last_ts;
+  sv->frame_duration = t->frame_duration;
+  motion_predict(t, ts);
+  out->frame_duration = t->frame_duration;
+  double vel[6] = {0, 0, 0, 0, 0, 0};
+  if (t->frame_duration > 0) {
+    double vl[6];
+    velocity_log(t, vl);
+    for (int i = 0; i < 6; ++i) vel[i] = vl[i] / t->frame_duration;
+    if ((rc = apply_velocity(frame, vel, s)) != KDS_OK) return restore(t, *sv, rc);
+  }
+  memcpy(out->velocity, vel, sizeof(vel));
+  if (!t->keyframe) {
+    // first frame: Init, and SLAMProc_ makes it the keyframe at the origin
+    const Iso I = iso_identity();
+    if ((rc = make_keyframe(t, frame, I, s)) != KDS_OK) return restore(t, *sv, rc);
+    t->pose_global = I;
+    t->have_frame = true;
+    out->status = KDS_STATUS_INIT;
+    out->new_keyframe = 1;
+    out->keyframe_count = t->keyframe_count;
+    memcpy(out->pose_in_kf, I.m, sizeof(I.m));
+    memcpy(out->pose_in_world, I.m, sizeof(I.m));
+    ++t->frame_idx;
+    *done = true;
+    return KDS_OK;
+  }
+  *X0 = iso_mul(t->pose_in_kf, motion_prediction(t));
+  return KDS_OK;
+}
+
+// The step after the alignment (X, stats, result, CT velocities cv): the divergence
+// check, doUpdate, the CT morph and the keyframe test.
+int post_step(kds_tracker* t, kds_tree* frame, const Iso& X, const kds_stats& st, int32_t result, const double* cv,
+              cudaStream_t s, const Saved& sv, kds_tracker_result* out) {
+  out->result = result;
+  out->stats = st;
+  if (!iso_finite(X)) {
+    set_error("kds_tracker_add_frame: solver diverged at frame %d", t->frame_idx);
+    return restore(t, sv, KDS_ERR_DIVERGED);
+  }
+  t->pose_in_kf = X;
+  const Iso pose_in_world = iso_mul(t->kf_pose_in_world, X);
+  motion_update(t, iso_mul(iso_inv(sv.pose_in_kf_prev), X));
+  int rc = KDS_OK;
+  if (t->P.aligner_type == KDS_CTICP) {
+    if ((rc = apply_velocity(frame, cv, s)) != KDS_OK) return rc;
+    memcpy(out->ct_velocity, cv, sizeof(double) * 6);
+  }
+  t->pose_global = pose_in_world;
+  out->status = KDS_STATUS_TRACKING;
+  memcpy(out->pose_in_kf, X.m, sizeof(X.m));
+  memcpy(out->pose_in_world, pose_in_world.m, sizeof(X.m));
+  if (should_switch(t, X, st)) {
+    if ((rc = make_keyframe(t, frame, pose_in_world, s)) != KDS_OK) return rc;
+    out->new_keyframe = 1;
+  }
+  out->keyframe_count = t->keyframe_count;
+  ++t->frame_idx;
+  return KDS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -238,7 +330,6 @@ void kds_tracker_params_default(kds_tracker_params* p) {
   memset(p, 0, sizeof(*p));
   p->aligner_type = KDS_CTICP;
   kds_aligner_params_default(&p->aligner);
-  p->aligner.velocity_damping = 100.f;
   p->motion_model = KDS_MOTION_ZERO_VEL;
   p->motion_model_alpha = 0.9f;
   p->min_inlier_frac = 0.6f;
@@ -272,53 +363,12 @@ int kds_tracker_create(const kds_tracker_params* p, void* stream, kds_tracker** 
 int kds_tracker_add_frame(kds_tracker* t, kds_tree* frame, double ts, const double T_base_lidar[12],
                           kds_tracker_result* out) {
   if (!t || !frame || !out) { set_error("kds_tracker_add_frame: NULL argument"); return KDS_ERR_INVALID_ARG; }
-  if (!std::isfinite(ts)) { set_error("kds_tracker_add_frame: timestamp is not finite"); return KDS_ERR_INVALID_ARG; }
-  memset(out, 0, sizeof(*out));
-  out->result = -1;
-  out->frame_idx = t->frame_idx;
-  int rc = KDS_OK;
-  // makeFrame: the frame tree into the base frame
-  if (T_base_lidar) {
-    float Xf[12];
-    for (int i = 0; i < 12; ++i) Xf[i] = (float)T_base_lidar[i];
-    if ((rc = tree_apply_isometry(frame, Xf, t->stream)) != KDS_OK) return rc;
-  }
-  const Iso pose_in_kf_prev = t->pose_in_kf;
-  const double last_ts_prev = t->last_ts, frame_duration_prev = t->frame_duration;
-  // a failed step leaves the motion model as it was
-  auto fail = [&](int code) {
-    t->last_ts = last_ts_prev;
-    t->frame_duration = frame_duration_prev;
-    return code;
-  };
-  motion_predict(t, ts);
-  out->frame_duration = t->frame_duration;
-  // pre-deskew by the predicted velocity
-  double vel[6] = {0, 0, 0, 0, 0, 0};
-  if (t->frame_duration > 0) {
-    double vl[6];
-    velocity_log(t, vl);
-    for (int i = 0; i < 6; ++i) vel[i] = vl[i] / t->frame_duration;
-    if ((rc = apply_velocity(t, frame, vel)) != KDS_OK) return fail(rc);
-  }
-  memcpy(out->velocity, vel, sizeof(vel));
-
-  if (!t->keyframe) {
-    // first frame: Init, and SLAMProc_ makes it the keyframe at the origin
-    const Iso I = iso_identity();
-    if ((rc = make_keyframe(t, frame, I)) != KDS_OK) return fail(rc);
-    t->pose_global = I;
-    t->have_frame = true;
-    out->status = KDS_STATUS_INIT;
-    out->new_keyframe = 1;
-    out->keyframe_count = t->keyframe_count;
-    memcpy(out->pose_in_kf, I.m, sizeof(I.m));
-    memcpy(out->pose_in_world, I.m, sizeof(I.m));
-    ++t->frame_idx;
-    return KDS_OK;
-  }
-
-  const Iso X0 = iso_mul(t->pose_in_kf, motion_prediction(t));
+  Saved sv;
+  bool done = false;
+  Iso X0;
+  int rc = pre_step(t, frame, ts, T_base_lidar, t->stream, out, &sv, &done, &X0);
+  if (rc != KDS_OK || done) return rc;
+  // alignFrames: fixed = keyframe, moving = frame, fixed X = I, X = X0, zero velocities
   const Iso I = iso_identity();
   const double zero6[6] = {0, 0, 0, 0, 0, 0};
   int32_t result = 0;
@@ -328,37 +378,75 @@ int kds_tracker_add_frame(kds_tracker* t, kds_tree* frame, double ts, const doub
       (rc = kds_aligner_set_x(t->aligner, X0.m)) != KDS_OK ||
       (rc = kds_aligner_set_velocities(t->aligner, zero6)) != KDS_OK ||
       (rc = kds_aligner_compute(t->aligner, 0, &result)) != KDS_OK)
-    return fail(rc);
+    return restore(t, sv, rc);
   Iso X;
   kds_stats st;
+  double cv[6] = {0, 0, 0, 0, 0, 0};
   kds_aligner_get_x(t->aligner, X.m);
   kds_aligner_get_stats(t->aligner, &st);
-  out->result = result;
-  out->stats = st;
-  if (!iso_finite(X)) {
-    set_error("kds_tracker_add_frame: solver diverged at frame %d", t->frame_idx);
-    return fail(KDS_ERR_DIVERGED);
+  if (t->P.aligner_type == KDS_CTICP) kds_aligner_get_velocities(t->aligner, cv);
+  return post_step(t, frame, X, st, result, cv, t->stream, sv, out);
+}
+
+int kds_tracker_add_frames(kds_tracker* const* trackers, kds_tree* const* frames, const double* ts,
+                           const double* T_base_lidar, int32_t n, kds_batch* batch, void* stream,
+                           kds_tracker_result* out, int32_t* codes) {
+  if (n < 0 || (n > 0 && (!trackers || !frames || !ts || !batch || !out))) {
+    set_error("kds_tracker_add_frames: NULL argument or negative count");
+    return KDS_ERR_INVALID_ARG;
   }
-  t->pose_in_kf = X;
-  const Iso pose_in_world = iso_mul(t->kf_pose_in_world, X);
-  motion_update(t, iso_mul(iso_inv(pose_in_kf_prev), X));
-  if (t->P.aligner_type == KDS_CTICP) {
-    double cv[6];
-    kds_aligner_get_velocities(t->aligner, cv);
-    if ((rc = apply_velocity(t, frame, cv)) != KDS_OK) return rc;
-    memcpy(out->ct_velocity, cv, sizeof(cv));
+  for (int32_t i = 0; i < n; ++i) {
+    if (!trackers[i] || !frames[i]) { set_error("kds_tracker_add_frames: NULL tracker or frame %d", i); return KDS_ERR_INVALID_ARG; }
+    for (int32_t j = 0; j < i; ++j)
+      if (trackers[j] == trackers[i]) { set_error("kds_tracker_add_frames: tracker %d repeated", i); return KDS_ERR_INVALID_ARG; }
   }
-  t->pose_global = pose_in_world;
-  out->status = KDS_STATUS_TRACKING;
-  memcpy(out->pose_in_kf, X.m, sizeof(X.m));
-  memcpy(out->pose_in_world, pose_in_world.m, sizeof(X.m));
-  if (should_switch(t, X, st)) {
-    if ((rc = make_keyframe(t, frame, pose_in_world)) != KDS_OK) return rc;
-    out->new_keyframe = 1;
+  cudaStream_t s = as_stream(stream);
+  std::vector<Saved> sv((size_t)n);
+  std::vector<int32_t> rcs((size_t)n, KDS_OK), job_of((size_t)n, -1);
+  std::vector<kds_job> jobs;
+  jobs.reserve((size_t)n);
+  const Iso I = iso_identity();
+  for (int32_t i = 0; i < n; ++i) {
+    bool done = false;
+    Iso X0;
+    rcs[i] = pre_step(trackers[i], frames[i], ts[i], T_base_lidar ? T_base_lidar + 12 * (size_t)i : nullptr, s,
+                      &out[i], &sv[i], &done, &X0);
+    if (rcs[i] != KDS_OK || done) continue;
+    kds_job j;
+    memset(&j, 0, sizeof(j));
+    j.type = trackers[i]->P.aligner_type;
+    j.mode = KDS_JOB_COMPUTE;
+    j.fixed = trackers[i]->keyframe;
+    j.moving = frames[i];
+    j.params = trackers[i]->P.aligner;
+    memcpy(j.X, X0.m, sizeof(j.X));
+    memcpy(j.fixed_X, I.m, sizeof(j.fixed_X));
+    job_of[i] = (int32_t)jobs.size();
+    jobs.push_back(j);
   }
-  out->keyframe_count = t->keyframe_count;
-  ++t->frame_idx;
-  return KDS_OK;
+  if (!jobs.empty()) {
+    int rc = kds_batch_run(batch, jobs.data(), (int32_t)jobs.size(), 1, s);
+    if (rc != KDS_OK) {
+      for (int32_t i = 0; i < n; ++i)
+        if (job_of[i] >= 0) rcs[i] = restore(trackers[i], sv[i], rc);
+      job_of.assign((size_t)n, -1);
+    }
+  }
+  for (int32_t i = 0; i < n; ++i) {
+    if (job_of[i] < 0) continue;
+    const kds_job& j = jobs[(size_t)job_of[i]];
+    Iso X;
+    memcpy(X.m, j.X, sizeof(X.m));
+    double cv[6] = {0, 0, 0, 0, 0, 0};
+    if (j.type == KDS_CTICP) memcpy(cv, j.v, sizeof(cv));
+    rcs[i] = post_step(trackers[i], frames[i], X, j.stats, j.result, cv, s, sv[i], &out[i]);
+  }
+  int first = KDS_OK;
+  for (int32_t i = 0; i < n; ++i) {
+    if (codes) codes[i] = rcs[i];
+    if (first == KDS_OK && rcs[i] != KDS_OK) first = rcs[i];
+  }
+  return first;
 }
 
 int kds_tracker_get_pose(const kds_tracker* t, double pose_global[12], double pose_in_kf[12]) {

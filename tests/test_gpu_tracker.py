@@ -38,7 +38,7 @@ def trajectory(scene, n, vel=(2.0, 0.1, 0.0, 0.0, 0.0, 0.1), seed=50):
         P = streams.compose(P, M)
 
 
-def run_both(scene, n, kind, const_vel, T_base_lidar=None, **tp):
+def run_both(scene, n, kind, const_vel, T_base_lidar=None, vel=(2.0, 0.1, 0.0, 0.0, 0.0, 0.1), **tp):
     import kd_slam2_b200 as kds
     P = dict(max_error=0.5, max_iterations=10)
     if kind == orc.KIND_CT:
@@ -51,7 +51,7 @@ def run_both(scene, n, kind, const_vel, T_base_lidar=None, **tp):
     otrk = OTracker(kind, orc.align_params(**P), const_vel=const_vel, alpha=0.9, **tp)
     gen = kds.TreeGeneratorB2003D(**TREE_P)
     rows = []
-    for ts, xyz, st in trajectory(scene, n):
+    for ts, xyz, st in trajectory(scene, n, vel=vel):
         G = gen.make_tree(xyz, st)
         O = orc.OTree.build(xyz, st, orc.tree_params(**TREE_P))
         rg = trk.add_frame(G, ts, T_base_lidar)
@@ -114,6 +114,17 @@ def test_icp_zero_vel_with_base_transform_matches_oracle(scene):
         assert not np.any(rg["velocity"]) and not np.any(rg["ct_velocity"])
 
 
+def test_rotation_switches_keyframes_as_the_oracle_does(scene):
+    """A turning trajectory (0.5 rad/s yaw: 2.9 deg per frame) with max_kf_rot_deg 4: the
+    rotation test of shouldSwitchKeyframe switches every second frame (5.7 deg), away
+    from the threshold; translation and inlier tests stay off."""
+    trk, otrk, rows = run_both(scene, 8, orc.KIND_CT, True, vel=(1.0, 0.0, 0.0, 0.0, 0.0, 0.5), max_kf_rot_deg=4.0,
+                               max_kf_trans=100.0, min_inlier_frac=0.0)
+    compare(rows)
+    flags = [r[0]["new_keyframe"] for r in rows]
+    assert sum(flags[1:]) >= 3, flags
+
+
 def test_first_frame_reset_and_argument_errors(scene):
     import kd_slam2_b200 as kds
     from kd_slam2_b200 import abi as L
@@ -138,3 +149,51 @@ def test_first_frame_reset_and_argument_errors(scene):
     p.motion_model = 7
     h = C.c_void_p()
     assert kds.lib().kds_tracker_create(C.byref(p), None, C.byref(h)) == L.KDS_ERR_INVALID_ARG and not h.value
+
+
+def test_batched_trackers_equal_sequential_trackers(scene):
+    """kds_tracker_add_frames over four streams (two CT-ICP + ConstVel, two ICP + ZeroVel,
+    different starts and speeds) gives every tracker exactly what kds_tracker_add_frame
+    gives it one frame at a time."""
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import streams, synth
+    gen = kds.TreeGeneratorB2003D(**TREE_P)
+    P = dict(max_error=0.5, max_iterations=10)
+
+    def make(i):
+        if i % 2 == 0:
+            al, mm = kds.CTICPB2003D(velocity_damping=100.0, **P), kds.ConstVelMotionModel3D()
+        else:
+            al, mm = kds.ICPB2003D(**P), kds.ZeroVelMotionModel3D()
+        return kds.Tracker3D(odom_aligner=al, motion_model=mm, max_kf_trans=0.5, min_inlier_frac=0.3)
+
+    seqs = []
+    for i in range(4):
+        v = np.array([1.5 + 0.25 * i, 0.1, 0.0, 0.0, 0.0, 0.05 * (i - 1)])
+        Pi = synth.pose((2.0 * i - 3.0, 1.0 - i, 1.8), (0.0, 0.0, 0.3 * i))
+        M = streams.motion(v, 0.1)
+        frames = []
+        for k in range(6):
+            xyz, st = synth.scan(scene, Pi, vel=v, beams=16, cols=1024, seed=300 + 10 * i + k, t_start=0.1 * k)
+            frames.append((0.1 * k, xyz, st))
+            Pi = streams.compose(Pi, M)
+        seqs.append(frames)
+    seq_trk = [make(i) for i in range(4)]
+    bat_trk = [make(i) for i in range(4)]
+    batch = kds.Batch()
+    for k in range(6):
+        single = [seq_trk[i].add_frame(gen.make_tree(seqs[i][k][1], seqs[i][k][2]), seqs[i][k][0]) for i in range(4)]
+        trees = [gen.make_tree(seqs[i][k][1], seqs[i][k][2]) for i in range(4)]
+        multi, codes = kds.Tracker3D.add_frames(bat_trk, trees, [seqs[i][k][0] for i in range(4)], batch)
+        assert list(codes) == [0, 0, 0, 0]
+        for i, (a, b) in enumerate(zip(single, multi)):
+            for key in ("status", "result", "new_keyframe", "frame_idx", "keyframe_count", "frame_duration",
+                        "stats"):
+                assert a[key] == b[key], (k, i, key)
+            for key in ("pose_in_kf", "pose_in_world", "velocity", "ct_velocity"):
+                assert np.array_equal(a[key], b[key]), (k, i, key)
+    for a, b in zip(seq_trk, bat_trk):
+        assert np.array_equal(a.pose_global(), b.pose_global())
+        ka, _ = a.keyframe()
+        kb, _ = b.keyframe()
+        assert np.array_equal(ka["mean"], kb["mean"])

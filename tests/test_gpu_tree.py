@@ -64,6 +64,25 @@ def test_forest_build_equals_single_builds(scene):
             continue
         O = orc.OTree.build(xyz, st, orc.tree_params(leaf_max_points=16, propagate_normal=1))
         assert_same_tree(O, T)
+    # the packed form (kds_tree_build_batch: one array, offsets) gives the same trees
+    import ctypes as C
+    from kd_slam2_b200 import abi as L
+    xyz = np.ascontiguousarray(np.concatenate([c[0] for c in clouds]))
+    st = np.ascontiguousarray(np.concatenate([np.zeros(len(c[0])) if c[1] is None else c[1] for c in clouds]))
+    off = np.zeros(len(clouds) + 1, np.int64)
+    off[1:] = np.cumsum([len(c[0]) for c in clouds])
+    hs = (C.c_void_p * len(clouds))()
+    status = (C.c_int32 * len(clouds))()
+    rc = kds.lib().kds_tree_build_batch(xyz.ctypes.data, st.ctypes.data, off.ctypes.data, len(clouds),
+                                        L.KDS_MEM_HOST, C.byref(gen.params), None, hs, status)
+    assert rc == L.KDS_OK and status[2] == L.KDS_ERR_TREE_REJECTED
+    for i, T in enumerate(trees):
+        if T is None:
+            continue
+        P = kds.Tree(hs[i])
+        a, b = T.export(), P.export()
+        for k in ("mean", "dir", "dts_mean", "left", "right", "leaves", "perm"):
+            assert np.array_equal(a[k], b[k]), (i, k)
 
 
 def test_tree_build_skewed_scan_with_stamps(scene):

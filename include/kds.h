@@ -437,7 +437,8 @@ int kds_tracker_create(const kds_tracker_params* p, void* stream, kds_tracker** 
  * velocity morphs, as the reference's frame tree is.  A frame that becomes the
  * keyframe is copied into the tracker, so the caller keeps ownership of every tree it
  * passes.  A non-finite aligned pose returns KDS_ERR_DIVERGED and leaves the tracker's
- * pose and motion model as they were before the step (the reference throws). */
+ * pose and motion model as they were before the step (the reference throws).  The call
+ * returns with its device work done (the morphed tree and the keyframe copy are final). */
 int kds_tracker_add_frame(kds_tracker* t, kds_tree* frame, double ts, const double T_base_lidar[12],
                           kds_tracker_result* out);
 /* The same step for n independent trackers at once (many sensor streams, no reference

@@ -148,7 +148,6 @@ struct kds_tracker {
   Iso kf_pose_in_world = iso_identity();
   Iso pose_in_kf = iso_identity();
   Iso pose_global = iso_identity();  // the last frame's pose_in_world
-  bool have_frame = false;
   // ZeroVelMotionModel_ state (zero_vel_motion_model_.h:23-35) and ConstVel's _T_delta_log
   double last_ts = -1.0;
   double frame_duration = 0.0;
@@ -276,7 +275,6 @@ int pre_step(kds_tracker* t, kds_tree* frame, double ts, const double* T_base_li
     const Iso I = iso_identity();
     if ((rc = make_keyframe(t, frame, I, s)) != KDS_OK) return restore(t, *sv, rc);
     t->pose_global = I;
-    t->have_frame = true;
     out->status = KDS_STATUS_INIT;
     out->new_keyframe = 1;
     out->keyframe_count = t->keyframe_count;
@@ -319,6 +317,14 @@ int post_step(kds_tracker* t, kds_tree* frame, const Iso& X, const kds_stats& st
   out->keyframe_count = t->keyframe_count;
   ++t->frame_idx;
   return KDS_OK;
+}
+
+// A step returns with its device work done: the frame tree's morphs and the keyframe
+// copy are final when the call returns, whichever stream the caller uses next.
+int finish(cudaStream_t s, int rc) {
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess && rc == KDS_OK) return cuda_status(e, "tracker step", __FILE__, __LINE__);
+  return rc;
 }
 
 }  // namespace
@@ -367,7 +373,7 @@ int kds_tracker_add_frame(kds_tracker* t, kds_tree* frame, double ts, const doub
   bool done = false;
   Iso X0;
   int rc = pre_step(t, frame, ts, T_base_lidar, t->stream, out, &sv, &done, &X0);
-  if (rc != KDS_OK || done) return rc;
+  if (rc != KDS_OK || done) return finish(t->stream, rc);
   // alignFrames: fixed = keyframe, moving = frame, fixed X = I, X = X0, zero velocities
   const Iso I = iso_identity();
   const double zero6[6] = {0, 0, 0, 0, 0, 0};
@@ -385,7 +391,8 @@ int kds_tracker_add_frame(kds_tracker* t, kds_tree* frame, double ts, const doub
   kds_aligner_get_x(t->aligner, X.m);
   kds_aligner_get_stats(t->aligner, &st);
   if (t->P.aligner_type == KDS_CTICP) kds_aligner_get_velocities(t->aligner, cv);
-  return post_step(t, frame, X, st, result, cv, t->stream, sv, out);
+  rc = post_step(t, frame, X, st, result, cv, t->stream, sv, out);
+  return finish(t->stream, rc);
 }
 
 int kds_tracker_add_frames(kds_tracker* const* trackers, kds_tree* const* frames, const double* ts,
@@ -446,7 +453,7 @@ int kds_tracker_add_frames(kds_tracker* const* trackers, kds_tree* const* frames
     if (codes) codes[i] = rcs[i];
     if (first == KDS_OK && rcs[i] != KDS_OK) first = rcs[i];
   }
-  return first;
+  return finish(s, first);
 }
 
 int kds_tracker_get_pose(const kds_tracker* t, double pose_global[12], double pose_in_kf[12]) {
@@ -472,7 +479,6 @@ int kds_tracker_reset(kds_tracker* t) {
     t->keyframe = nullptr;
   }
   t->kf_pose_in_world = t->pose_in_kf = t->pose_global = iso_identity();
-  t->have_frame = false;
   t->frame_idx = 0;
   t->keyframe_count = 0;
   return KDS_OK;

@@ -402,6 +402,7 @@ int kds_tracker_add_frames(kds_tracker* const* trackers, kds_tree* const* frames
     set_error("kds_tracker_add_frames: NULL argument or negative count");
     return KDS_ERR_INVALID_ARG;
   }
+  if (n == 0) return KDS_OK;
   for (int32_t i = 0; i < n; ++i) {
     if (!trackers[i] || !frames[i]) { set_error("kds_tracker_add_frames: NULL tracker or frame %d", i); return KDS_ERR_INVALID_ARG; }
     for (int32_t j = 0; j < i; ++j)

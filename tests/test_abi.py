@@ -92,6 +92,7 @@ def test_calls_without_a_device_fail_with_a_status_not_a_crash():
     tp = L.TrackerParams()
     lib().kds_tracker_params_default(C.byref(tp))
     assert lib().kds_tracker_create(C.byref(tp), None, C.byref(h)) == L.KDS_ERR_NO_DEVICE and not h.value
+    assert b"device" in lib().kds_last_error()
     # argument checks come before any device use
     xp = (C.c_void_p * 1)(None)
     counts = (C.c_int64 * 1)(-1)
@@ -100,7 +101,6 @@ def test_calls_without_a_device_fail_with_a_status_not_a_crash():
     assert lib().kds_tree_build_batch_gather(xp, None, counts, 1, None, None, hs, st) == L.KDS_ERR_INVALID_ARG
     assert lib().kds_tracker_add_frames(None, None, None, None, 1, None, None, None, None) == L.KDS_ERR_INVALID_ARG
     assert lib().kds_tracker_add_frames(None, None, None, None, 0, None, None, None, None) == L.KDS_OK
-    assert b"device" in lib().kds_last_error()
 
 
 def test_struct_layouts_match_the_c_header(tmp_path):

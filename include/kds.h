@@ -215,6 +215,11 @@ int kds_tree_apply_isometry(kds_tree* t, const float X[12], void* stream);
 /* Replaces TreeCUDA_::extractCompressedLeaves (kd/tree/tree_cuda_impl_.h:42-112):
  * writes [mean, dir] per leaf (6 floats), optionally morphed by v (may be NULL). */
 int kds_tree_extract_compressed_leaves(const kds_tree* t, const float* v6, float* out, void* stream);
+/* The same gather into a device buffer of the caller (num_leaves * 6 floats): no
+ * allocation and no copy, asynchronous on `stream` -- a headless stand-in for the
+ * viewer's leaf events, where the reference allocates, copies and frees per call
+ * (kd/tree/tree_cuda_impl_.h:97-112). */
+int kds_tree_extract_compressed_leaves_device(const kds_tree* t, const float* v6, float* out_device, void* stream);
 
 /* Releases the tree's device memory to the stream-ordered pool on the stream it was
  * built on.  As with TreeCUDA_'s destructor, no work using the tree may be pending on

@@ -185,6 +185,16 @@ class Tree:
                "kds_tree_extract_compressed_leaves")
         return out
 
+    def extract_compressed_leaves_device(self, out, v=None, stream=None) -> None:
+        """The same gather into a CUDA tensor `out` of shape (num_leaves, 6), float32
+        (kds_tree_extract_compressed_leaves_device: no allocation, asynchronous)."""
+        if tuple(out.shape) != (self.num_leaves, 6) or str(out.dtype) != "torch.float32" or not out.is_cuda \
+                or not out.is_contiguous():
+            raise ValueError("out must be a contiguous float32 CUDA tensor of shape (num_leaves, 6)")
+        vv = None if v is None else np.ascontiguousarray(v, np.float32)
+        _check(_lib.kds_tree_extract_compressed_leaves_device(self._h, _ptr(vv), out.data_ptr(), stream),
+               "kds_tree_extract_compressed_leaves_device")
+
 
 class TreeGeneratorB2003D:
     """TreeGenerator3D with the same PARAM names and defaults; builds on the GPU."""

@@ -303,6 +303,7 @@ SIGNATURES = {
     "kds_tree_apply_velocities": (C.c_int, [_P, _P, _I32, _P]),
     "kds_tree_apply_isometry": (C.c_int, [_P, _P, _P]),
     "kds_tree_extract_compressed_leaves": (C.c_int, [_P, _P, _P, _P]),
+    "kds_tree_extract_compressed_leaves_device": (C.c_int, [_P, _P, _P, _P]),
     "kds_tree_free": (None, [_P]),
     "kds_aligner_params_default": (None, [C.POINTER(AlignerParams)]),
     "kds_aligner_create": (C.c_int, [_I32, C.POINTER(AlignerParams), C.POINTER(_P)]),

@@ -320,7 +320,15 @@ int kds_tree_apply_isometry(kds_tree* t, const float X[12], void* stream) {
 
 int kds_tree_extract_compressed_leaves(const kds_tree* t, const float* v6, float* out, void* stream) {
   if (!t || !out) { set_error("kds_tree_extract_compressed_leaves: NULL argument"); return KDS_ERR_INVALID_ARG; }
-  return tree_extract_leaves(t, v6, out, as_stream(stream));
+  return tree_extract_leaves(t, v6, out, nullptr, as_stream(stream));
+}
+
+int kds_tree_extract_compressed_leaves_device(const kds_tree* t, const float* v6, float* out_device, void* stream) {
+  if (!t || !out_device) {
+    set_error("kds_tree_extract_compressed_leaves_device: NULL argument");
+    return KDS_ERR_INVALID_ARG;
+  }
+  return tree_extract_leaves(t, v6, nullptr, out_device, as_stream(stream));
 }
 
 void kds_tree_free(kds_tree* t) {

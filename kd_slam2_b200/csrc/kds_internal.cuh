@@ -224,7 +224,7 @@ int tree_import(const float* mean, const float* dir, const double* dts_mean, con
                 double ts_start, kds_tree** out);
 int tree_apply_velocities(kds_tree* t, const float* v, int skip_leaves, cudaStream_t s);
 int tree_apply_isometry(kds_tree* t, const float* X, cudaStream_t s);
-int tree_extract_leaves(const kds_tree* t, const float* v6, float* out_host, cudaStream_t s);
+int tree_extract_leaves(const kds_tree* t, const float* v6, float* out_host, float* out_device, cudaStream_t s);
 int tree_from_msg(const kds_kdtree3f* msg, kds_tree** out);
 int tree_clone(const kds_tree* src, cudaStream_t s, kds_tree** out);
 int points_voxelize(const float* xyz, const double* stamps, int64_t n, int32_t mem, double msg_t,

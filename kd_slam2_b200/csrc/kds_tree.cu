@@ -410,16 +410,22 @@ int tree_apply_isometry(kds_tree* t, const float* X, cudaStream_t s) {
   return tree_gather_leaves(t->d, s);
 }
 
-int tree_extract_leaves(const kds_tree* t, const float* v6, float* out_host, cudaStream_t s) {
+// Gathers [mean, dir] per leaf, optionally morphed by v6.  out_device: the caller's
+// device buffer (no allocation, asynchronous on s); otherwise out_host through a
+// stream-ordered temporary, returning when the host copy is complete.
+int tree_extract_leaves(const kds_tree* t, const float* v6, float* out_host, float* out_device, cudaStream_t s) {
   if (t->d.num_leaves == 0) return KDS_OK;
-  float* d = nullptr;
-  KDS_CK(cudaMalloc(&d, sizeof(float) * 6 * t->d.num_leaves));
   Vel6 vv;
   for (int i = 0; i < 6; ++i) vv.v[i] = v6 ? v6[i] : 0.f;
+  float* d = out_device;
+  if (!d) KDS_CK(cudaMallocAsync(&d, sizeof(float) * 6 * t->d.num_leaves, s));
   k_extract_leaves<<<nblk(t->d.num_leaves, 256), 256, 0, s>>>(t->d, vv, v6 ? 1 : 0, d); ::kds::count_launch();
-  cudaError_t e = cudaMemcpyAsync(out_host, d, sizeof(float) * 6 * t->d.num_leaves, cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaGetLastError();
+  if (out_device) return e == cudaSuccess ? KDS_OK : cuda_status(e, "extract leaves", __FILE__, __LINE__);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out_host, d, sizeof(float) * 6 * t->d.num_leaves, cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(d, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  cudaFree(d);
   if (e != cudaSuccess) return cuda_status(e, "extract leaves", __FILE__, __LINE__);
   return KDS_OK;
 }

@@ -181,6 +181,15 @@ def test_morph_and_isometry_match_oracle(scene):
     assert np.array_equal(ref.view(np.uint32), e3["mean"][10].view(np.uint32))
     L = G3.extract_compressed_leaves()
     assert np.array_equal(L[:, :3], e3["mean"][e3["leaves"]])
+    # into a device buffer: the same values, with and without a morph
+    import torch
+    D = torch.empty((G3.num_leaves, 6), dtype=torch.float32, device="cuda")
+    G3.extract_compressed_leaves_device(D)
+    torch.cuda.synchronize()
+    assert np.array_equal(D.cpu().numpy(), L)
+    G3.extract_compressed_leaves_device(D, v=v)
+    torch.cuda.synchronize()
+    assert np.array_equal(D.cpu().numpy(), G3.extract_compressed_leaves(v))
 
 
 def test_tree_build_bit_exact_on_stream_scans():

@@ -460,6 +460,23 @@ int kds_tracker_add_frames(kds_tracker* const* trackers, kds_tree* const* frames
 int kds_tracker_get_pose(const kds_tracker* t, double pose_global[12], double pose_in_kf[12]);
 /* The keyframe tree the next frame is aligned to (owned by the tracker; NULL before the first frame). */
 int kds_tracker_get_keyframe(const kds_tracker* t, const kds_tree** kf, double pose_in_world[12]);
+/* Checkpoint / resume of a tracker (no reference counterpart: the reference saves its map
+ * as a bag of keyframe trees plus the factor graph, lib/kd_io/kd_map_io_.h:19-186).  The
+ * state is plain data; the keyframe travels separately as a tree (kds_tree_to_msg /
+ * kds_tree_from_msg carry everything the alignment reads).  A tracker restored with
+ * set_state and that keyframe continues exactly as the saved one would. */
+typedef struct {
+  kds_tracker_params params;
+  double last_ts, frame_duration;   /* ZeroVelMotionModel_ state */
+  double T_delta_log[6];            /* ConstVelMotionModel_ state */
+  double kf_pose_in_world[12], pose_in_kf[12], pose_global[12];
+  int32_t frame_idx, keyframe_count;
+  int32_t has_keyframe, pad_;
+} kds_tracker_state;
+int kds_tracker_get_state(const kds_tracker* t, kds_tracker_state* st);
+/* keyframe: required when st->has_keyframe (copied into the tracker); params must match
+ * the tracker's aligner type and motion model. */
+int kds_tracker_set_state(kds_tracker* t, const kds_tracker_state* st, const kds_tree* keyframe);
 /* Motion model reset (ZeroVelMotionModel_::reset / ConstVelMotionModel_::reset), keyframe dropped. */
 int kds_tracker_reset(kds_tracker* t);
 void kds_tracker_free(kds_tracker* t);

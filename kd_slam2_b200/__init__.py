@@ -555,6 +555,25 @@ class Tracker3D:
     def reset(self) -> None:
         _check(_lib.kds_tracker_reset(self._h), "kds_tracker_reset")
 
+    def checkpoint(self) -> dict:
+        """The tracker's state (kds_tracker_get_state, as bytes) and its keyframe as a
+        KDTree3f message (Tree.to_msg), both plain host data."""
+        st = L.TrackerState()
+        _check(_lib.kds_tracker_get_state(self._h, C.byref(st)), "kds_tracker_get_state")
+        kf = None
+        if st.has_keyframe:
+            h = C.c_void_p()
+            _check(_lib.kds_tracker_get_keyframe(self._h, C.byref(h), None), "kds_tracker_get_keyframe")
+            kf = _TreeView(h.value).to_msg()
+        return {"state": bytes(st), "keyframe": kf}
+
+    def restore(self, ckpt: dict) -> None:
+        """Resumes from checkpoint() output (kds_tracker_set_state)."""
+        st = L.TrackerState.from_buffer_copy(ckpt["state"])
+        kf = Tree.from_msg(ckpt["keyframe"]) if ckpt["keyframe"] is not None else None
+        _check(_lib.kds_tracker_set_state(self._h, C.byref(st), kf.handle if kf is not None else None),
+               "kds_tracker_set_state")
+
 
 class Batch:
     """Many independent alignments / linearizations per launch (kds_batch_run)."""

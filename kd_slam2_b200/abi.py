@@ -283,6 +283,23 @@ class TrackerResult(C.Structure):
         ("stats", Stats),
     ]
 
+
+class TrackerState(C.Structure):
+    """kds_tracker_state: a tracker checkpoint without its keyframe tree."""
+    _fields_ = [
+        ("params", TrackerParams),
+        ("last_ts", C.c_double),
+        ("frame_duration", C.c_double),
+        ("T_delta_log", C.c_double * 6),
+        ("kf_pose_in_world", C.c_double * 12),
+        ("pose_in_kf", C.c_double * 12),
+        ("pose_global", C.c_double * 12),
+        ("frame_idx", C.c_int32),
+        ("keyframe_count", C.c_int32),
+        ("has_keyframe", C.c_int32),
+        ("pad_", C.c_int32),
+    ]
+
 SIGNATURES = {
     "kds_last_error": (C.c_char_p, []),
     "kds_init": (C.c_int, [_I32, _I32]),
@@ -359,6 +376,8 @@ SIGNATURES = {
     "kds_tracker_add_frames": (C.c_int, [_P, _P, _P, _P, _I32, _P, _P, C.POINTER(TrackerResult), _P]),
     "kds_tracker_get_pose": (C.c_int, [_P, _P, _P]),
     "kds_tracker_get_keyframe": (C.c_int, [_P, C.POINTER(_P), _P]),
+    "kds_tracker_get_state": (C.c_int, [_P, C.POINTER(TrackerState)]),
+    "kds_tracker_set_state": (C.c_int, [_P, C.POINTER(TrackerState), _P]),
     "kds_tracker_reset": (C.c_int, [_P]),
     "kds_tracker_free": (None, [_P]),
     "kds_linearize_static": (C.c_int, [_P, _P, _I32, C.POINTER(AlignerParams), _P, _P, _P, _P, _I32, _P, _P, _P,

@@ -471,6 +471,60 @@ int kds_tracker_get_keyframe(const kds_tracker* t, const kds_tree** kf, double p
   return KDS_OK;
 }
 
+int kds_tracker_get_state(const kds_tracker* t, kds_tracker_state* st) {
+  if (!t || !st) { set_error("kds_tracker_get_state: NULL argument"); return KDS_ERR_INVALID_ARG; }
+  memset(st, 0, sizeof(*st));
+  st->params = t->P;
+  st->last_ts = t->last_ts;
+  st->frame_duration = t->frame_duration;
+  memcpy(st->T_delta_log, t->T_delta_log, sizeof(st->T_delta_log));
+  memcpy(st->kf_pose_in_world, t->kf_pose_in_world.m, sizeof(double) * 12);
+  memcpy(st->pose_in_kf, t->pose_in_kf.m, sizeof(double) * 12);
+  memcpy(st->pose_global, t->pose_global.m, sizeof(double) * 12);
+  st->frame_idx = t->frame_idx;
+  st->keyframe_count = t->keyframe_count;
+  st->has_keyframe = t->keyframe ? 1 : 0;
+  return KDS_OK;
+}
+
+int kds_tracker_set_state(kds_tracker* t, const kds_tracker_state* st, const kds_tree* keyframe) {
+  if (!t || !st) { set_error("kds_tracker_set_state: NULL argument"); return KDS_ERR_INVALID_ARG; }
+  if (st->params.aligner_type != t->P.aligner_type || st->params.motion_model != t->P.motion_model) {
+    set_error("kds_tracker_set_state: the state's aligner type or motion model differs from the tracker's");
+    return KDS_ERR_INVALID_ARG;
+  }
+  if (st->has_keyframe && !keyframe) { set_error("kds_tracker_set_state: the state needs its keyframe tree"); return KDS_ERR_INVALID_ARG; }
+  kds_tree* copy = nullptr;
+  if (st->has_keyframe) {
+    int rc = tree_clone(keyframe, t->stream, &copy);
+    if (rc != KDS_OK) return rc;
+    cudaError_t e = cudaStreamSynchronize(t->stream);
+    if (e != cudaSuccess) {
+      tree_release(copy->d);
+      delete copy;
+      return cuda_status(e, "kds_tracker_set_state", __FILE__, __LINE__);
+    }
+  }
+  if (t->keyframe) {
+    tree_release(t->keyframe->d);
+    delete t->keyframe;
+  }
+  t->keyframe = copy;
+  t->P.motion_model_alpha = st->params.motion_model_alpha;
+  t->P.min_inlier_frac = st->params.min_inlier_frac;
+  t->P.max_kf_trans = st->params.max_kf_trans;
+  t->P.max_kf_rot_deg = st->params.max_kf_rot_deg;
+  t->last_ts = st->last_ts;
+  t->frame_duration = st->frame_duration;
+  memcpy(t->T_delta_log, st->T_delta_log, sizeof(t->T_delta_log));
+  memcpy(t->kf_pose_in_world.m, st->kf_pose_in_world, sizeof(double) * 12);
+  memcpy(t->pose_in_kf.m, st->pose_in_kf, sizeof(double) * 12);
+  memcpy(t->pose_global.m, st->pose_global, sizeof(double) * 12);
+  t->frame_idx = st->frame_idx;
+  t->keyframe_count = st->keyframe_count;
+  return KDS_OK;
+}
+
 int kds_tracker_reset(kds_tracker* t) {
   if (!t) { set_error("kds_tracker_reset: NULL tracker"); return KDS_ERR_INVALID_ARG; }
   motion_reset(t);

@@ -112,6 +112,7 @@ def test_struct_layouts_match_the_c_header(tmp_path):
         pytest.skip("gcc not available")
     checks = [("kds_tracker_params", L.TrackerParams, ["aligner", "motion_model", "max_kf_rot_deg"]),
               ("kds_tracker_result", L.TrackerResult, ["frame_duration", "pose_in_kf", "velocity", "stats"]),
+              ("kds_tracker_state", L.TrackerState, ["last_ts", "T_delta_log", "pose_global", "has_keyframe"]),
               ("kds_aligner_params", L.AlignerParams, ["velocity_damping", "d_score"]),
               ("kds_stats", L.Stats, ["chi2", "pert_vel_norm"])]
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "kds.h"', "int main(void) {"]

@@ -197,3 +197,37 @@ def test_batched_trackers_equal_sequential_trackers(scene):
         ka, _ = a.keyframe()
         kb, _ = b.keyframe()
         assert np.array_equal(ka["mean"], kb["mean"])
+
+
+def test_checkpoint_resume_continues_identically(scene):
+    """A tracker checkpointed after five frames (state + keyframe as a KDTree3f message,
+    through plain bytes and a pickle) and restored into a new tracker gives the same
+    results on the following frames as the original."""
+    import pickle
+
+    import kd_slam2_b200 as kds
+    gen = kds.TreeGeneratorB2003D(**TREE_P)
+
+    def make():
+        return kds.Tracker3D(odom_aligner=kds.CTICPB2003D(max_error=0.5, max_iterations=10, velocity_damping=100.0),
+                             motion_model=kds.ConstVelMotionModel3D(), max_kf_trans=0.5, min_inlier_frac=0.3)
+
+    frames = list(trajectory(scene, 9))
+    a = make()
+    for ts, xyz, st in frames[:5]:
+        a.add_frame(gen.make_tree(xyz, st), ts)
+    ck = pickle.loads(pickle.dumps(a.checkpoint()))
+    b = make()
+    b.restore(ck)
+    assert np.array_equal(a.pose_global(), b.pose_global())
+    for ts, xyz, st in frames[5:]:
+        ra = a.add_frame(gen.make_tree(xyz, st), ts)
+        rb = b.add_frame(gen.make_tree(xyz, st), ts)
+        for key in ("status", "result", "new_keyframe", "frame_idx", "keyframe_count", "stats"):
+            assert ra[key] == rb[key], key
+        for key in ("pose_in_kf", "pose_in_world", "velocity", "ct_velocity"):
+            assert np.array_equal(ra[key], rb[key]), key
+    # a state for another motion model is refused
+    z = kds.Tracker3D(odom_aligner=kds.CTICPB2003D(), motion_model=kds.ZeroVelMotionModel3D())
+    with pytest.raises(kds.KdsError):
+        z.restore(ck)

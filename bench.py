@@ -437,12 +437,14 @@ def tracker_step(frames: int = 24, cpu_frames: int = 6, cpu: bool = True):
         return out, ms
 
     gpu_chain(2)  # warm-up
+    l0 = kds.lib().kds_launch_count()
     res, ms = gpu_chain(frames)
+    launches = kds.lib().kds_launch_count() - l0
     steady = ms[1:]
     line = {"frames": frames, "points_per_frame": int(np.mean([len(x) for _, x, _ in seq[:frames]])),
             "keyframes": int(res[-1]["keyframe_count"]),
             "ms_per_frame_p50": float(np.percentile(steady, 50)), "ms_per_frame_max": float(np.max(steady)),
-            "frames_per_s": 1e3 / float(np.mean(steady)),
+            "frames_per_s": 1e3 / float(np.mean(steady)), "gpu_launches": int(launches),
             "note": "host-timed tree build + add_frame per frame, first frame (keyframe init) excluded"}
     line["many_streams"] = tracker_streams()
     if not cpu:
@@ -521,8 +523,11 @@ def tracker_streams(num_streams: int = 32, frames: int = 8):
         return poses, ms
 
     batched()  # warm-up (graph capture, pools)
+    l0 = kds.lib().kds_launch_count()
     pb, mb = batched()
+    l1 = kds.lib().kds_launch_count()
     ps, msq = one_at_a_time()
+    l2 = kds.lib().kds_launch_count()
     same = all(np.array_equal(a, b) for ra, rb in zip(pb, ps) for a, b in zip(ra, rb))
     fb = num_streams * (frames - 1) / (sum(mb[1:]) / 1e3)
     fs = num_streams * (frames - 1) / (sum(msq[1:]) / 1e3)
@@ -531,6 +536,7 @@ def tracker_streams(num_streams: int = 32, frames: int = 8):
             "batched_frames_per_s": fb, "batched_ms_per_step": float(np.mean(mb[1:])),
             "one_at_a_time_frames_per_s": fs, "one_at_a_time_ms_per_step": float(np.mean(msq[1:])),
             "speedup": fb / fs, "identical_poses": bool(same),
+            "gpu_launches": {"batched": int(l1 - l0), "one_at_a_time": int(l2 - l1)},
             "note": "host-timed steps (one frame of every stream), first step excluded"}
 
 
@@ -547,6 +553,12 @@ def main():
                     help="run only the tracker-step leg and print its JSON (for profiling it)")
     args = ap.parse_args()
     if args.tracker_only:
+        # the same device setup as the full run before its legs
+        import torch
+
+        import kd_slam2_b200 as kds
+        torch.cuda.set_device(0)
+        kds.init(0)
         print(json.dumps({"tracker_step": tracker_step(cpu=not args.no_cpu)}), flush=True)
         return
     if args.warmup < 3:

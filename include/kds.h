@@ -317,6 +317,15 @@ int kds_aligner_count_touched_nodes(kds_aligner* a, int64_t* count);
  * ran the Gauss-Newton step (entry, partials summed, state staged, factorization start,
  * factorized, solved, pose updated, done).  Measurement hook only. */
 int kds_phase_stamps(uint64_t out[16]);
+/* Diagnostics hook (no reference counterpart): the number of polls of the bounded wait
+ * with which each linearization block waits for its TMA copy of the fixed tree's top
+ * nodes into shared memory, on the current device (default 1,048,576).  When that wait
+ * gives up, the block reads the whole tree from global memory instead -- the results are
+ * the same -- and the call returns KDS_ERR_TIMEOUT with its outputs written.  Before
+ * exiting, a block waits again (up to 1,048,576 polls, whatever this setting) so that no
+ * copy outlives it; if even that wait gives up, the error text says so and the CUDA
+ * context should not be used further.  Tests set 0 to exercise the fallback path. */
+int kds_set_tma_wait_limit(int32_t polls);
 void kds_aligner_free(kds_aligner* a);
 
 /* ------------------------------------------------------------------------------
@@ -474,8 +483,11 @@ typedef struct {
   int32_t has_keyframe, pad_;
 } kds_tracker_state;
 int kds_tracker_get_state(const kds_tracker* t, kds_tracker_state* st);
-/* keyframe: required when st->has_keyframe (copied into the tracker); params must match
- * the tracker's aligner type and motion model. */
+/* keyframe: required when st->has_keyframe (copied into the tracker).  st->params must
+ * match the tracker's aligner type, motion model and every aligner parameter (compared
+ * field by field); otherwise the call changes nothing and returns KDS_ERR_INVALID_ARG
+ * naming the first field that differs.  The motion model's alpha and the keyframe
+ * thresholds are taken from the state. */
 int kds_tracker_set_state(kds_tracker* t, const kds_tracker_state* st, const kds_tree* keyframe);
 /* Motion model reset (ZeroVelMotionModel_::reset / ConstVelMotionModel_::reset), keyframe dropped. */
 int kds_tracker_reset(kds_tracker* t);
@@ -583,7 +595,10 @@ void kds_server_free(kds_server* s);
  * The first call on each device resolves the array's address and sets kernel
  * attributes; make that first call before any stream capture.  All calls share the
  * array, so calls that overlap on the GPU (other streams, other threads) race on it.
- * The call blocks until its results have reached the host.  H, b, stats may be NULL. */
+ * The call blocks until its results have reached the host.  H, b, stats may be NULL.
+ * The call has its own error slot inside the array (read back with the outputs in one
+ * copy on `stream`), so it never reports another call's device error.  On
+ * KDS_ERR_TIMEOUT (kds_set_tma_wait_limit) H, b and stats are written and valid. */
 int kds_linearize_static(const kds_tree* fixed, const kds_tree* moving, int32_t type,
                          const kds_aligner_params* params, const double X[12], const double fixed_X[12],
                          const double v[6], const double fixed_v[6], int32_t stats_mode, void* stream, double* H,

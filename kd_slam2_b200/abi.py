@@ -352,6 +352,7 @@ SIGNATURES = {
     "kds_aligner_get_profile": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(_I32)]),
     "kds_aligner_count_touched_nodes": (C.c_int, [_P, C.POINTER(_I64)]),
     "kds_phase_stamps": (C.c_int, [_P]),
+    "kds_set_tma_wait_limit": (C.c_int, [C.c_int32]),
     "kds_aligner_free": (None, [_P]),
     "kds_batch_create": (C.c_int, [C.POINTER(_P)]),
     "kds_batch_run": (C.c_int, [_P, C.POINTER(Job), _I32, _I32, _P]),

@@ -2,10 +2,10 @@
 
     python -m kd_slam2_b200.build          # or kd_slam2_b200.build.build()
 
-kds_tree.cu is compiled with -fmad=false: the tree build must round every multiply
-and add separately so that it reproduces the CPU definition bit for bit.  The
-alignment kernels keep contraction on and use explicit __fmul_rn/__fadd_rn on their
-gating path instead.
+The tree build, the tree operations and the alignment kernels are compiled with
+-fmad=false: they round every multiply and add separately so that they reproduce the
+CPU oracle bit for bit (the alignment kernels also spell their per-leaf and pose
+arithmetic with explicit __fmul_rn/__fadd_rn and __dmul_rn/__dadd_rn).
 """
 from __future__ import annotations
 
@@ -26,7 +26,7 @@ NVCC_COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "
 UNITS = [
     ("kds_tree.cu", ["-fmad=false"]),
     ("kds_build.cu", ["-fmad=false"]),
-    ("kds_align.cu", []),
+    ("kds_align.cu", ["-fmad=false"]),
     ("kds_api.cu", []),
     ("kds_serve.cu", ["-fmad=false"]),
     ("kds_factor.cu", []),

@@ -32,22 +32,27 @@
 
 namespace kds {
 
+// Every float operation of the per-leaf path -- gates, errors and Jacobians -- rounds
+// once, in the operation order of the CPU oracle (itself the reference's order,
+// kd/d3/icp_.h:40-60, kd/d3/cticp_impl_.h:10-73, kd/utils/geometry_3d_impl_.h:143-174):
+// 3-term sums as x0 + (x1 + x2), as Eigen reduces a fixed-size-3 dot product.  So the
+// per-leaf terms, and with the fixed summation order below H and b, are bit-identical
+// to the oracle's.
 __device__ __forceinline__ F3 cross3(F3 a, F3 b) {
-  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+  return f3(fs(fm(a.y, b.z), fm(a.z, b.y)), fs(fm(a.z, b.x), fm(a.x, b.z)), fs(fm(a.x, b.y), fm(a.y, b.x)));
 }
-__device__ __forceinline__ float dot3f(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
-// M = A * B (3x3 row-major), relaxed rounding (Jacobian path only)
+// C = A * B (3x3 row-major), each coefficient a dot3x of a row and a column
 __device__ __forceinline__ void mm3(const float* A, const float* B, float* C) {
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) C[i * 3 + j] = A[i * 3] * B[j] + A[i * 3 + 1] * B[3 + j] + A[i * 3 + 2] * B[6 + j];
+    for (int j = 0; j < 3; ++j)
+      C[i * 3 + j] = fa(fm(A[i * 3], B[j]), fa(fm(A[i * 3 + 1], B[3 + j]), fm(A[i * 3 + 2], B[6 + j])));
 }
-__device__ __forceinline__ F3 mv3(const float* A, F3 p) {
-  return f3(A[0] * p.x + A[1] * p.y + A[2] * p.z, A[3] * p.x + A[4] * p.y + A[5] * p.z,
-            A[6] * p.x + A[7] * p.y + A[8] * p.z);
-}
+__device__ __forceinline__ F3 mv3(const float* A, F3 p) { return mat_vec_x(A, p); }
+// column c of a row-major 3x3
+__device__ __forceinline__ F3 col3(const float* A, int c) { return f3(A[c], A[3 + c], A[6 + c]); }
 
 // Pieces of dRxp (kd/utils/geometry_3d_impl_.h:143-174) shared by both of its calls:
 // R = rodrigues(w) and Q = n n^T + (R^T - I) S / angle, so that
@@ -58,7 +63,7 @@ struct DRxp {
   bool small;
 };
 __device__ __forceinline__ void drxp_setup(F3 w, DRxp& d) {
-  float angle = sqrtf(dot3f(w, w));
+  float angle = __fsqrt_rn(dot3x(w, w));
   d.small = angle < 1e-9f;
   if (d.small) {
 #pragma unroll
@@ -66,17 +71,17 @@ __device__ __forceinline__ void drxp_setup(F3 w, DRxp& d) {
     return;
   }
   rodrigues_x(w, d.R);
-  float inv = 1.0f / angle;
-  F3 n = f3(w.x * inv, w.y * inv, w.z * inv);
+  float inv = __fdiv_rn(1.0f, angle);
+  F3 n = f3(fm(w.x, inv), fm(w.y, inv), fm(w.z, inv));
   float S[9] = {0.f, -n.z, n.y, n.z, 0.f, -n.x, -n.y, n.x, 0.f};
-  float RtmI[9] = {d.R[0] - 1.f, d.R[3], d.R[6], d.R[1], d.R[4] - 1.f, d.R[7], d.R[2], d.R[5], d.R[8] - 1.f};
+  float RtmI[9] = {fs(d.R[0], 1.f), d.R[3], d.R[6], d.R[1], fs(d.R[4], 1.f), d.R[7], d.R[2], d.R[5], fs(d.R[8], 1.f)};
   float A[9];
   mm3(RtmI, S, A);
   float nn[3] = {n.x, n.y, n.z};
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) d.Q[i * 3 + j] = nn[i] * nn[j] + A[i * 3 + j] * inv;
+    for (int j = 0; j < 3; ++j) d.Q[i * 3 + j] = fa(fm(nn[i], nn[j]), fm(A[i * 3 + j], inv));
 }
 // out = Ra * d(R u)/dw  (3x3)
 __device__ __forceinline__ void ra_drxp(const DRxp& d, const float* Ra, F3 u, float* out) {
@@ -98,52 +103,49 @@ __device__ __forceinline__ void ra_drxp(const DRxp& d, const float* Ra, F3 u, fl
 // errorAndJacobianVelocityA (kd/d3/cticp_impl_.h:10-39) -> J[0..5]
 __device__ __forceinline__ void jac_vel_A(const float* Xm, F3 pa_l, F3 na_l, F3 pb_g, F3 nb_g, const float* va, float dt,
                                           float* J) {
-  F3 tm = f3(va[0] * dt, va[1] * dt, va[2] * dt);
-  F3 wa = f3(va[3] * dt, va[4] * dt, va[5] * dt);
+  F3 tm = f3(fm(va[0], dt), fm(va[1], dt), fm(va[2], dt));
+  F3 wa = f3(fm(va[3], dt), fm(va[4], dt), fm(va[5], dt));
   DRxp d;
   drxp_setup(wa, d);
   float Ra[9] = {Xm[0], Xm[1], Xm[2], Xm[4], Xm[5], Xm[6], Xm[8], Xm[9], Xm[10]};
-  F3 pam = mv3(d.R, pa_l);
-  pam = f3(pam.x + tm.x, pam.y + tm.y, pam.z + tm.z);
+  F3 pam = add3x(mv3(d.R, pa_l), tm);
   F3 nam = mv3(d.R, na_l);
-  F3 pag = mv3(Ra, pam);
-  pag = f3(pag.x + Xm[3], pag.y + Xm[7], pag.z + Xm[11]);
+  F3 pag = add3x(mv3(Ra, pam), f3(Xm[3], Xm[7], Xm[11]));
   F3 nag = mv3(Ra, nam);
-  F3 n = f3(nag.x + nb_g.x, nag.y + nb_g.y, nag.z + nb_g.z);
-  F3 dp = f3(pag.x - pb_g.x, pag.y - pb_g.y, pag.z - pb_g.z);
+  F3 n = add3x(nag, nb_g);
+  F3 dp = sub3x(pag, pb_g);
   float A[9], B[9];
   ra_drxp(d, Ra, pa_l, A);
   ra_drxp(d, Ra, na_l, B);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    J[c] = (n.x * Ra[c] + n.y * Ra[3 + c] + n.z * Ra[6 + c]) * dt;
-    J[3 + c] = (n.x * A[c] + n.y * A[3 + c] + n.z * A[6 + c] + dp.x * B[c] + dp.y * B[3 + c] + dp.z * B[6 + c]) * dt;
+    J[c] = fm(dot3x(n, col3(Ra, c)), dt);
+    J[3 + c] = fm(fa(dot3x(n, col3(A, c)), dot3x(dp, col3(B, c))), dt);
   }
 }
 
 // errorAndJacobianVelocityB (kd/d3/cticp_impl_.h:43-73) -> J[0..5]
 __device__ __forceinline__ void jac_vel_B(const float* Xf, F3 pa_g, F3 na_g, F3 pb_l, F3 nb_l, const float* vb, float dt,
                                           float* J) {
-  F3 tm = f3(vb[0] * dt, vb[1] * dt, vb[2] * dt);
-  F3 wb = f3(vb[3] * dt, vb[4] * dt, vb[5] * dt);
+  F3 tm = f3(fm(vb[0], dt), fm(vb[1], dt), fm(vb[2], dt));
+  F3 wb = f3(fm(vb[3], dt), fm(vb[4], dt), fm(vb[5], dt));
   DRxp d;
   drxp_setup(wb, d);
   float Rb[9] = {Xf[0], Xf[1], Xf[2], Xf[4], Xf[5], Xf[6], Xf[8], Xf[9], Xf[10]};
-  F3 pbm = mv3(d.R, pb_l);
-  pbm = f3(pbm.x + tm.x, pbm.y + tm.y, pbm.z + tm.z);
+  F3 pbm = add3x(mv3(d.R, pb_l), tm);
   F3 nbm = mv3(d.R, nb_l);
-  F3 pbg = mv3(Rb, pbm);
-  pbg = f3(pbg.x + Xf[3], pbg.y + Xf[7], pbg.z + Xf[11]);
+  F3 pbg = add3x(mv3(Rb, pbm), f3(Xf[3], Xf[7], Xf[11]));
   F3 nbg = mv3(Rb, nbm);
-  F3 n = f3(na_g.x + nbg.x, na_g.y + nbg.y, na_g.z + nbg.z);
-  F3 dp = f3(pa_g.x - pbg.x, pa_g.y - pbg.y, pa_g.z - pbg.z);
+  F3 n = add3x(na_g, nbg);
+  F3 nn = f3(-n.x, -n.y, -n.z);
+  F3 dp = sub3x(pa_g, pbg);
   float A[9], B[9];
   ra_drxp(d, Rb, pb_l, A);
   ra_drxp(d, Rb, nb_l, B);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    J[c] = -(n.x * Rb[c] + n.y * Rb[3 + c] + n.z * Rb[6 + c]) * dt;
-    J[3 + c] = (-(n.x * A[c] + n.y * A[3 + c] + n.z * A[6 + c]) + dp.x * B[c] + dp.y * B[3 + c] + dp.z * B[6 + c]) * dt;
+    J[c] = fm(dot3x(nn, col3(Rb, c)), dt);
+    J[3 + c] = fm(fa(dot3x(nn, col3(A, c)), dot3x(dp, col3(B, c))), dt);
   }
 }
 
@@ -193,7 +195,7 @@ __device__ __forceinline__ void leaf_term(const CacheF& C, const DNode* F, int f
   if (fabsf(e) > P.max_error) { status = ST_ERR_FN; return; }
   F3 c1 = cross3(pm, nfx), c2 = cross3(pfx, nm);
   J[0] = ns.x; J[1] = ns.y; J[2] = ns.z;
-  J[3] = c1.x + c2.x; J[4] = c1.y + c2.y; J[5] = c1.z + c2.z;
+  J[3] = fa(c1.x, c2.x); J[4] = fa(c1.y, c2.y); J[5] = fa(c1.z, c2.z);
   if (KIND != 0) jac_vel_A(C.Xm, m, n, pfx, nfx, C.v, dt, J + 6);
   float chi2 = fm(e, e);
   float kt = P.kernel_threshold;
@@ -278,10 +280,10 @@ __device__ __forceinline__ void tile_body(const JobIn& Jn, const LinDev& L, cons
 #pragma unroll 8
     for (int l = 0; l < 32; ++l) {
       const float* fr = wf + l * kMaxFS;
-      float val = fr[r] * fr[c] * fr[D + 1];
-      float y = val - comp;
-      float t = s + y;
-      comp = (t - s) - y;
+      float val = fm(fm(fr[r], fr[c]), fr[D + 1]);
+      float y = fs(val, comp);
+      float t = fa(s, y);
+      comp = fs(fs(t, s), y);
       s = t;
     }
     wp[k] = (double)s - (double)comp;
@@ -299,32 +301,82 @@ __device__ __forceinline__ void tile_body(const JobIn& Jn, const LinDev& L, cons
 
 // ---------------------------------------------------------------------------
 // FP64 finalize (one thread) -- ICP_::oneRound / CTICP_::oneRound.
+// Pose algebra in FP64 with one rounding per operation and 3-term sums as
+// x0 + (x1 + x2), the CPU oracle's order for Eigen's Transform product and inverse.
+__device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double ddot3(double a0, double a1, double a2, double b0, double b1, double b2) {
+  return da(dm(a0, b0), da(dm(a1, b1), dm(a2, b2)));
+}
 __device__ void iso_mul_d(const double* A, const double* B, double* C) {
   for (int i = 0; i < 3; ++i) {
-    for (int j = 0; j < 3; ++j)
-      C[i * 4 + j] = A[i * 4] * B[j] + A[i * 4 + 1] * B[4 + j] + A[i * 4 + 2] * B[8 + j];
-    C[i * 4 + 3] = A[i * 4] * B[3] + A[i * 4 + 1] * B[7] + A[i * 4 + 2] * B[11] + A[i * 4 + 3];
+    for (int j = 0; j < 3; ++j) C[i * 4 + j] = ddot3(A[i * 4], A[i * 4 + 1], A[i * 4 + 2], B[j], B[4 + j], B[8 + j]);
+    C[i * 4 + 3] = da(ddot3(A[i * 4], A[i * 4 + 1], A[i * 4 + 2], B[3], B[7], B[11]), A[i * 4 + 3]);
   }
 }
 __device__ void iso_inv_d(const double* A, double* B) {
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) B[i * 4 + j] = A[j * 4 + i];
-  for (int i = 0; i < 3; ++i) B[i * 4 + 3] = -(B[i * 4] * A[3] + B[i * 4 + 1] * A[7] + B[i * 4 + 2] * A[11]);
+  for (int i = 0; i < 3; ++i) B[i * 4 + 3] = -ddot3(A[i], A[4 + i], A[8 + i], A[3], A[7], A[11]);
 }
+
+// Canonical FP64 sine/cosine (this project's own, shared with the CPU oracle so that the
+// pose update is bit-identical there): Cody-Waite reduction by pi/2 with a three-part
+// constant (Cody & Waite 1980; parts of 33, 33 and 53 bits, so q * C1 and q * C2 are
+// exact for |q| < 2^20), then the Taylor series of sin to r^17 and of cos to r^18 on
+// [-pi/4, pi/4] in Horner form (truncation below 1e-19).
+__device__ void sincos_canon_d(double x, double* s_out, double* c_out) {
+  const double q = rint(dm(x, 0x1.45f306dc9c883p-1));
+  const long long j = (long long)q;
+  double r = ds(x, dm(q, 0x1.921fb54400000p+0));
+  r = ds(r, dm(q, 0x1.0b4611a600000p-34));
+  r = ds(r, dm(q, 0x1.3198a2e037073p-69));
+  const double r2 = dm(r, r);
+  double t = 0x1.952c77030ad4ap-49;             // 1/17!
+  t = da(-0x1.ae7f3e733b81fp-41, dm(r2, t));    // 1/15!
+  t = da(0x1.6124613a86d09p-33, dm(r2, t));     // 1/13!
+  t = da(-0x1.ae64567f544e4p-26, dm(r2, t));    // 1/11!
+  t = da(0x1.71de3a556c734p-19, dm(r2, t));     // 1/9!
+  t = da(-0x1.a01a01a01a01ap-13, dm(r2, t));    // 1/7!
+  t = da(0x1.1111111111111p-7, dm(r2, t));      // 1/5!
+  t = da(-0x1.5555555555555p-3, dm(r2, t));     // 1/3!
+  const double sn = da(r, dm(r, dm(r2, t)));
+  double u = -0x1.6827863b97d97p-53;            // 1/18!
+  u = da(0x1.ae7f3e733b81fp-45, dm(r2, u));     // 1/16!
+  u = da(-0x1.93974a8c07c9dp-37, dm(r2, u));    // 1/14!
+  u = da(0x1.1eed8eff8d898p-29, dm(r2, u));     // 1/12!
+  u = da(-0x1.27e4fb7789f5cp-22, dm(r2, u));    // 1/10!
+  u = da(0x1.a01a01a01a01ap-16, dm(r2, u));     // 1/8!
+  u = da(-0x1.6c16c16c16c17p-10, dm(r2, u));    // 1/6!
+  u = da(0x1.5555555555555p-5, dm(r2, u));      // 1/4!
+  u = da(-0.5, dm(r2, u));
+  const double cs = da(1.0, dm(r2, u));
+  switch ((int)(j & 3)) {
+    case 0: *s_out = sn; *c_out = cs; break;
+    case 1: *s_out = cs; *c_out = -sn; break;
+    case 2: *s_out = -sn; *c_out = -cs; break;
+    default: *s_out = -cs; *c_out = sn; break;
+  }
+}
+
+// rodrigues (kd/utils/geometry_3d_impl_.h:37-46) in FP64: I + sin(a) S + (1 - cos(a)) S^2
 __device__ void rodrigues_d(const double* w, double* R) {
-  double a = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+  const double a = sqrt(ddot3(w[0], w[1], w[2], w[0], w[1], w[2]));
   if (a < 1e-9) {
     for (int i = 0; i < 9; ++i) R[i] = (i % 4 == 0) ? 1.0 : 0.0;
     return;
   }
-  double n[3] = {w[0] / a, w[1] / a, w[2] / a};
-  double S[9] = {0, -n[2], n[1], n[2], 0, -n[0], -n[1], n[0], 0};
+  const double inv = 1.0 / a;
+  const double n[3] = {dm(w[0], inv), dm(w[1], inv), dm(w[2], inv)};
+  const double S[9] = {0, -n[2], n[1], n[2], 0, -n[0], -n[1], n[0], 0};
   double s, c;
-  sincos(a, &s, &c);
+  sincos_canon_d(a, &s, &c);
+  const double omc = ds(1.0, c);
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) {
-      double s2 = S[i * 3] * S[j] + S[i * 3 + 1] * S[3 + j] + S[i * 3 + 2] * S[6 + j];
-      R[i * 3 + j] = ((i == j) ? 1.0 : 0.0) + s * S[i * 3 + j] + (1.0 - c) * s2;
+      const double s2 = ddot3(S[i * 3], S[i * 3 + 1], S[i * 3 + 2], S[j], S[3 + j], S[6 + j]);
+      R[i * 3 + j] = da(da((i == j) ? 1.0 : 0.0, dm(s, S[i * 3 + j])), dm(omc, s2));
     }
 }
 __device__ void expmap_d(const double* v, double* X) {
@@ -459,12 +511,18 @@ __device__ void tail_warp(const JobIn& Jn, JobState& S, JobOut& O, kds_stats* lo
 // entry, partials summed, state staged, solve start, factorized, solved, updated, done.
 __device__ int g_phase_on;
 __device__ unsigned long long g_phase[16];
-// Set by a kernel whose bounded wait on a TMA copy gave up; read and cleared by the host.
+// Error bits of a k_linearize launch whose caller passed no error slot of its own (the
+// served loop): 1 = a bounded wait for the tree-top copy gave up and the block read the
+// tree from global memory (results valid); 2 = the copy was still not seen complete when
+// the block was about to exit (the CUDA context is suspect).
 __device__ int g_kernel_error;
+// Polls of the first bounded wait for the tree-top copy (kds_set_tma_wait_limit).  The
+// wait a block makes before it exits always allows 2^20 polls.
+__device__ int g_wait_spins = 1 << 20;
 
 // Bounded wait for the phase with the given parity of an mbarrier to complete.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (int i = 0; i < (1 << 20); ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, int spins = 1 << 20) {
+  for (int i = 0; i < spins; ++i) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -714,11 +772,13 @@ __device__ void tail_warp(const JobIn& Jn, JobState& S, JobOut& O, kds_stats* lo
 }
 
 // One Gauss-Newton iteration over the tiles [tile0, tile0 + gridDim.x) of one kind.
+__device__ __forceinline__ void report_error(int32_t* err, int bits) { atomicOr(err ? err : &g_kernel_error, bits); }
+
 template <int KIND>
 __global__ void __launch_bounds__(kBlock, 4) k_linearize(const JobIn* __restrict__ jobs, JobState* states, JobOut* outs,
                                                       kds_stats* logs, LinDev* lins, const TileDev* __restrict__ tiles,
                                                       int tile0, int stage, double* partials, int32_t* dbg_match,
-                                                      int32_t* dbg_status) {
+                                                      int32_t* dbg_status, int32_t* err) {
   constexpr int D = KindDim<KIND>::D;
   constexpr int M = D * (D + 1) / 2 + D;
   __shared__ CacheF sC;
@@ -754,13 +814,16 @@ __global__ void __launch_bounds__(kBlock, 4) k_linearize(const JobIn* __restrict
   if (threadIdx.x < (int)(sizeof(CacheF) / 4))
     reinterpret_cast<float*>(&sC)[threadIdx.x] = reinterpret_cast<const float*>(&L.cache)[threadIdx.x];
   __syncthreads();
-  if (bytes > 0 && !mbar_wait(mbar, 0u)) {
-    // copy not observed complete: record it, wait once more (bounded), then read
-    // the whole tree from global memory
-    g_kernel_error = 1;
-    mbar_wait(mbar, 0u);
+  if (bytes > 0 && !mbar_wait(mbar, 0u, g_wait_spins)) {
+    // copy not observed complete: record it and read the whole tree from global memory
+    report_error(err, 1);
     nst = 0;
   }
+  // Before the block exits, thread 0 waits (bounded) for the copy to land, so that no
+  // bulk copy into this block's shared memory outlives the block.
+  auto settle = [&]() {
+    if (threadIdx.x == 0 && bytes > 0 && !mbar_wait(mbar, 0u)) report_error(err, 2);
+  };
   if (stamp) g_phase[1] = clock64();
   tile_body<KIND>(Jn, L, sC, T, sN, nst, swp, sfac, dbg_match, dbg_status);
   __syncthreads();
@@ -781,9 +844,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_linearize(const JobIn* __restrict
   }
   __syncthreads();
   if (stamp) g_phase[3] = clock64();
-  if (!s_last) return;
+  if (!s_last) {
+    settle();
+    return;
+  }
   __threadfence();
   job_tail(Jn, S, outs[T.job], logs ? logs + (size_t)T.job * kMaxLog : nullptr, lins, partials, swp, M);
+  settle();
 }
 
 // Resets control state, seeds state from the job inputs and writes the first caches.
@@ -819,8 +886,10 @@ __device__ void init_job(int j, const JobIn* jobs, JobState* states, JobOut* out
   if (!Jn.keep_cache) refresh_caches(S, lins, Jn.lin_begin, Jn.lin_count);
 }
 
-__global__ void k_init_jobs(const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins, int num_jobs) {
+__global__ void k_init_jobs(const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins, int num_jobs,
+                            int32_t* err) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j == 0 && err) *err = 0;
   if (j >= num_jobs) return;
   init_job(j, jobs, states, outs, lins);
 }
@@ -858,7 +927,7 @@ __global__ void k_popc(const uint32_t* bitmap, int64_t words, unsigned long long
 int count_touched(Runner& R, int kind, int64_t fixed_nodes, int64_t* out, cudaStream_t s) {
   *out = 0;
   if (R.num_jobs < 1 || fixed_nodes <= 0) return KDS_OK;
-  k_init_jobs<<<1, 128, 0, s>>>(R.d_jobs, R.d_states, R.d_outs, R.d_lins, 1); ::kds::count_launch();
+  k_init_jobs<<<1, 128, 0, s>>>(R.d_jobs, R.d_states, R.d_outs, R.d_lins, 1, R.d_err); ::kds::count_launch();
   int64_t words = (fixed_nodes + 31) / 32;
   uint32_t* bm = nullptr;
   unsigned long long* cnt = nullptr;
@@ -896,7 +965,7 @@ int Runner::reserve(int nj, int nl, int nt) {
   cap_tiles = std::max({nt, ot + ot / 2, 1});
   size_t bytes = sizeof(JobIn) * cap_jobs + sizeof(JobState) * cap_jobs + sizeof(JobOut) * cap_jobs +
                  sizeof(kds_stats) * kMaxLog * cap_jobs + sizeof(LinDev) * cap_lins + sizeof(TileDev) * cap_tiles +
-                 sizeof(double) * kPStride * cap_tiles + 8 * 256;
+                 sizeof(double) * kPStride * cap_tiles + 9 * 256;
   cudaError_t e = cudaMalloc(&block, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -918,6 +987,7 @@ int Runner::reserve(int nj, int nl, int nt) {
   d_lins = (LinDev*)carve(sizeof(LinDev) * cap_lins);
   d_tiles = (TileDev*)carve(sizeof(TileDev) * cap_tiles);
   d_partials = (double*)carve(sizeof(double) * kPStride * cap_tiles);
+  d_err = (int32_t*)carve(sizeof(int32_t));
   return KDS_OK;
 }
 
@@ -994,6 +1064,12 @@ int phase_stamps(int on, unsigned long long* out16) {
   return KDS_OK;
 }
 
+int set_wait_spins(int32_t spins) {
+  if (spins < 0) { set_error("kds_set_tma_wait_limit: negative limit %d", spins); return KDS_ERR_INVALID_ARG; }
+  KDS_CK(cudaMemcpyToSymbol(g_wait_spins, &spins, sizeof(int32_t)));
+  return KDS_OK;
+}
+
 int Runner::ensure_events(int n) {
   while ((int)prof_ev.size() < n) {
     cudaEvent_t e;
@@ -1021,7 +1097,8 @@ double Runner::profile_mean_ms(int* launches) const {
 
 int Runner::enqueue(cudaStream_t s, int32_t* dbg_match, int32_t* dbg_status) {
   if (num_jobs == 0) return KDS_OK;
-  k_init_jobs<<<(num_jobs + 127) / 128, 128, 0, s>>>(d_jobs, d_states, d_outs, d_lins, num_jobs); ::kds::count_launch();
+  k_init_jobs<<<(num_jobs + 127) / 128, 128, 0, s>>>(d_jobs, d_states, d_outs, d_lins, num_jobs, d_err);
+  ::kds::count_launch();
   int L = max_launches();
   int nk = (kind_count[0] ? 1 : 0) + (kind_count[1] ? 1 : 0) + (kind_count[2] ? 1 : 0);
   prof_launches = profiling ? L * nk : 0;
@@ -1046,15 +1123,15 @@ int Runner::enqueue(cudaStream_t s, int32_t* dbg_match, int32_t* dbg_status) {
       if (kind == 0)
         k_linearize<0><<<kind_count[0], kBlock, stage_bytes, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins,
                                                                      d_tiles, kind_begin[0], stage, d_partials,
-                                                                     dbg_match, dbg_status);
+                                                                     dbg_match, dbg_status, d_err);
       else if (kind == 1)
         k_linearize<1><<<kind_count[1], kBlock, stage_bytes, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins,
                                                                      d_tiles, kind_begin[1], stage, d_partials,
-                                                                     dbg_match, dbg_status);
+                                                                     dbg_match, dbg_status, d_err);
       else
         k_linearize<2><<<kind_count[2], kBlock, stage_bytes, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins,
                                                                      d_tiles, kind_begin[2], stage, d_partials,
-                                                                     dbg_match, dbg_status);
+                                                                     dbg_match, dbg_status, d_err);
       ::kds::count_launch();
       if (profiling) KDS_CK(cudaEventRecordWithFlags(prof_ev[ev++], s, cudaEventRecordExternal));
     }
@@ -1111,16 +1188,23 @@ int Runner::fetch(cudaStream_t s, std::vector<JobOut>& outs, std::vector<kds_sta
     logs->resize((size_t)num_jobs * kMaxLog);
     KDS_CK(cudaMemcpyAsync(logs->data(), d_logs, sizeof(kds_stats) * kMaxLog * num_jobs, cudaMemcpyDeviceToHost, s));
   }
+  int32_t err = 0;
+  KDS_CK(cudaMemcpyAsync(&err, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   KDS_CK(cudaStreamSynchronize(s));
-  int err = 0;
-  KDS_CK(cudaMemcpyFromSymbol(&err, g_kernel_error, sizeof(int)));
-  if (err) {
-    int zero = 0;
-    KDS_CK(cudaMemcpyToSymbol(g_kernel_error, &zero, sizeof(int)));
-    set_error("a bounded wait for a tree-top copy gave up; results were computed from global memory");
-    return KDS_ERR_TIMEOUT;
-  }
-  return KDS_OK;
+  return timeout_status(err);
+}
+
+// KDS_OK, or KDS_ERR_TIMEOUT with a message for the error bits of a launch sequence.
+int timeout_status(int32_t err) {
+  if (!err) return KDS_OK;
+  if (err & 2)
+    set_error("a bounded wait for a tree-top copy gave up and the copy was still not seen complete when its block "
+              "exited: the results were computed from global memory, but the CUDA context should be considered "
+              "unusable");
+  else
+    set_error("a bounded wait for a tree-top copy gave up; the results were computed from global memory and are "
+              "valid");
+  return KDS_ERR_TIMEOUT;
 }
 
 // ---------------------------------------------------------------------------
@@ -1180,13 +1264,13 @@ int launch_linearize(int kind, int ntiles, const JobIn* jobs, JobState* states, 
   const size_t stage_bytes = (size_t)kServeStage * sizeof(DNode);
   if (kind == 0)
     k_linearize<0><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kServeStage,
-                                                       partials, nullptr, nullptr);
+                                                       partials, nullptr, nullptr, nullptr);
   else if (kind == 1)
     k_linearize<1><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kServeStage,
-                                                       partials, nullptr, nullptr);
+                                                       partials, nullptr, nullptr, nullptr);
   else
     k_linearize<2><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kServeStage,
-                                                       partials, nullptr, nullptr);
+                                                       partials, nullptr, nullptr, nullptr);
   count_launch();
   KDS_CK(cudaGetLastError());
   return KDS_OK;
@@ -1235,10 +1319,17 @@ namespace {
 constexpr int kStaticMaxTiles = 512;  // 512 tiles x 128 = 65,536 moving surfels per call
 constexpr int kStaticStage = 2047;    // fixed-tree nodes staged per block (64 KB)
 
+// What the call reads back: the job's outputs and the launch's own error bits.
+struct StaticResult {
+  JobOut out;
+  int32_t err;
+  int32_t pad_[3];
+};
+
 struct StaticScratch {
   JobIn job;
   JobState state;
-  JobOut out;
+  StaticResult res;
   LinDev lin;
   TileDev tiles[kStaticMaxTiles];
   double partials[(size_t)kStaticMaxTiles * kPStride];
@@ -1254,6 +1345,7 @@ __global__ void k_static_setup(StaticScratch* scr, JobIn job, LinDev lin, int nt
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     scr->job = job;
     scr->lin = lin;
+    scr->res.err = 0;
   }
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
     TileDev d;
@@ -1334,37 +1426,30 @@ int linearize_static(const TreeDev& fixed, const TreeDev& moving, int32_t type, 
   for (int i = 0; i < 6; ++i) L.fv[i] = fv ? fv[i] : 0.0;
   k_static_setup<<<1, 256, 0, s>>>(scr, J, L, (int)ntiles);
   count_launch();
-  k_init_jobs<<<1, 128, 0, s>>>(&scr->job, &scr->state, &scr->out, &scr->lin, 1);
+  k_init_jobs<<<1, 128, 0, s>>>(&scr->job, &scr->state, &scr->res.out, &scr->lin, 1, &scr->res.err);
   count_launch();
   if (ntiles > 0) {
     const size_t stage_bytes = (size_t)kStaticStage * sizeof(DNode);
     if (J.kind == 0)
-      k_linearize<0><<<(unsigned)ntiles, kBlock, stage_bytes, s>>>(&scr->job, &scr->state, &scr->out, nullptr,
+      k_linearize<0><<<(unsigned)ntiles, kBlock, stage_bytes, s>>>(&scr->job, &scr->state, &scr->res.out, nullptr,
                                                                   &scr->lin, scr->tiles, 0, kStaticStage,
-                                                                  scr->partials, nullptr, nullptr);
+                                                                  scr->partials, nullptr, nullptr, &scr->res.err);
     else
-      k_linearize<1><<<(unsigned)ntiles, kBlock, stage_bytes, s>>>(&scr->job, &scr->state, &scr->out, nullptr,
+      k_linearize<1><<<(unsigned)ntiles, kBlock, stage_bytes, s>>>(&scr->job, &scr->state, &scr->res.out, nullptr,
                                                                   &scr->lin, scr->tiles, 0, kStaticStage,
-                                                                  scr->partials, nullptr, nullptr);
+                                                                  scr->partials, nullptr, nullptr, &scr->res.err);
     count_launch();
   }
   KDS_CK(cudaGetLastError());
-  JobOut O;
-  KDS_CK(cudaMemcpyAsync(&O, &scr->out, sizeof(JobOut), cudaMemcpyDeviceToHost, s));
+  // outputs and error bits in one copy on the caller's stream
+  StaticResult R;
+  KDS_CK(cudaMemcpyAsync(&R, &scr->res, sizeof(StaticResult), cudaMemcpyDeviceToHost, s));
   KDS_CK(cudaStreamSynchronize(s));
-  int err = 0;
-  KDS_CK(cudaMemcpyFromSymbol(&err, g_kernel_error, sizeof(int)));
-  if (err) {
-    int zero = 0;
-    KDS_CK(cudaMemcpyToSymbol(g_kernel_error, &zero, sizeof(int)));
-    set_error("a bounded wait for a tree-top copy gave up; results were computed from global memory");
-    return KDS_ERR_TIMEOUT;
-  }
   const int D = type == KDS_ICP ? 6 : 12;
-  if (H) memcpy(H, O.H, sizeof(double) * D * D);
-  if (b) memcpy(b, O.b, sizeof(double) * D);
-  if (stats) *stats = O.stats;
-  return KDS_OK;
+  if (H) memcpy(H, R.out.H, sizeof(double) * D * D);
+  if (b) memcpy(b, R.out.b, sizeof(double) * D);
+  if (stats) *stats = R.out.stats;
+  return timeout_status(R.err);
 }
 
 }  // namespace kds

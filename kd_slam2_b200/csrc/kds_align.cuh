@@ -104,6 +104,7 @@ struct Runner {
   LinDev* d_lins = nullptr;
   TileDev* d_tiles = nullptr;
   double* d_partials = nullptr;  // scratch: one kPStride partial per tile
+  int32_t* d_err = nullptr;      // error bits of the last launch sequence (zeroed by k_init_jobs)
   std::vector<JobIn> h_jobs;
   std::vector<LinDev> h_lins;
   std::vector<TileDev> h_tiles;
@@ -137,6 +138,12 @@ struct Runner {
 };
 
 int count_touched(Runner& R, int kind, int64_t fixed_nodes, int64_t* out, cudaStream_t s);
+// KDS_OK for err == 0, else KDS_ERR_TIMEOUT with a message for the error bits of
+// k_linearize (1: a tree-top copy wait gave up, results valid; 2: the copy was not seen
+// complete at block exit, context suspect).
+int timeout_status(int32_t err);
+// Polls of the first bounded wait for the tree-top copy, on the current device.
+int set_wait_spins(int32_t spins);
 // on: 1/0 enables/disables the phase stamps (-1 leaves it); out16 (nullable) receives them
 int phase_stamps(int on, unsigned long long* out16);
 

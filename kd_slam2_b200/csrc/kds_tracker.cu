@@ -493,6 +493,25 @@ int kds_tracker_set_state(kds_tracker* t, const kds_tracker_state* st, const kds
     set_error("kds_tracker_set_state: the state's aligner type or motion model differs from the tracker's");
     return KDS_ERR_INVALID_ARG;
   }
+  {  // the aligner settings decide every later pose: a state saved under others is refused
+    const kds_aligner_params& a = st->params.aligner;
+    const kds_aligner_params& b = t->P.aligner;
+    const char* diff = nullptr;
+    if (a.kernel_threshold != b.kernel_threshold) diff = "kernel_threshold";
+    else if (a.damping != b.damping) diff = "damping";
+    else if (a.max_error != b.max_error) diff = "max_error";
+    else if (a.min_normal_cos != b.min_normal_cos) diff = "min_normal_cos";
+    else if (a.min_good_measurements != b.min_good_measurements) diff = "min_good_measurements";
+    else if (a.max_iterations != b.max_iterations) diff = "max_iterations";
+    else if (a.velocity_damping != b.velocity_damping) diff = "velocity_damping";
+    else if (a.term_crit != b.term_crit) diff = "term_crit";
+    else if (a.d_pert != b.d_pert) diff = "d_pert";
+    else if (a.d_score != b.d_score) diff = "d_score";
+    if (diff) {
+      set_error("kds_tracker_set_state: the state's aligner parameter %s differs from the tracker's", diff);
+      return KDS_ERR_INVALID_ARG;
+    }
+  }
   if (st->has_keyframe && !keyframe) { set_error("kds_tracker_set_state: the state needs its keyframe tree"); return KDS_ERR_INVALID_ARG; }
   kds_tree* copy = nullptr;
   if (st->has_keyframe) {

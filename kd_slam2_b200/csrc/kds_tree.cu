@@ -290,7 +290,8 @@ int tree_import(const float* mean, const float* dir, const double* dts_mean, con
   size_t nb = num_nodes;
   void* stg = nullptr;
   size_t bytes = nb * (3 * 4 * 2 + 8 * 2 + 8 * 2 + 4 * 2) + 64;
-  cudaError_t ce = cudaMalloc(&stg, bytes);
+  // staging from the stream-ordered pool: no device-wide synchronisation on release
+  cudaError_t ce = cudaMallocAsync(&stg, bytes, s);
   if (ce != cudaSuccess) { cudaGetLastError(); tree_release(t->d); delete t; set_error("import staging OOM"); return KDS_ERR_OOM; }
   char* p = (char*)stg;
   float* dm = (float*)p; p += nb * 12;
@@ -332,8 +333,8 @@ static int import_finish(kds_tree* t, int32_t* flag, int32_t* rank, int32_t* til
   tree_gather_leaves(t->d, s);
   int32_t bad = 0;
   cudaMemcpyAsync(&bad, dbad, 4, cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(stg, s);
   cudaError_t ce = cudaStreamSynchronize(s);
-  cudaFree(stg);
   if (ce != cudaSuccess || rc2) {
     tree_release(t->d);
     delete t;
@@ -373,7 +374,7 @@ int tree_from_msg(const kds_kdtree3f* msg, kds_tree** out) {
   // staging: the raw records, then three int32 arrays and two flags
   void* stg = nullptr;
   const size_t rec_bytes = (((size_t)n * sizeof(kds_kdnode3f)) + 255) & ~(size_t)255;
-  cudaError_t ce = cudaMalloc(&stg, rec_bytes + (size_t)n * 12 + 64);
+  cudaError_t ce = cudaMallocAsync(&stg, rec_bytes + (size_t)n * 12 + 64, s);
   if (ce != cudaSuccess) {
     cudaGetLastError();
     tree_release(t->d);

@@ -93,6 +93,13 @@ def load() -> C.CDLL:
                                   C.POINTER(OPrior), P, P, P, C.c_int32, C.c_int32, C.POINTER(OResult)]),
         "orc_linearize": (None, [C.c_int32, P, P, P, P, P, C.POINTER(AlignParams), C.c_int32, P, P, P, P,
                                  C.POINTER(OStats)]),
+        "orc_align_recorded": (C.c_int32, [C.c_int32, P, P, C.c_int32, P, C.POINTER(AlignParams), P, P, P,
+                                           C.POINTER(OResult), P, P]),
+        "orc_align_replay64": (None, [C.c_int32, P, P, C.c_int32, P, C.POINTER(AlignParams), P, P, P, C.c_int32,
+                                      P, P]),
+        "orc_sincos_canon_d": (None, [C.c_double, P, P]),
+        "orc_product_caches": (None, [P, P, P]),
+        "orc_pose_hessian": (C.c_int32, [P, P]),
         "orc_sincosf": (None, [C.c_float, P, P]),
         "orc_err_jac_vel_A": (None, [C.c_int32, P, P, P, P, P, P, P, P, C.c_double]),
         "orc_err_jac_vel_B": (None, [C.c_int32, P, P, P, P, P, P, P, P, C.c_double]),
@@ -222,6 +229,59 @@ def align(kind: int, mode: int, fixed, moving: OTree, params: AlignParams, X0, v
             "stats": res.stats.as_dict(), "log": [res.log[i].as_dict() for i in range(min(res.iterations, 64))]}
 
 
+def _fixed_entries(fixed, fixed_X):
+    if isinstance(fixed, OTree):
+        fixed = [(fixed, np.eye(3, 4) if fixed_X is None else fixed_X)]
+    hs = (C.c_void_p * len(fixed))(*[f.h for f, _ in fixed])
+    FX = np.ascontiguousarray(np.stack([np.asarray(x, np.float64).reshape(12) for _, x in fixed]))
+    return fixed, hs, FX
+
+
+def align_recorded(kind: int, fixed, moving: OTree, params: AlignParams, X0, v0=None, fixed_X=None, fixed_v=None):
+    """MODE_MIXED compute() (the product's semantics and summation order) that also
+    returns every iteration's correspondences and status, shape (iterations, entries,
+    moving leaves), for align_replay64."""
+    lib = load()
+    fixed, hs, FX = _fixed_entries(fixed, fixed_X)
+    X = np.ascontiguousarray(np.asarray(X0, np.float64).reshape(12)).copy()
+    v = np.zeros(6) if v0 is None else np.ascontiguousarray(v0, np.float64).copy()
+    fv = np.zeros(6) if fixed_v is None else np.ascontiguousarray(fixed_v, np.float64)
+    nl = moving.num_leaves
+    cap = max(1, params.max_iterations) * len(fixed) * nl
+    match = np.zeros(cap, np.int32)
+    status = np.zeros(cap, np.int32)
+    res = OResult()
+    ret = lib.orc_align_recorded(kind, hs, FX.ctypes.data, len(fixed), moving.h, C.byref(params), X.ctypes.data,
+                                 v.ctypes.data, fv.ctypes.data, C.byref(res), match.ctypes.data, status.ctypes.data)
+    it = res.iterations
+    shape = (it, len(fixed), nl)
+    return {"ret": ret, "X": X.reshape(3, 4), "v": v, "iterations": it,
+            "match": match[:it * len(fixed) * nl].reshape(shape), "status": status[:it * len(fixed) * nl].reshape(shape)}
+
+
+def align_replay64(kind: int, fixed, moving: OTree, params: AlignParams, X0, match, status, v0=None, fixed_X=None,
+                   fixed_v=None):
+    """All-FP64 Gauss-Newton steps that reuse recorded correspondences and inlier sets
+    (one step per recorded iteration): the arithmetic error of the FP32 per-leaf terms
+    with every branch held fixed.  Returns (X, v)."""
+    lib = load()
+    fixed, hs, FX = _fixed_entries(fixed, fixed_X)
+    X = np.ascontiguousarray(np.asarray(X0, np.float64).reshape(12)).copy()
+    v = np.zeros(6) if v0 is None else np.ascontiguousarray(v0, np.float64).copy()
+    fv = np.zeros(6) if fixed_v is None else np.ascontiguousarray(fixed_v, np.float64)
+    m = np.ascontiguousarray(match, np.int32)
+    st = np.ascontiguousarray(status, np.int32)
+    lib.orc_align_replay64(kind, hs, FX.ctypes.data, len(fixed), moving.h, C.byref(params), X.ctypes.data,
+                           v.ctypes.data, fv.ctypes.data, int(m.shape[0]), m.ctypes.data, st.ctypes.data)
+    return X.reshape(3, 4), v
+
+
+def sincos_canon_d(x: float):
+    s, c = C.c_double(), C.c_double()
+    load().orc_sincos_canon_d(float(x), C.byref(s), C.byref(c))
+    return s.value, c.value
+
+
 def linearize(kind: int, fixed: OTree, moving: OTree, caches36, params: AlignParams, v=None, fixed_v=None,
               stats_mode: bool = False):
     lib = load()
@@ -252,6 +312,24 @@ def sincosf(x: float):
     s, c = C.c_float(), C.c_float()
     load().orc_sincosf(x, C.byref(s), C.byref(c))
     return s.value, c.value
+
+
+def pose_hessian(H12) -> np.ndarray:
+    """CTICP_::poseHessian: Schur complement of a 12x12 CT-ICP H over its velocity block."""
+    H = np.ascontiguousarray(np.asarray(H12, np.float64).reshape(144))
+    out = np.zeros(36)
+    if not load().orc_pose_hessian(H.ctypes.data, out.ctypes.data):
+        raise ValueError("velocity block is singular")
+    return out.reshape(6, 6)
+
+
+def product_caches(X, Xf=None) -> np.ndarray:
+    """Float caches Xm, Xf, Xmf exactly as the product derives them from FP64 poses."""
+    X = np.ascontiguousarray(np.asarray(X, np.float64).reshape(12))
+    Xf = np.ascontiguousarray(np.eye(3, 4) if Xf is None else np.asarray(Xf, np.float64).reshape(12))
+    out = np.zeros(36, np.float32)
+    load().orc_product_caches(X.ctypes.data, Xf.ctypes.data, out.ctypes.data)
+    return out
 
 
 def caches_from(X, Xf=None) -> np.ndarray:

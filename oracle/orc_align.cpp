@@ -20,12 +20,15 @@
 //   MODE_REF32  float everywhere, StableAdder_ sums over num_threads chunks, float LDLT
 //               and pose update -- the reference CPU path as written.
 //   MODE_MIXED  float per-leaf terms, FP64 sums / solve / pose -- the product's
-//               semantics up to summation order.
+//               semantics, in the product's own summation order (128-leaf tiles, warp
+//               Kahan sums, FP64 partials), its Cholesky and its canonical FP64 expmap,
+//               so that a run is bit-identical to the GPU's.
 //   MODE_FP64   everything in double -- the precision reference.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <future>
+#include <type_traits>
 #include <vector>
 
 #include "orc_align.hpp"
@@ -129,9 +132,12 @@ void err_jac_vel_B(T& e, T* J, const Iso<T>& Tb, const V3<T>& pa_g, const V3<T>&
   for (int i = 0; i < 6; ++i) J[i] = J[i] * dt;
 }
 
+// forced_status >= 0 replays a recorded correspondence: the fixed leaf is forced_match,
+// the gates are skipped and the leaf contributes iff forced_status is inlier or outlier
+// (the robust weight is recomputed in T from the error).
 template <class T>
 static LeafRes<T> leaf_term(int kind, const Tree& F, const Node& ml, const Cache<T>& C, const T* vel, const T* fvel,
-                            const AlignParams& P, bool stats_mode) {
+                            const AlignParams& P, bool stats_mode, int forced_match = -1, int forced_status = -1) {
   LeafRes<T> r;
   for (int i = 0; i < 18; ++i) r.J[i] = T(0);
   V3<T> m = nmean<T>(ml), nrm = ndir<T>(ml);
@@ -139,8 +145,10 @@ static LeafRes<T> leaf_term(int kind, const Tree& F, const Node& ml, const Cache
   T dt = (T)ml.dts_mean;
   if (kind != KIND_ICP) warp_leaf(vel, dt, m, nrm, mw, nw);
   V3<T> p_mif = apply_iso(C.Xmf, mw);
-  int idx = descend(F, p_mif);
+  const bool forced = forced_status >= 0;
+  int idx = forced ? forced_match : descend(F, p_mif);
   r.match = idx;
+  if (forced && forced_status != ST_INLIER && forced_status != ST_OUTLIER) { r.status = forced_status; return r; }
   if (idx < 0) { r.status = ST_BAD; return r; }
   const Node& fl = F.nodes[idx];
   V3<T> pf = nmean<T>(fl), nf = ndir<T>(fl);
@@ -149,10 +157,10 @@ static LeafRes<T> leaf_term(int kind, const Tree& F, const Node& ml, const Cache
   V3<T> p_fixed = apply_iso(C.Xf, pf);
   V3<T> n_fixed = apply_rot(C.Xf, nf);
   // ICP_3D_Traits::errorAndJacobian
-  if (dot3(n_fixed, n_moving) < (T)P.min_normal_cos) { r.status = ST_ERR_NORMAL; return r; }
+  if (!forced && dot3(n_fixed, n_moving) < (T)P.min_normal_cos) { r.status = ST_ERR_NORMAL; return r; }
   V3<T> ns = vadd(n_moving, n_fixed);
   T e = dot3(vsub(p_moving, p_fixed), ns);
-  if (std::fabs(e) > (T)P.max_error) { r.status = ST_ERR_FN; return r; }
+  if (!forced && std::fabs(e) > (T)P.max_error) { r.status = ST_ERR_FN; return r; }
   V3<T> jr = vadd(cross(p_moving, n_fixed), cross(p_fixed, n_moving));
   for (int i = 0; i < 3; ++i) { r.J[i] = ns[i]; r.J[3 + i] = jr[i]; }
   if (kind != KIND_ICP) {
@@ -247,6 +255,111 @@ template <class T> static void leaf_stats(const LeafRes<T>& r, StatsAcc<T>& s) {
   }
   s.chi2 = r.chi2;
   s.chi2k = r.chi2 * r.gamma;
+}
+
+// ---------------------------------------------------------------------------
+// The product's summation order (kd_slam2_b200/csrc/kds_align.cu: tile_body,
+// k_linearize, job_tail), restated so that MODE_MIXED's H and b are bit-identical to
+// the GPU's.  The moving leaves are cut into tiles of 128 (per fixed entry, in leaf
+// order), a tile into 4 warps of 32 lanes (lane = leaf, missing leaves count as zero
+// rows).  Per warp and packed entry (r, c): a float Kahan sum over the 32 lanes of
+// (J_r * J_c) * gamma (c = D: J_r * e * gamma), then s - comp in double.  The warp
+// sums of chi2 and gamma * chi2 (doubles) are the xor-butterfly over offsets 16..1.
+// The tile partial is ((((0 + w0) + w1) + w2) + w3); the job's sum runs over its tiles
+// in order into 4 interleaved accumulators, combined as (a0 + a1) + (a2 + a3).
+constexpr int kTileLeaves = 128;
+constexpr int kPartStride = 200;  // doubles per tile partial
+constexpr int kPartStats = 192;   // 7 stats values: counts x5, chi2, chi2 kernelized
+
+static void packed_rc(int D, int k, int& r, int& c) {
+  int T = D * (D + 1) / 2;
+  if (k >= T) { r = k - T; c = D; return; }
+  int rr = 0, off = 0;
+  while (off + (D - rr) <= k) { off += D - rr; ++rr; }
+  r = rr;
+  c = rr + (k - off);
+}
+
+static double butterfly32(const double* v) {
+  double a[32], b[32];
+  for (int l = 0; l < 32; ++l) a[l] = v[l];
+  for (int off = 16; off > 0; off >>= 1) {
+    for (int l = 0; l < 32; ++l) b[l] = a[l] + a[l ^ off];
+    for (int l = 0; l < 32; ++l) a[l] = b[l];
+  }
+  return a[0];
+}
+
+// Appends one partial per tile of Mv's leaves against F.
+static void gpu_tile_partials(int kind, const Tree& F, const Tree& Mv, const Cache<float>& C, const float* vel,
+                              const float* fvel, const AlignParams& P, bool stats_mode, std::vector<double>& parts,
+                              int32_t* match_out, int32_t* status_out, int32_t* rec_match, int32_t* rec_status) {
+  const int D = kind_dim(kind);
+  const int K = packed_dim(D);
+  const size_t n = Mv.leaves.size();
+  for (size_t b0 = 0; b0 < n; b0 += kTileLeaves) {
+    double wp[4][kPartStride];
+    for (int w = 0; w < 4; ++w) {
+      float rows[32][20];
+      double chi2[32], chi2k[32];
+      int cnt[5] = {0, 0, 0, 0, 0};
+      for (int l = 0; l < 32; ++l) {
+        const size_t i = b0 + (size_t)w * 32 + l;
+        bool contrib = false;
+        LeafRes<float> r;
+        if (i < n) {
+          const Node& ml = Mv.nodes[Mv.leaves[i]];
+          r = leaf_term(kind, F, ml, C, vel, fvel, P, stats_mode);
+          if (match_out) { match_out[i] = r.match; status_out[i] = r.status; }
+          if (rec_match) { rec_match[i] = r.match; rec_status[i] = r.status; }
+          contrib = r.status == ST_INLIER || r.status == ST_OUTLIER;
+          cnt[r.status] += 1;
+        }
+        for (int k = 0; k < D; ++k) rows[l][k] = contrib ? r.J[k] : 0.f;
+        rows[l][D] = contrib ? r.e : 0.f;
+        rows[l][D + 1] = contrib ? r.gamma : 0.f;
+        chi2[l] = contrib ? (double)(r.e * r.e) : 0.0;
+        chi2k[l] = contrib ? (double)((r.e * r.e) * r.gamma) : 0.0;
+      }
+      for (int k = 0; k < K; ++k) {
+        int rr, cc;
+        packed_rc(D, k, rr, cc);
+        float s = 0.f, comp = 0.f;
+        for (int l = 0; l < 32; ++l) {
+          float val = (rows[l][rr] * rows[l][cc]) * rows[l][D + 1];
+          float y = val - comp;
+          float t = s + y;
+          comp = (t - s) - y;
+          s = t;
+        }
+        wp[w][k] = (double)s - (double)comp;
+      }
+      for (int q = 0; q < 5; ++q) wp[w][kPartStats + q] = (double)cnt[q];
+      wp[w][kPartStats + 5] = butterfly32(chi2);
+      wp[w][kPartStats + 6] = butterfly32(chi2k);
+    }
+    const size_t o = parts.size();
+    parts.resize(o + kPartStride, 0.0);
+    for (int k = 0; k < kPartStride; ++k) {
+      if ((k >= K && k < kPartStats) || k >= kPartStats + 7) continue;
+      double acc = 0.0;
+      for (int w = 0; w < 4; ++w) acc += wp[w][k];
+      parts[o + k] = acc;
+    }
+  }
+}
+
+// The job's sum of its tile partials (job_tail): 4 interleaved accumulators in tile order.
+static void gpu_reduce_tiles(const std::vector<double>& parts, double* red) {
+  const size_t nt = parts.size() / kPartStride;
+  for (int k = 0; k < kPartStride; ++k) {
+    double a4[4] = {0.0, 0.0, 0.0, 0.0};
+    size_t t = 0;
+    for (; t + 4 <= nt; t += 4)
+      for (int u = 0; u < 4; ++u) a4[u] += parts[(t + u) * kPartStride + k];
+    for (; t < nt; ++t) a4[0] += parts[t * kPartStride + k];
+    red[k] = (a4[0] + a4[1]) + (a4[2] + a4[3]);
+  }
 }
 
 // One linearization over all moving leaves against one fixed tree.
@@ -357,10 +470,21 @@ template <class T> static T score_of(const OStats& s) {
   return (T)(ratio / (s.chi2_kernelized / (float)s.num_inliers + 1e-6f));
 }
 
+// gpu_order (MODE_MIXED): the product's summation order, Cholesky and canonical expmap,
+// so that every iteration is bit-identical to the GPU's.  rec (nullable) receives the
+// correspondences and status of every iteration (iteration-major, fixed entries in
+// order, leaves in order) for the FP64 replay.
+struct Record {
+  std::vector<int32_t> match, status;
+};
+
 template <class StateT, class LeafT, class SumT>
 static int run_align(int kind, const std::vector<const Tree*>& fixed, const std::vector<Iso<double>>& fixed_X,
                      const Tree& Mv, const AlignParams& P, const OPrior* prior, double* X12, double* v6,
-                     const double* fv6, int stats_mode, bool stable_adder, int num_threads, OResult* out) {
+                     const double* fv6, int stats_mode, bool stable_adder, int num_threads, OResult* out,
+                     bool gpu_order = false, Record* rec = nullptr) {
+  constexpr bool kMixed = std::is_same<StateT, double>::value && std::is_same<LeafT, float>::value &&
+                          std::is_same<SumT, double>::value;
   const int D = (kind == KIND_ICP) ? 6 : 12;
   const int K = packed_dim(D);
   Iso<StateT> X = iso_from12<StateT>(X12);
@@ -379,7 +503,38 @@ static int run_align(int kind, const std::vector<const Tree*>& fixed, const std:
     for (int i = 0; i < 6; ++i) vl[i] = (LeafT)v[i];
     for (int k = 0; k < K; ++k) Hb[k] = SumT(0);
     StatsAcc<SumT> st;
-    for (size_t f = 0; f < fixed.size(); ++f) {
+    bool done_sum = false;
+    if constexpr (kMixed) {
+      if (gpu_order) {
+        std::vector<double> parts;
+        const size_t nl = Mv.leaves.size();
+        size_t r0 = 0;
+        if (rec) {
+          r0 = rec->match.size();
+          rec->match.resize(r0 + nl * fixed.size());
+          rec->status.resize(r0 + nl * fixed.size());
+        }
+        for (size_t f = 0; f < fixed.size(); ++f) {
+          Iso<StateT> Xf = iso_cast<StateT>(fixed_X[f]);
+          Cache<LeafT> C = make_cache<StateT, LeafT>(X, Xf);
+          gpu_tile_partials(kind, *fixed[f], Mv, C, vl, fvl, P, stats_mode != 0, parts, nullptr, nullptr,
+                            rec ? rec->match.data() + r0 + f * nl : nullptr,
+                            rec ? rec->status.data() + r0 + f * nl : nullptr);
+        }
+        double red[kPartStride];
+        gpu_reduce_tiles(parts, red);
+        for (int k = 0; k < K; ++k) Hb[k] = red[k];
+        st.ni = (int)red[kPartStats + 0];
+        st.no = (int)red[kPartStats + 1];
+        st.nb = (int)red[kPartStats + 2];
+        st.nn = (int)red[kPartStats + 3];
+        st.nf = (int)red[kPartStats + 4];
+        st.chi2 = red[kPartStats + 5];
+        st.chi2k = red[kPartStats + 6];
+        done_sum = true;
+      }
+    }
+    for (size_t f = 0; f < fixed.size() && !done_sum; ++f) {
       Iso<StateT> Xf = iso_cast<StateT>(fixed_X[f]);
       Cache<LeafT> C = make_cache<StateT, LeafT>(X, Xf);
       StatsAcc<SumT> s1;
@@ -450,7 +605,14 @@ static int run_align(int kind, const std::vector<const Tree*>& fixed, const std:
       A[i * D + i] += (i < 6) ? (StateT)P.damping : (StateT)P.velocity_damping;
       rhs[i] = -b[i];
     }
-    ldlt_solve<StateT>(D, A, rhs, dx);
+    bool solved = false;
+    if constexpr (kMixed) {
+      if (gpu_order) {
+        chol_solve_cols(D, A, rhs, dx);
+        solved = true;
+      }
+    }
+    if (!solved) ldlt_solve<StateT>(D, A, rhs, dx);
     for (int i = 0; i < D; ++i) out->dx[i] = (double)dx[i];
     StateT pp = 0, pv = 0;
     for (int i = 0; i < 6; ++i) pp += dx[i] * dx[i];
@@ -461,7 +623,15 @@ static int run_align(int kind, const std::vector<const Tree*>& fixed, const std:
     }
     out->stats = S;
     if (!stats_mode) {
-      Iso<StateT> dX = expmap<StateT>(dx);
+      Iso<StateT> dX;
+      bool canon = false;
+      if constexpr (kMixed) {
+        if (gpu_order) {
+          dX = expmap_canon(dx);
+          canon = true;
+        }
+      }
+      if (!canon) dX = expmap<StateT>(dx);
       X = iso_mul(dX, X);
       if (D == 12)
         for (int i = 0; i < 6; ++i) v[i] += dx[6 + i];
@@ -493,7 +663,7 @@ int align(int kind, int mode, const std::vector<const Tree*>& fixed, const std::
                                           num_threads, out);
   if (mode == MODE_MIXED)
     return run_align<double, float, double>(kind, fixed, fixed_X, moving, P, prior, X12, v6, fv6, stats_mode, false,
-                                            1, out);
+                                            1, out, true);
   return run_align<double, double, double>(kind, fixed, fixed_X, moving, P, prior, X12, v6, fv6, stats_mode, false,
                                            1, out);
 }
@@ -507,13 +677,21 @@ void linearize_at(int kind, const Tree& F, const Tree& Mv, const float* caches36
   C.Xf = iso_from12<float>(caches36 + 12);
   C.Xmf = iso_from12<float>(caches36 + 24);
   const int D = kind_dim(kind);
-  const int K = packed_dim(D);
-  std::vector<double> Hb(K);
-  StatsAcc<double> st;
   float vz[6] = {0, 0, 0, 0, 0, 0};
-  linearize<float, double>(kind, F, Mv, C, v6 ? v6 : vz, fv6 ? fv6 : vz, P, stats_mode != 0, false, 1, Hb.data(),
-                           st, match_out, status_out);
-  unpack_Hb(D, Hb.data(), H_out, b_out);
+  std::vector<double> parts;
+  gpu_tile_partials(kind, F, Mv, C, v6 ? v6 : vz, fv6 ? fv6 : vz, P, stats_mode != 0, parts, match_out, status_out,
+                    nullptr, nullptr);
+  double red[kPartStride];
+  gpu_reduce_tiles(parts, red);
+  StatsAcc<double> st;
+  st.ni = (int)red[kPartStats + 0];
+  st.no = (int)red[kPartStats + 1];
+  st.nb = (int)red[kPartStats + 2];
+  st.nn = (int)red[kPartStats + 3];
+  st.nf = (int)red[kPartStats + 4];
+  st.chi2 = red[kPartStats + 5];
+  st.chi2k = red[kPartStats + 6];
+  unpack_Hb(D, red, H_out, b_out);
   st_out->num_inliers = st.ni; st_out->num_outliers = st.no; st_out->num_bad = st.nb;
   st_out->num_err_normal = st.nn; st_out->num_err_fn = st.nf;
   st_out->chi2 = (float)st.chi2;
@@ -530,5 +708,119 @@ template void err_jac_vel_A<double>(double&, double*, const Iso<double>&, const 
                                     const V3<double>&, const V3<double>&, const double*, double);
 template void err_jac_vel_B<double>(double&, double*, const Iso<double>&, const V3<double>&, const V3<double>&,
                                     const V3<double>&, const V3<double>&, const double*, double);
+
+
+// CTICP_::poseHessian (kd/cticp/cticp_.h:169-177): the pose-only information matrix of
+// a 12x12 CT-ICP H by the Schur complement over the velocity block,
+// H_pp - H_pv (H_vv + 1e-9 I)^-1 H_pv^T, in FP64.  The inverse is Gauss-Jordan
+// elimination with partial pivoting (Eigen's .inverse() of a 6x6 is partial-pivoting LU).
+// Returns false when the velocity block is singular.
+bool pose_hessian(const double* H12, double* out36) {
+  double A[6][12];
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) {
+      A[i][j] = H12[(6 + i) * 12 + 6 + j] + (i == j ? 1e-9 : 0.0);
+      A[i][6 + j] = (i == j) ? 1.0 : 0.0;
+    }
+  for (int c = 0; c < 6; ++c) {
+    int p = c;
+    for (int r = c + 1; r < 6; ++r)
+      if (std::fabs(A[r][c]) > std::fabs(A[p][c])) p = r;
+    if (A[p][c] == 0.0) return false;
+    if (p != c)
+      for (int k = 0; k < 12; ++k) std::swap(A[p][k], A[c][k]);
+    const double d = A[c][c];
+    for (int k = 0; k < 12; ++k) A[c][k] = A[c][k] / d;
+    for (int r = 0; r < 6; ++r) {
+      if (r == c) continue;
+      const double f = A[r][c];
+      for (int k = 0; k < 12; ++k) A[r][k] = A[r][k] - f * A[c][k];
+    }
+  }
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) {
+      double acc = 0.0;  // (H_pv Hvv^-1 H_pv^T)_ij
+      for (int k = 0; k < 6; ++k) {
+        double t = 0.0;
+        for (int l = 0; l < 6; ++l) t += A[k][6 + l] * H12[j * 12 + 6 + l];
+        acc += H12[i * 12 + 6 + k] * t;
+      }
+      out36[i * 6 + j] = H12[i * 12 + j] - acc;
+    }
+  return true;
+}
+
+// The float caches (Xm, Xf, Xmf) the product derives from FP64 poses at the start of
+// every iteration, with its operation order (make_cache).
+void product_caches(const double* X12, const double* Xf12, float* out36) {
+  Cache<float> c = make_cache<double, float>(iso_from12<double>(X12), iso_from12<double>(Xf12));
+  iso_to12(c.Xm, out36);
+  iso_to12(c.Xf, out36 + 12);
+  iso_to12(c.Xmf, out36 + 24);
+}
+
+// MODE_MIXED run that also returns every iteration's correspondences and status.
+int align_recorded(int kind, const std::vector<const Tree*>& fixed, const std::vector<Iso<double>>& fixed_X,
+                   const Tree& moving, const AlignParams& P, double* X12, double* v6, const double* fv6,
+                   OResult* out, std::vector<int32_t>& match, std::vector<int32_t>& status) {
+  std::memset(out, 0, sizeof(OResult));
+  Record rec;
+  int ret = run_align<double, float, double>(kind, fixed, fixed_X, moving, P, nullptr, X12, v6, fv6, 0, false, 1, out,
+                                             true, &rec);
+  match.swap(rec.match);
+  status.swap(rec.status);
+  return ret;
+}
+
+// FP64 replay of a recorded run: `iterations` Gauss-Newton steps in all-FP64 arithmetic
+// (per-leaf terms, sums, LDL^T solve, expmap with libm sine/cosine), where iteration it
+// uses the recorded fixed leaf of every moving leaf and lets exactly the recorded
+// inliers and outliers contribute (the robust weight is recomputed in FP64 from the
+// FP64 error).  The distance of its pose from the recorded run's is the arithmetic
+// error of the FP32 per-leaf terms alone, with every branch held fixed.
+void align_replay64(int kind, const std::vector<const Tree*>& fixed, const std::vector<Iso<double>>& fixed_X,
+                    const Tree& Mv, const AlignParams& P, double* X12, double* v6, const double* fv6, int iterations,
+                    const int32_t* match, const int32_t* status) {
+  const int D = (kind == KIND_ICP) ? 6 : 12;
+  const int K = packed_dim(D);
+  Iso<double> X = iso_from12<double>(X12);
+  double v[6], fv[6];
+  for (int i = 0; i < 6; ++i) {
+    v[i] = kind == KIND_ICP ? 0.0 : v6[i];
+    fv[i] = fv6 ? fv6[i] : 0.0;
+  }
+  const size_t nl = Mv.leaves.size();
+  std::vector<double> Hb(K), item(K);
+  for (int it = 0; it < iterations; ++it) {
+    for (int k = 0; k < K; ++k) Hb[k] = 0.0;
+    for (size_t f = 0; f < fixed.size(); ++f) {
+      Cache<double> C = make_cache<double, double>(X, fixed_X[f]);
+      const size_t base = ((size_t)it * fixed.size() + f) * nl;
+      for (size_t i = 0; i < nl; ++i) {
+        const Node& ml = Mv.nodes[Mv.leaves[i]];
+        LeafRes<double> r = leaf_term(kind, *fixed[f], ml, C, v, fv, P, false, match[base + i], status[base + i]);
+        if (r.status != ST_INLIER && r.status != ST_OUTLIER) continue;
+        const double kt = (double)P.kernel_threshold;
+        r.gamma = r.chi2 > kt ? std::sqrt(kt / r.chi2) : 1.0;
+        pack_item(r, D, item.data());
+        for (int k = 0; k < K; ++k) Hb[k] += item[k];
+      }
+    }
+    double H[144], b[12], A[144], rhs[12], dx[12];
+    unpack_Hb(D, Hb.data(), H, b);
+    for (int i = 0; i < D * D; ++i) A[i] = H[i];
+    for (int i = 0; i < D; ++i) {
+      A[i * D + i] += (i < 6) ? (double)P.damping : (double)P.velocity_damping;
+      rhs[i] = -b[i];
+    }
+    ldlt_solve<double>(D, A, rhs, dx);
+    X = iso_mul(expmap<double>(dx), X);
+    if (D == 12)
+      for (int i = 0; i < 6; ++i) v[i] += dx[6 + i];
+  }
+  iso_to12(X, X12);
+  if (kind != KIND_ICP)
+    for (int i = 0; i < 6; ++i) v6[i] = v[i];
+}
 
 }  // namespace orc

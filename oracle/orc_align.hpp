@@ -53,6 +53,15 @@ int align(int kind, int mode, const std::vector<const Tree*>& fixed, const std::
           const Tree& moving, const AlignParams& P, const OPrior* prior, double* X12, double* v6, const double* fv6,
           int stats_mode, int num_threads, OResult* out);
 
+bool pose_hessian(const double* H12, double* out36);
+void product_caches(const double* X12, const double* Xf12, float* out36);
+int align_recorded(int kind, const std::vector<const Tree*>& fixed, const std::vector<Iso<double>>& fixed_X,
+                   const Tree& moving, const AlignParams& P, double* X12, double* v6, const double* fv6,
+                   OResult* out, std::vector<int32_t>& match, std::vector<int32_t>& status);
+void align_replay64(int kind, const std::vector<const Tree*>& fixed, const std::vector<Iso<double>>& fixed_X,
+                    const Tree& Mv, const AlignParams& P, double* X12, double* v6, const double* fv6, int iterations,
+                    const int32_t* match, const int32_t* status);
+
 void linearize_at(int kind, const Tree& F, const Tree& Mv, const float* caches36, const float* v6, const float* fv6,
                   const AlignParams& P, int stats_mode, int32_t* match_out, int32_t* status_out, double* H_out,
                   double* b_out, OStats* st_out);

@@ -84,6 +84,42 @@ int32_t orc_align(int32_t kind, int32_t mode, void* const* fixed, const double* 
   return align(kind, mode, F, FX, *(const Tree*)moving, *P, prior, X12, v6, fv6, stats_mode, num_threads, out);
 }
 
+// MODE_MIXED compute() that also writes every iteration's correspondences and status:
+// match/status hold max_iterations x num_fixed x moving leaves entries.
+int32_t orc_align_recorded(int32_t kind, void* const* fixed, const double* fixed_X, int32_t num_fixed, void* moving,
+                           const AlignParams* P, double* X12, double* v6, const double* fv6, OResult* out,
+                           int32_t* match, int32_t* status) {
+  std::vector<const Tree*> F;
+  std::vector<Iso<double>> FX;
+  for (int i = 0; i < num_fixed; ++i) {
+    F.push_back((const Tree*)fixed[i]);
+    FX.push_back(iso_from12<double>(fixed_X + 12 * i));
+  }
+  std::vector<int32_t> m, s;
+  int32_t ret = align_recorded(kind, F, FX, *(const Tree*)moving, *P, X12, v6, fv6, out, m, s);
+  std::memcpy(match, m.data(), m.size() * sizeof(int32_t));
+  std::memcpy(status, s.data(), s.size() * sizeof(int32_t));
+  return ret;
+}
+
+void orc_align_replay64(int32_t kind, void* const* fixed, const double* fixed_X, int32_t num_fixed, void* moving,
+                        const AlignParams* P, double* X12, double* v6, const double* fv6, int32_t iterations,
+                        const int32_t* match, const int32_t* status) {
+  std::vector<const Tree*> F;
+  std::vector<Iso<double>> FX;
+  for (int i = 0; i < num_fixed; ++i) {
+    F.push_back((const Tree*)fixed[i]);
+    FX.push_back(iso_from12<double>(fixed_X + 12 * i));
+  }
+  align_replay64(kind, F, FX, *(const Tree*)moving, *P, X12, v6, fv6, iterations, match, status);
+}
+
+void orc_sincos_canon_d(double x, double* s, double* c) { sincos_canon_d(x, s, c); }
+
+int32_t orc_pose_hessian(const double* H144, double* out36) { return pose_hessian(H144, out36) ? 1 : 0; }
+
+void orc_product_caches(const double* X12, const double* Xf12, float* out36) { product_caches(X12, Xf12, out36); }
+
 void orc_linearize(int32_t kind, void* fixed, void* moving, const float* caches36, const float* v6, const float* fv6,
                    const AlignParams* P, int32_t stats_mode, int32_t* match, int32_t* status, double* H, double* b,
                    OStats* st) {

@@ -184,6 +184,45 @@ inline void sincos_canon(float x, float* s_out, float* c_out) {
 inline void sincos_t(float x, float* s, float* c) { sincos_canon(x, s, c); }
 inline void sincos_t(double x, double* s, double* c) { *s = std::sin(x); *c = std::cos(x); }
 
+// Canonical double-precision sine/cosine of the product's FP64 pose update
+// (kd_slam2_b200/csrc/kds_align.cu, sincos_canon_d), restated so that MODE_MIXED's
+// expmap is bit-identical to the GPU's: Cody-Waite reduction by pi/2 with a three-part
+// constant of 33 + 33 + 53 bits, then the Taylor series of sin to r^17 and of cos to
+// r^18 in Horner form.  Within 2 ulp of libm (tests/test_oracle_pins.py).
+inline void sincos_canon_d(double x, double* s_out, double* c_out) {
+  const double q = std::nearbyint(x * 0x1.45f306dc9c883p-1);
+  const long long j = (long long)q;
+  double r = x - q * 0x1.921fb54400000p+0;
+  r = r - q * 0x1.0b4611a600000p-34;
+  r = r - q * 0x1.3198a2e037073p-69;
+  const double r2 = r * r;
+  double t = 0x1.952c77030ad4ap-49;
+  t = -0x1.ae7f3e733b81fp-41 + r2 * t;
+  t = 0x1.6124613a86d09p-33 + r2 * t;
+  t = -0x1.ae64567f544e4p-26 + r2 * t;
+  t = 0x1.71de3a556c734p-19 + r2 * t;
+  t = -0x1.a01a01a01a01ap-13 + r2 * t;
+  t = 0x1.1111111111111p-7 + r2 * t;
+  t = -0x1.5555555555555p-3 + r2 * t;
+  const double sn = r + r * (r2 * t);
+  double u = -0x1.6827863b97d97p-53;
+  u = 0x1.ae7f3e733b81fp-45 + r2 * u;
+  u = -0x1.93974a8c07c9dp-37 + r2 * u;
+  u = 0x1.1eed8eff8d898p-29 + r2 * u;
+  u = -0x1.27e4fb7789f5cp-22 + r2 * u;
+  u = 0x1.a01a01a01a01ap-16 + r2 * u;
+  u = -0x1.6c16c16c16c17p-10 + r2 * u;
+  u = 0x1.5555555555555p-5 + r2 * u;
+  u = -0.5 + r2 * u;
+  const double cs = 1.0 + r2 * u;
+  switch ((int)(j & 3)) {
+    case 0: *s_out = sn; *c_out = cs; break;
+    case 1: *s_out = cs; *c_out = -sn; break;
+    case 2: *s_out = -sn; *c_out = -cs; break;
+    default: *s_out = -cs; *c_out = sn; break;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // GeometryTraits_<3> restated (kd/utils/geometry_3d_impl_.h).
 template <class T> inline M3<T> rodrigues_angle(T s, T c, const M3<T>& S, const M3<T>& S2) {
@@ -245,6 +284,59 @@ template <class T> inline Iso<T> expmap(const T* v) {
   X.t = v3<T>(v[0], v[1], v[2]);
   X.R = rodrigues(v3<T>(v[3], v[4], v[5]));
   return X;
+}
+// The same in FP64 with the canonical sine/cosine (MODE_MIXED: the product's pose update).
+inline Iso<double> expmap_canon(const double* v) {
+  Iso<double> X;
+  X.t = v3<double>(v[0], v[1], v[2]);
+  V3<double> w = v3<double>(v[3], v[4], v[5]);
+  double angle = std::sqrt(dot3(w, w));
+  if (angle < 1e-9) {
+    X.R = meye<double>();
+    return X;
+  }
+  double inv = 1.0 / angle;
+  M3<double> S = skew(vscale(w, inv));
+  M3<double> S2 = mat_mul(S, S);
+  double s, c;
+  sincos_canon_d(angle, &s, &c);
+  X.R = rodrigues_angle(s, c, S, S2);
+  return X;
+}
+
+// The product's FP64 solve (kd_slam2_b200/csrc/kds_align.cu, tail_warp): Cholesky of
+// the lower triangle of A (n <= 12) by column sweeps -- per pivot one square root and one
+// reciprocal, the column scaled by it, the trailing triangle updated -- then L y = rhs
+// and L^T x = y by column sweeps.  Returns false (x = 0) when a pivot is not positive.
+inline bool chol_solve_cols(int n, const double* A_in, const double* rhs, double* x) {
+  double A[12][12], inv[12], y[12];
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) A[i][j] = A_in[i * n + j];
+  bool ok = true;
+  for (int k = 0; k < n; ++k) {
+    double d = A[k][k];
+    ok = ok && (d > 0.0);
+    double lkk = std::sqrt(std::fmax(d, 1e-300));
+    double iv = 1.0 / lkk;
+    for (int i = k + 1; i < n; ++i) A[i][k] = A[i][k] * iv;
+    A[k][k] = lkk;
+    inv[k] = iv;
+    for (int i = k + 1; i < n; ++i)
+      for (int j = k + 1; j <= i; ++j) A[i][j] = A[i][j] - A[i][k] * A[j][k];
+  }
+  for (int i = 0; i < n; ++i) y[i] = rhs[i];
+  for (int k = 0; k < n; ++k) {
+    const double yk = y[k] * inv[k];
+    y[k] = yk;
+    for (int i = k + 1; i < n; ++i) y[i] = y[i] - A[i][k] * yk;
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    const double xk = y[k] * inv[k];
+    y[k] = xk;
+    for (int i = 0; i < k; ++i) y[i] = y[i] - A[k][i] * xk;
+  }
+  for (int i = 0; i < n; ++i) x[i] = ok ? y[i] : 0.0;
+  return ok;
 }
 // logSO3 (geometry_3d_impl_.h:48-59)
 template <class T> inline V3<T> logSO3(const M3<T>& R) {

@@ -59,3 +59,21 @@ def pose_err(A, B):
     dR = A[:, :3].T @ B[:, :3]
     c = np.clip((np.trace(dR) - 1) / 2, -1, 1)
     return float(np.linalg.norm(A[:, 3] - B[:, 3])), float(np.arccos(c))
+
+
+def assert_same_tree(O, G):
+    """Oracle tree O and GPU tree G: node arrays, leaf list, point order and root frame
+    bit-identical."""
+    eo, eg = O.export(), G.export()
+    assert len(eo["mean"]) == len(eg["mean"])
+    for k in ("left", "right", "level", "start", "end", "leaves", "perm"):
+        assert np.array_equal(eo[k], eg[k]), k
+    for k in ("mean", "dir"):
+        assert np.array_equal(eo[k].view(np.uint32), eg[k].view(np.uint32)), k
+    for k in ("dts_mean", "dts_cov"):
+        assert np.array_equal(eo[k].view(np.uint64), eg[k].view(np.uint64)), k
+    assert eo["ts_start"] == eg["ts_start"]
+    assert G.info.num_unpruned == eo["num_unpruned"]
+    ro, rg = O.root(), G.root()  # Tree_::root_* as TreeCPU_'s constructor sets them
+    for k in ("root_mean", "root_eigenvalues", "root_eigenvectors"):
+        assert np.array_equal(ro[k].view(np.uint32), rg[k].view(np.uint32)), k

@@ -1,10 +1,12 @@
 """GPU ICP / CT-ICP against the oracle.
 
-Per linearization at identical float caches: fixed-leaf indices and status masks are
-bit-exact; H and b agree to the FP32-reordering tolerance RTOL_HB relative to max|H|.
-Whole compute(): the pose agrees with the oracle in the product's own semantics
-(MODE_MIXED: float per-leaf terms, FP64 sums/solve/pose) within 1e-5 m / 1e-5 rad,
-and with the all-FP64 oracle within the stated POSE_TOL_FP64.
+Per linearization at identical float caches: fixed-leaf indices, status masks, H and b
+are bit-exact (the oracle's MODE_MIXED sums in the product's tile / warp-Kahan order).
+Whole compute(): pose, velocities, result code and stats are bit-identical to the
+oracle in the product's semantics (MODE_MIXED: float per-leaf terms, FP64 sums,
+Cholesky and pose update), and the pose is within the stated POSE_TOL_FP64 of the
+all-FP64 oracle.  With a pose prior the prior's FP64 terms are summed in another order
+than the oracle's, so that case is held to POSE_TOL.
 """
 import numpy as np
 import pytest
@@ -14,8 +16,7 @@ from oracle import orc
 
 pytestmark = pytest.mark.gpu
 
-RTOL_HB = 2e-5          # |H_gpu - H_oracle| <= RTOL_HB * max|H_oracle|
-POSE_TOL = 1e-5         # m and rad, against the oracle in the product's semantics
+POSE_TOL = 1e-5         # m and rad, against MODE_MIXED where a pose prior is summed in
 POSE_TOL_FP64 = 1e-4    # m and rad, against the all-FP64 oracle
 
 
@@ -48,11 +49,18 @@ def ct_trees(scene):
     return Gf, Gm, Of, Om, vel
 
 
-def hb_close(Hg, Ho, bg, bo):
-    s = max(1e-12, np.abs(Ho).max())
-    assert np.abs(Hg - Ho).max() <= RTOL_HB * s, np.abs(Hg - Ho).max() / s
-    sb = max(1e-12, np.abs(bo).max(), np.abs(Ho).max() * 1e-3)
-    assert np.abs(bg - bo).max() <= RTOL_HB * sb * 10, np.abs(bg - bo).max() / sb
+def hb_equal(Hg, Ho, bg, bo):
+    assert np.array_equal(Hg, Ho), np.abs(Hg - Ho).max() / max(1e-300, np.abs(Ho).max())
+    assert np.array_equal(bg, bo), np.abs(bg - bo).max() / max(1e-300, np.abs(bo).max())
+
+
+def same_run(a, ro):
+    """GPU aligner state after compute() against an oracle MODE_MIXED result: identical."""
+    assert np.array_equal(a.get_x(), ro["X"]), pose_err(a.get_x(), ro["X"])
+    assert np.array_equal(a.velocities(), ro["v"]), np.abs(a.velocities() - ro["v"]).max()
+    st = a.stats
+    for k in ("num_inliers", "num_outliers", "num_bad", "num_err_normal", "num_err_fn", "chi2", "chi2_kernelized"):
+        assert st[k] == ro["stats"][k], (k, st[k], ro["stats"][k])
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2])
@@ -74,7 +82,7 @@ def test_icp_linearization_bit_exact_correspondences(trees, seed, stats_mode):
     for k in ("num_inliers", "num_outliers", "num_bad", "num_err_normal", "num_err_fn"):
         assert stg[k] == sto[k], k
     assert stg["num_outliers"] > 0 and stg["num_bad"] > 0  # every gate is exercised
-    hb_close(Hg, Ho, bg, bo)
+    hb_equal(Hg, Ho, bg, bo)
 
 
 @pytest.mark.parametrize("seed", [0, 1])
@@ -93,7 +101,7 @@ def test_ct_linearization_bit_exact_correspondences(ct_trees, seed):
     mo, so, Ho, bo, sto = orc.linearize(orc.KIND_CT, Of, Om, c, orc.align_params(**P), v=v)
     assert np.array_equal(mg, mo)
     assert np.array_equal(sg, so)
-    hb_close(Hg, Ho, bg, bo)
+    hb_equal(Hg, Ho, bg, bo)
 
 
 def test_ct_dual_linearization(ct_trees):
@@ -109,12 +117,11 @@ def test_ct_dual_linearization(ct_trees):
     d = a.dual()
     mo, so, Ho, bo, _ = orc.linearize(orc.KIND_CT_DUAL, Of, Om, c, orc.align_params(max_error=0.5), v=v, fixed_v=fv)
     assert np.array_equal(mg, mo) and np.array_equal(sg, so)
-    hb_close(Hg, Ho[:12, :12], bg, bo[:12])
-    s = np.abs(Ho).max()
-    assert np.abs(d["H_dual_vel_B"] - Ho[12:, 12:]).max() <= RTOL_HB * s
-    assert np.abs(d["H_dual_cross_pose_vel_B"] - Ho[:6, 12:]).max() <= RTOL_HB * s
-    assert np.abs(d["H_dual_cross_vel_AB"] - Ho[6:12, 12:]).max() <= RTOL_HB * s
-    assert np.abs(d["b_dual_vel_B"] - bo[12:]).max() <= RTOL_HB * max(s, 1.0) * 10
+    hb_equal(Hg, Ho[:12, :12], bg, bo[:12])
+    assert np.array_equal(d["H_dual_vel_B"], Ho[12:, 12:])
+    assert np.array_equal(d["H_dual_cross_pose_vel_B"], Ho[:6, 12:])
+    assert np.array_equal(d["H_dual_cross_vel_AB"], Ho[6:12, 12:])
+    assert np.array_equal(d["b_dual_vel_B"], bo[12:])
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2, 3])
@@ -132,14 +139,10 @@ def test_icp_compute_matches_oracle(trees, seed):
     ro = orc.align(orc.KIND_ICP, orc.MODE_MIXED, Of, Om, orc.align_params(**P), X0)
     r64 = orc.align(orc.KIND_ICP, orc.MODE_FP64, Of, Om, orc.align_params(**P), X0)
     assert ret == ro["ret"] == 10
-    dt, dr = pose_err(a.get_x(), ro["X"])
-    assert dt <= POSE_TOL and dr <= POSE_TOL, (dt, dr)
+    same_run(a, ro)
     dt, dr = pose_err(a.get_x(), r64["X"])
     assert dt <= POSE_TOL_FP64 and dr <= POSE_TOL_FP64, (dt, dr)
     assert len(a.stats_log) == 10
-    st = a.stats
-    for k in ("num_inliers", "num_outliers", "num_bad", "num_err_normal", "num_err_fn"):
-        assert abs(st[k] - ro["stats"][k]) <= 2, k
 
 
 def test_ct_compute_matches_oracle(ct_trees):
@@ -155,11 +158,12 @@ def test_ct_compute_matches_oracle(ct_trees):
     ret = a.compute()
     ro = orc.align(orc.KIND_CT, orc.MODE_MIXED, Of, Om, orc.align_params(**P), X0, v0=np.zeros(6))
     assert ret == ro["ret"]
-    dt, dr = pose_err(a.get_x(), ro["X"])
-    assert dt <= POSE_TOL and dr <= POSE_TOL, (dt, dr)
-    assert np.abs(a.velocities() - ro["v"]).max() <= 1e-4
-    # the pose Hessian (Schur complement over the velocity block) is finite and symmetric
-    Hp = a.get_pose_hessian()
+    same_run(a, ro)
+    # CTICP_::poseHessian: the Schur complement over the velocity block of the last
+    # iteration's H (bit-identical to the oracle's) against the oracle's restatement
+    assert np.array_equal(a.H, ro["H"])
+    Hp, Ho = a.get_pose_hessian(), orc.pose_hessian(ro["H"])
+    assert np.abs(Hp - Ho).max() <= 1e-9 * np.abs(Ho).max(), np.abs(Hp - Ho).max() / np.abs(Ho).max()
     assert np.allclose(Hp, Hp.T, rtol=1e-9, atol=1e-6)
 
 
@@ -175,6 +179,7 @@ def test_term_crit_prior_and_result_codes(trees):
     ret = a.compute()
     ro = orc.align(orc.KIND_ICP, orc.MODE_MIXED, Of, Om, orc.align_params(term_crit=1, **P), X0)
     assert 0 < ret < 20 and ret == ro["ret"]
+    same_run(a, ro)
     # pose prior pulls the estimate towards Z
     from kd_slam2_b200 import synth
     Z = synth.pose((0.05, 0.0, 0.0))
@@ -215,8 +220,7 @@ def test_fixed_forest_sums_entries(trees):
     a.set_x(X0)
     a.compute()
     ro = orc.align(orc.KIND_ICP, orc.MODE_MIXED, [(Of, np.eye(3, 4)), (Of, Xb)], Om, orc.align_params(**P), X0)
-    dt, dr = pose_err(a.get_x(), ro["X"])
-    assert dt <= POSE_TOL and dr <= POSE_TOL
+    same_run(a, ro)
 
 
 def test_batch_equals_single_alignments(trees, ct_trees):
@@ -242,3 +246,37 @@ def test_batch_equals_single_alignments(trees, ct_trees):
         assert list(s.X) == list(m.X)
         assert list(s.v) == list(m.v)
         assert s.stats.num_inliers == m.stats.num_inliers
+
+
+def test_tree_top_wait_fallback(trees):
+    """With the bounded wait for the tree-top TMA copy cut to zero polls, every block of
+    compute() reads the fixed tree from global memory: the call reports KDS_ERR_TIMEOUT
+    from the runner's own error slot, the results are identical to a normal run, and the
+    next compute() with the default limit reports nothing."""
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import abi
+    Gf, Gm, _, _ = trees
+    X0 = perturbation(np.random.default_rng(31), 0.2, 2.0)
+
+    def run():
+        a = kds.ICPB2003D(max_error=0.5, max_iterations=6)
+        a.set_fixed(Gf)
+        a.set_moving(Gm)
+        a.set_x(X0)
+        return a
+
+    ref = run()
+    ref.compute()
+    lib = kds.lib()
+    assert lib.kds_set_tma_wait_limit(0) == abi.KDS_OK
+    try:
+        a = run()
+        with pytest.raises(kds.KdsError) as ei:
+            a.compute()
+    finally:
+        assert lib.kds_set_tma_wait_limit(1 << 20) == abi.KDS_OK
+    assert ei.value.code == abi.KDS_ERR_TIMEOUT and "valid" in str(ei.value)
+    assert np.array_equal(a.get_x(), ref.get_x())
+    b = run()
+    b.compute()
+    assert np.array_equal(b.get_x(), ref.get_x())

@@ -231,3 +231,11 @@ def test_checkpoint_resume_continues_identically(scene):
     z = kds.Tracker3D(odom_aligner=kds.CTICPB2003D(), motion_model=kds.ZeroVelMotionModel3D())
     with pytest.raises(kds.KdsError):
         z.restore(ck)
+    # so is a state saved under other aligner settings, naming the setting, and the
+    # tracker is left as it was
+    w = kds.Tracker3D(odom_aligner=kds.CTICPB2003D(max_error=0.5, max_iterations=12, velocity_damping=100.0),
+                      motion_model=kds.ConstVelMotionModel3D(), max_kf_trans=0.5, min_inlier_frac=0.3)
+    before = w.pose_global()
+    with pytest.raises(kds.KdsError, match="max_iterations"):
+        w.restore(ck)
+    assert np.array_equal(w.pose_global(), before)

@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from conftest import make_scan
+from conftest import assert_same_tree, make_scan
 from oracle import orc
 
 pytestmark = pytest.mark.gpu
@@ -13,22 +13,6 @@ def build_both(xyz, st, **params):
     O = orc.OTree.build(xyz, st, orc.tree_params(**params))
     G = kds.TreeGeneratorB2003D(**params).make_tree(xyz, st)
     return O, G
-
-
-def assert_same_tree(O, G):
-    eo, eg = O.export(), G.export()
-    assert len(eo["mean"]) == len(eg["mean"])
-    for k in ("left", "right", "level", "start", "end", "leaves", "perm"):
-        assert np.array_equal(eo[k], eg[k]), k
-    for k in ("mean", "dir"):
-        assert np.array_equal(eo[k].view(np.uint32), eg[k].view(np.uint32)), k
-    for k in ("dts_mean", "dts_cov"):
-        assert np.array_equal(eo[k].view(np.uint64), eg[k].view(np.uint64)), k
-    assert eo["ts_start"] == eg["ts_start"]
-    assert G.info.num_unpruned == eo["num_unpruned"]
-    ro, rg = O.root(), G.root()  # Tree_::root_* as TreeCPU_'s constructor sets them
-    for k in ("root_mean", "root_eigenvalues", "root_eigenvectors"):
-        assert np.array_equal(ro[k].view(np.uint32), rg[k].view(np.uint32)), k
 
 
 @pytest.mark.parametrize("seed,beams,params", [

@@ -1,11 +1,15 @@
-"""kds_linearize_static, the linearization that allocates nothing, against the
-aligner's own buildQuadraticForm (kds_aligner_build_quadratic_form + get_hb/get_stats).
+"""kds_linearize_static, the linearization for callers that cannot allocate device memory
+(real-time loops that reserve all their memory at start-up, code that must not wait on
+cudaMalloc/cudaFree), against the aligner's own buildQuadraticForm and the oracle.
 
-Both run the same kernels over the same 128-leaf tiles, so H, b and the stats counters
-are expected to agree; the test allows RTOL_HB relative to max|H|, the tolerance the
-other linearization tests use.  Each case makes two calls in a row with different
-inputs, because every call reuses the same static scratch.  The file name sorts last
-so that it also runs after the rest of the suite.
+The static call runs the same kernels over the same 128-leaf tiles as
+kds_aligner_build_quadratic_form, so H, b and the stats must be bit-identical to it; the
+oracle's linearization in the product's summation order, at the caches the product
+derives from the same poses, must be bit-identical too.  Each case makes two calls in a
+row with different inputs, because every call reuses the same static scratch, and the
+second call must leave the device's free memory and the default memory pool's
+reservation and use unchanged.  The file name sorts last so that it also runs after the
+rest of the suite.
 """
 import ctypes as C
 
@@ -13,10 +17,10 @@ import numpy as np
 import pytest
 
 from conftest import make_scan, perturbation
+from oracle import orc
 
 pytestmark = pytest.mark.gpu
 
-RTOL_HB = 2e-5
 STATIC_MAX_LEAVES = 65536
 
 
@@ -45,14 +49,28 @@ def _reference_form(aligner, X, v=None, stats_mode=False):
     return aligner.H, aligner.b, aligner.stats
 
 
-def _close(Hs, bs, ss, Ha, ba, sa):
-    s = max(1e-12, np.abs(Ha).max())
-    assert np.abs(Hs - Ha).max() <= RTOL_HB * s, np.abs(Hs - Ha).max() / s
-    sb = max(1e-12, np.abs(ba).max(), s * 1e-3)
-    assert np.abs(bs - ba).max() <= RTOL_HB * sb * 10, np.abs(bs - ba).max() / sb
-    for k in ("num_inliers", "num_outliers", "num_bad", "num_err_normal", "num_err_fn"):
+def _same(Hs, bs, ss, Ha, ba, sa):
+    assert np.array_equal(Hs, Ha), np.abs(Hs - Ha).max()
+    assert np.array_equal(bs, ba), np.abs(bs - ba).max()
+    for k in ("num_inliers", "num_outliers", "num_bad", "num_err_normal", "num_err_fn", "chi2", "chi2_kernelized"):
         assert ss[k] == sa[k], (k, ss[k], sa[k])
     assert ss["num_inliers"] > 0
+
+
+def _memory_state():
+    """Free device memory and the default pool's reserved and used bytes (current device)."""
+    from cuda.bindings import runtime as rt
+    err, free, _total = rt.cudaMemGetInfo()
+    assert err == rt.cudaError_t.cudaSuccess
+    err, dev = rt.cudaGetDevice()
+    err, pool = rt.cudaDeviceGetDefaultMemPool(dev)
+    assert err == rt.cudaError_t.cudaSuccess
+    out = [free]
+    for attr in (rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemCurrent, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent):
+        err, val = rt.cudaMemPoolGetAttribute(pool, attr)
+        assert err == rt.cudaError_t.cudaSuccess
+        out.append(int(val))
+    return tuple(out)
 
 
 @pytest.fixture(scope="module")
@@ -71,6 +89,8 @@ def test_icp_two_calls_match_build_quadratic_form(clouds):
     (xf, sf), (xm, sm), _, _ = clouds
     gen = kds.TreeGeneratorB2003D(leaf_max_points=16)
     Gf, Gm = gen.make_tree(xf, sf), gen.make_tree(xm, sm)
+    Of = orc.OTree.build(xf, sf, orc.tree_params(leaf_max_points=16))
+    Om = orc.OTree.build(xm, sm, orc.tree_params(leaf_max_points=16))
     assert 0 < Gm.num_leaves <= STATIC_MAX_LEAVES
     P = dict(max_error=0.5, kernel_threshold=0.01)
     a = kds.ICPB2003D(**P)
@@ -84,7 +104,18 @@ def test_icp_two_calls_match_build_quadratic_form(clouds):
         rc, Hs, bs, ss = _static(kds.lib(), Gf, Gm, abi.KDS_ICP, params, X, Xf, stats_mode=stats_mode)
         assert rc == abi.KDS_OK, (call, kds.lib().kds_last_error())
         Ha, ba, sa = _reference_form(a, X, stats_mode=bool(stats_mode))
-        _close(Hs, bs, ss, Ha, ba, sa)
+        _same(Hs, bs, ss, Ha, ba, sa)
+        _, _, Ho, bo, so = orc.linearize(orc.KIND_ICP, Of, Om, orc.product_caches(X, Xf), orc.align_params(**P),
+                                         stats_mode=bool(stats_mode))
+        _same(Hs, bs, ss, Ho, bo, so)
+    # the second static call reserved and used no device memory: nothing changed between
+    # the state after the first call and the state after the second (the aligner's own
+    # buildQuadraticForm ran before the second call, so compare what it left behind)
+    X = perturbation(rng, 0.3, 3.0)
+    before = _memory_state()
+    rc, _, _, _ = _static(kds.lib(), Gf, Gm, abi.KDS_ICP, params, X, Xf)
+    assert rc == abi.KDS_OK
+    assert _memory_state() == before
 
 
 def test_ct_two_calls_match_build_quadratic_form(clouds):
@@ -93,6 +124,8 @@ def test_ct_two_calls_match_build_quadratic_form(clouds):
     (xf, sf), _, (xc, sc), vel = clouds
     gen = kds.TreeGeneratorB2003D(leaf_max_points=16)
     Gf, Gc = gen.make_tree(xf, sf), gen.make_tree(xc, sc)
+    Of = orc.OTree.build(xf, sf, orc.tree_params(leaf_max_points=16))
+    Oc = orc.OTree.build(xc, sc, orc.tree_params(leaf_max_points=16))
     assert 0 < Gc.num_leaves <= STATIC_MAX_LEAVES
     P = dict(max_error=0.5, velocity_damping=10.0)
     a = kds.CTICPB2003D(**P)
@@ -104,10 +137,43 @@ def test_ct_two_calls_match_build_quadratic_form(clouds):
     for call in range(2):
         X = perturbation(rng, 0.2, 2.0)
         v = vel + rng.normal(scale=0.3, size=6) * np.array([1, 1, 1, 0.05, 0.05, 0.05])
+        before = _memory_state()
         rc, Hs, bs, ss = _static(kds.lib(), Gf, Gc, abi.KDS_CTICP, params, X, Xf, v=v)
         assert rc == abi.KDS_OK, (call, kds.lib().kds_last_error())
+        if call == 1:  # the first call of a process may load the library's kernels
+            assert _memory_state() == before
         Ha, ba, sa = _reference_form(a, X, v=v)
-        _close(Hs, bs, ss, Ha, ba, sa)
+        _same(Hs, bs, ss, Ha, ba, sa)
+        _, _, Ho, bo, so = orc.linearize(orc.KIND_CT, Of, Oc, orc.product_caches(X, Xf), orc.align_params(**P),
+                                         v=np.asarray(v, np.float32))
+        _same(Hs, bs, ss, Ho, bo, so)
+
+
+def test_tree_top_wait_fallback_reports_own_timeout(clouds):
+    """With the bounded wait for the tree-top copy cut to zero polls every block falls back
+    to global memory: the call returns KDS_ERR_TIMEOUT from its own error slot, with the
+    same H, b and stats; the next call with the default limit returns KDS_OK."""
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import abi
+    (xf, sf), (xm, sm), _, _ = clouds
+    gen = kds.TreeGeneratorB2003D(leaf_max_points=16)
+    Gf, Gm = gen.make_tree(xf, sf), gen.make_tree(xm, sm)
+    params = kds.aligner_params(max_error=0.5)
+    X = perturbation(np.random.default_rng(21), 0.2, 2.0)
+    lib = kds.lib()
+    rc0, H0, b0, s0 = _static(lib, Gf, Gm, abi.KDS_ICP, params, X, kds.identity())
+    assert rc0 == abi.KDS_OK
+    assert lib.kds_set_tma_wait_limit(0) == abi.KDS_OK
+    try:
+        rc1, H1, b1, s1 = _static(lib, Gf, Gm, abi.KDS_ICP, params, X, kds.identity())
+    finally:
+        assert lib.kds_set_tma_wait_limit(1 << 20) == abi.KDS_OK
+    assert rc1 == abi.KDS_ERR_TIMEOUT
+    assert b"valid" in lib.kds_last_error()
+    _same(H1, b1, s1, H0, b0, s0)
+    rc2, H2, b2, s2 = _static(lib, Gf, Gm, abi.KDS_ICP, params, X, kds.identity())
+    assert rc2 == abi.KDS_OK
+    _same(H2, b2, s2, H0, b0, s0)
 
 
 def test_rejects_more_leaves_than_the_static_maximum():

@@ -158,43 +158,82 @@ def config_block(tr):
     }
 
 
-def cpu_sample(tr, max_seconds: float, threads: int):
-    """The reference CPU path (oracle MODE_REF32) on the requests of the first map window
-    (against each stream's initial map): tree build + ICP/CT-ICP per request."""
+def cpu_sample(tr, max_seconds: float, threads: int, parallel_level: int = -1):
+    """The reference CPU path on the requests of the first map window, against each
+    stream's initial map, in trace order: per request the tree build with the reference's
+    float arithmetic (StableAdder_ sums, closed-form eigen solve, swap partition, std::async
+    above parallel_level; -1 = the production default) and ICP_CPU_/CTICP_CPU_ in
+    MODE_REF32 with `threads` chunks.  Returns per-request build and align seconds and the
+    build seconds of the maps it used (the map rebuilds of the served trace cost the same)."""
     from oracle import orc
     tp = orc.tree_params(**TREE)
-    maps = {}
-    times, n_done = [], 0
+    maps, map_s = {}, []
+    build_s, align_s = [], []
     t_start = time.perf_counter()
     for r in tr.requests:
         if r.seq >= MAP_EVERY:
             continue
         if r.stream not in maps:
             m = tr.streams[r.stream].map_xyz
-            maps[r.stream] = orc.OTree.build(m, np.zeros(len(m)), tp)
+            t0 = time.perf_counter()
+            maps[r.stream] = orc.OTree.build_ref32(m, np.zeros(len(m)), tp, parallel_level)
+            map_s.append(time.perf_counter() - t0)
         t0 = time.perf_counter()
-        T = orc.OTree.build(r.xyz, r.stamps, tp)
+        T = orc.OTree.build_ref32(r.xyz, r.stamps, tp, parallel_level)
+        t1 = time.perf_counter()
         if r.kind == 1:
             orc.align(orc.KIND_CT, orc.MODE_REF32, maps[r.stream], T, orc.align_params(**CT), r.X0, v0=r.v0,
                       num_threads=threads)
         else:
             orc.align(orc.KIND_ICP, orc.MODE_REF32, maps[r.stream], T, orc.align_params(**ICP), r.X0,
                       num_threads=threads)
-        times.append(time.perf_counter() - t0)
-        n_done += 1
+        build_s.append(t1 - t0)
+        align_s.append(time.perf_counter() - t1)
         if time.perf_counter() - t_start > max_seconds:
             break
-    return times
+    return {"build_s": build_s, "align_s": align_s, "map_s": map_s}
+
+
+def map_rebuilds_per_request(tr) -> float:
+    """Map rebuilds of the served trace per request: every stream's map is rebuilt after
+    each complete window of MAP_EVERY requests except its last."""
+    n = 0
+    for sid in range(len(tr.streams)):
+        k = sum(1 for r in tr.requests if r.stream == sid)
+        n += max(0, (k + MAP_EVERY - 1) // MAP_EVERY - 1)
+    return n / len(tr.requests)
+
+
+def cpu_rate(smp, rebuild_rate: float) -> float:
+    """Requests per second of the CPU path over a sample: each request's build + align,
+    plus its share of map rebuilds at the mean measured map-build time."""
+    n = len(smp["build_s"])
+    t = float(np.sum(smp["build_s"]) + np.sum(smp["align_s"])) + n * rebuild_rate * float(np.mean(smp["map_s"]))
+    return n / t
 
 
 def cpu_baseline_leg(tr, served, threads: int) -> dict:
-    """The CPU baseline leg: the reference's CPU path (the oracle port) timed on a bounded
-    sample of the trace, and the served results checked against the same oracle (all-FP64
-    and the product's mixed-precision semantics) on the requests against the initial maps."""
-    ctimes = cpu_sample(tr, 12.0, threads)
-    return {"value": len(ctimes) / float(np.sum(ctimes)), "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{len(ctimes)} requests of the first map window in ~12 s: oracle tree build + "
-                      f"ICP_CPU_/CTICP_CPU_ MODE_REF32 with {threads} chunks, against the streams' initial maps",
+    """The CPU baseline leg: the reference's CPU path (the oracle's restatement of its float
+    arithmetic) timed on a bounded sample of the trace, build and alignment separately,
+    with the production parallel_level (-1) and the demos' (3); and the served results
+    checked against the oracle (all-FP64 and the product's semantics)."""
+    rr = map_rebuilds_per_request(tr)
+    smp = cpu_sample(tr, 12.0, threads, -1)
+    smp3 = cpu_sample(tr, 6.0, threads, 3)
+    n = len(smp["build_s"])
+    return {"value": cpu_rate(smp, rr), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} requests of the first map window in ~12 s, in trace order: tree build with the "
+                      f"reference's float arithmetic (parallel_level -1) + ICP_CPU_/CTICP_CPU_ MODE_REF32 "
+                      f"with {threads} chunks, against the streams' initial maps; map rebuilds counted at "
+                      f"{rr:.3f} per request (the trace's rate) x the mean measured map build",
+            "build_ms_mean": 1e3 * float(np.mean(smp["build_s"])),
+            "align_ms_mean": 1e3 * float(np.mean(smp["align_s"])),
+            "map_build_ms_mean": 1e3 * float(np.mean(smp["map_s"])),
+            "parallel_level_3": {"value": cpu_rate(smp3, rr), "requests": len(smp3["build_s"]),
+                                 "build_ms_mean": 1e3 * float(np.mean(smp3["build_s"])),
+                                 "map_build_ms_mean": 1e3 * float(np.mean(smp3["map_s"])),
+                                 "note": "std::async for both children of every node above level 3, as the "
+                                         "reference's ICP / CT-ICP demos set it"},
             "served_pose_error_vs_oracle": accuracy_sample(tr, served)}
 
 
@@ -230,16 +269,17 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from kd_slam2_b200 import streams
     tr, _ = make_traces()
     threads = min(os.cpu_count() or 1, 8)
+    rr = map_rebuilds_per_request(tr)
     cpu_sample(tr, 2.0 * max(1, args.warmup) / 3.0, threads)  # warm-up
     step_times = []
     n_total = 0
     for _ in range(max(1, args.steps)):
-        ts = cpu_sample(tr, 20.0, threads)
-        step_times.append(float(np.sum(ts)))
-        n_total += len(ts)
+        smp = cpu_sample(tr, 20.0, threads)
+        n = len(smp["build_s"])
+        step_times.append(n / cpu_rate(smp, rr))
+        n_total += n
     val = n_total / float(np.sum(step_times))
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
@@ -248,8 +288,10 @@ def run_reference_arm(args):
         "config": config_block(tr),
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": "each step: up to 20 s of the trace's first-window requests in order "
-                                   f"(oracle tree build + ICP_CPU_/CTICP_CPU_ MODE_REF32, {threads} chunks) "
-                                   "against the streams' initial maps"},
+                                   "(tree build with the reference's float arithmetic, parallel_level -1, + "
+                                   f"ICP_CPU_/CTICP_CPU_ MODE_REF32, {threads} chunks) against the streams' "
+                                   f"initial maps, plus map rebuilds at the trace's {rr:.3f} per request x the "
+                                   "mean measured map build"},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -331,6 +373,36 @@ def batched_ba(steps: int):
         asm_t.append(1e3 * (time.perf_counter() - t0))
     n = [len(k.xyz) for k in wl.keyframes]
     errs = np.array([pose_err(np.array(res[k].X[:]), wl.pairs[k].X_true) for k in range(len(jobs))])
+    # pose against the oracle on a sample of jobs (oracle trees from the GPU trees' exports)
+    from oracle import orc
+    otrees = {}
+
+    def otree(i):
+        if i not in otrees:
+            e = trees[i].export()
+            otrees[i] = orc.OTree.from_nodes(e["mean"], e["dir"], e["dts_mean"], e["left"], e["right"])
+        return otrees[i]
+
+    acc = {"t_vs_fp64_m": [], "r_vs_fp64_rad": [], "bit_identical_to_product_semantics_oracle": 0, "jobs": 0}
+    for k in list(range(0, len(jobs), max(1, len(jobs) // 8)))[:8]:
+        p = wl.pairs[k]
+        kind = orc.KIND_CT if p.kind == 1 else orc.KIND_ICP
+        P = orc.align_params(**(CT if p.kind == 1 else ICP))
+        kw = dict(v0=wl.keyframes[p.j].vel, fixed_v=wl.keyframes[p.i].vel) if p.kind == 1 else {}
+        r64 = orc.align(kind, orc.MODE_FP64, otree(p.i), otree(p.j), P, p.X0, **kw)
+        rmx = orc.align(kind, orc.MODE_MIXED, otree(p.i), otree(p.j), P, p.X0, **kw)
+        X = np.array(res[k].X[:]).reshape(3, 4)
+        a_, b_ = pose_err(X, r64["X"])
+        acc["t_vs_fp64_m"].append(a_)
+        acc["r_vs_fp64_rad"].append(b_)
+        acc["bit_identical_to_product_semantics_oracle"] += int(np.array_equal(X, rmx["X"]))
+        acc["jobs"] += 1
+    ba_pose = {"jobs": acc["jobs"], "bit_identical_to_product_semantics_oracle":
+               acc["bit_identical_to_product_semantics_oracle"],
+               "t_vs_fp64_m_max": float(np.max(acc["t_vs_fp64_m"])),
+               "r_vs_fp64_rad_max": float(np.max(acc["r_vs_fp64_rad"])),
+               "t_vs_fp64_m_median": float(np.median(acc["t_vs_fp64_m"])),
+               "r_vs_fp64_rad_median": float(np.median(acc["r_vs_fp64_rad"]))}
     return {
         "workload": "200 keyframes on a 2 km loop (%d-%d points, log-uniform), %d pairs within 30 m, each "
                     "aligned rigid (10 it.) and CT-ICP (15 it.) = %d jobs" % (min(n), max(n), len(wl.pairs) // 2,
@@ -343,6 +415,7 @@ def batched_ba(steps: int):
         "results_identical_to_plain": bool(same), "autotune_config": int(chosen),
         "autotune_ms": [float(x) for x in tune_ms],
         "median_t_err_vs_truth_m": float(np.median(errs[:, 0])), "median_r_err_vs_truth_rad": float(np.median(errs[:, 1])),
+        "pose_vs_oracle": ba_pose,
         "factor_step": {"factors": len(factors), "variables": nv, "blocks": int(len(brc)),
                         "enabled": int(np.sum(ben)), "linearize_ms": float(np.mean(lin_t)),
                         "assemble_ms": float(np.mean(asm_t)),
@@ -350,6 +423,138 @@ def batched_ba(steps: int):
                                 "kds_batch_assemble wall time (block layout on the host, sums on the "
                                 "device, blocks read back)"},
     }
+
+
+def single_alignments(steps: int, peak: float, peak_source: str, cpu: bool = True):
+    """The plain drop-in on the two single-alignment configurations (kd_slam2_b200/scans.py):
+    rigid ICP of a 16 x 1024 scan against a second scan's tree, and CT-ICP of a skewed
+    64 x 1024 scan against the 1.2M-surfel tree of 20 prior scans.  Per configuration:
+    the map tree build (device-resident points), then per alignment the scan's tree build
+    + compute(): with device-resident points (`value`) and with the points in page-locked
+    host memory copied inside each alignment (`e2e`), CUDA events around K alignments with
+    a device synchronize on both sides.  Beside them: the k_linearize roofline of one
+    compute (algorithmic bytes per launch / mean launch time on the aligner's stream), the
+    map build's points x levels rate, and the pose against the oracle -- bit-identity with
+    the product-semantics run and the distance to the all-FP64 run.  With cpu, the
+    reference CPU path (reference-arithmetic tree build + MODE_REF32 compute) on the same
+    alignment, host cores."""
+    import torch
+
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import scans
+    from oracle import orc
+    out = {}
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    for name in ("rigid_16x1024", "ct_64x1024_1m_map"):
+        wl = getattr(scans, name)()
+        ct = wl["kind"] == "ct"
+        gen = kds.TreeGeneratorB2003D(**wl["tree"])
+        mx = torch.from_numpy(wl["map_xyz"]).cuda()
+        M = gen.make_tree(mx, device=True)
+        M.free()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record()
+        M = gen.make_tree(mx, device=True)
+        torch.cuda.synchronize()
+        e1.record()
+        e1.synchronize()
+        map_ms = e0.elapsed_time(e1)
+        sx, ss = torch.from_numpy(wl["xyz"]).cuda(), torch.from_numpy(wl["st"]).cuda()
+        hx, hs = torch.from_numpy(wl["xyz"]).pin_memory(), torch.from_numpy(wl["st"]).pin_memory()
+        a = kds.CTICPB2003D(**wl["params"]) if ct else kds.ICPB2003D(**wl["params"])
+        a.set_fixed(M)
+        X0, v0 = wl["X0s"][0], wl["v0"]
+
+        def align(device: bool):
+            T = gen.make_tree(sx, ss, device=True) if device else gen.make_tree(hx.numpy(), hs.numpy())
+            a.set_moving(T)
+            a.set_x(X0)
+            if ct:
+                a.set_velocities(v0)
+            ret = a.compute()
+            X = np.array(a.get_x())
+            T.free()
+            return ret, X
+
+        def timed(device: bool, k: int):
+            for _ in range(3):
+                align(device)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(k):
+                ret, X = align(device)
+            torch.cuda.synchronize()
+            e1.record()
+            e1.synchronize()
+            return e0.elapsed_time(e1) / k, ret, X
+
+        k = max(5, 4 * steps)
+        ms, ret, X = timed(True, k)
+        ms_e2e, ret_h, X_h = timed(False, k)
+        # k_linearize roofline of one compute at the initial guess
+        T = gen.make_tree(sx, ss, device=True)
+        a.set_moving(T)
+        a.set_x(X0)
+        if ct:
+            a.set_velocities(v0)
+        touched = a.count_touched_nodes()
+        a.set_profiling(True)
+        a.compute()
+        lin_ms, launches = a.profile()
+        a.set_profiling(False)
+        leaves = T.num_leaves
+        tiles = (leaves + 127) // 128
+        D = 12 if ct else 6
+        part = (D * (D + 1) // 2 + D + 7) * 8 * 2
+        alg = 32.0 * leaves + 32.0 * touched + part * tiles
+        lin_ach = alg / (lin_ms * 1e-3) / 1e9 if lin_ms > 0 else None
+        # pose against the oracle (trees bit-identical to the GPU's: the map from its export)
+        me = M.export()
+        Om = orc.OTree.from_nodes(me["mean"], me["dir"], me["dts_mean"], me["left"], me["right"])
+        Os = orc.OTree.build(wl["xyz"], wl["st"], orc.tree_params(**wl["tree"]))
+        P = orc.align_params(**wl["params"])
+        kind = orc.KIND_CT if ct else orc.KIND_ICP
+        rm = orc.align(kind, orc.MODE_MIXED, Om, Os, P, X0, v0=v0)
+        r64 = orc.align(kind, orc.MODE_FP64, Om, Os, P, X0, v0=v0)
+        npts = len(wl["xyz"])
+        pl = M.info.depth * len(wl["map_xyz"])
+        line = {
+            "scan_points": npts, "scan_leaves": int(leaves), "map_points": int(len(wl["map_xyz"])),
+            "map_leaves": int(M.num_leaves), "map_depth": int(M.info.depth), "iterations": int(wl["params"]["max_iterations"]),
+            "ms_per_alignment": ms, "alignments_per_s": 1e3 / ms, "points_per_s": npts * 1e3 / ms,
+            "e2e": {"ms_per_alignment": ms_e2e, "alignments_per_s": 1e3 / ms_e2e,
+                    "h2d_bytes": int(npts * 20), "note": "scan points and stamps from page-locked host memory"},
+            "map_build_ms": map_ms, "map_build_point_levels_per_s": pl / (map_ms * 1e-3),
+            "map_build_roofline": {"achieved": 48.0 * pl / (map_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                                   "frac": 48.0 * pl / (map_ms * 1e-3) / 1e9 / peak, "peak_source": peak_source,
+                                   "model": "48 B per point per level"},
+            "roofline_linearize": {"achieved": lin_ach, "peak": peak, "unit": "GB/s",
+                                   "frac": lin_ach / peak if lin_ach else None, "peak_source": peak_source,
+                                   "mean_launch_ms": lin_ms, "launches": launches, "touched_fixed_nodes": int(touched),
+                                   "alg_bytes_per_launch": alg},
+            "result": int(ret), "results_identical_host_vs_device": bool(np.array_equal(X, X_h) and ret == ret_h),
+            "bit_identical_to_product_semantics_oracle": bool(np.array_equal(X, rm["X"]) and ret == rm["ret"]),
+            "pose_error_vs_fp64_oracle": {"t_m": pose_err(X, r64["X"])[0], "r_rad": pose_err(X, r64["X"])[1]},
+            "pose_error_vs_truth": {"t_m": pose_err(X, wl["X_true"])[0], "r_rad": pose_err(X, wl["X_true"])[1]},
+        }
+        if cpu:
+            threads = min(os.cpu_count() or 1, 8)
+            tp = orc.tree_params(**wl["tree"])
+            t0 = time.perf_counter()
+            Rm = orc.OTree.build_ref32(wl["map_xyz"], None, tp, -1)
+            t1 = time.perf_counter()
+            Rs = orc.OTree.build_ref32(wl["xyz"], wl["st"], tp, -1)
+            t2 = time.perf_counter()
+            orc.align(kind, orc.MODE_REF32, Rm, Rs, P, X0, v0=v0, num_threads=threads)
+            t3 = time.perf_counter()
+            line["cpu_baseline"] = {"ms_per_alignment": 1e3 * (t3 - t1), "build_ms": 1e3 * (t2 - t1),
+                                    "align_ms": 1e3 * (t3 - t2), "map_build_ms": 1e3 * (t1 - t0), "cores": threads,
+                                    "kind": "port", "sample": "one alignment: reference-arithmetic scan tree build "
+                                    "(parallel_level -1) + MODE_REF32 compute with %d chunks" % threads}
+        M.free()
+        out[name] = line
+    return out
 
 
 def scan_input(steps: int):
@@ -540,6 +745,52 @@ def tracker_streams(num_streams: int = 32, frames: int = 8):
             "note": "host-timed steps (one frame of every stream), first step excluded"}
 
 
+def forest_pass(steps: int, scans: int = 5) -> dict:
+    """The build workload of the served step on its own: the first `scans` requests of
+    every stream of the trace (80 clouds by default) built as one forest pass
+    (kds_tree_build_batch, device-resident inputs), CUDA events around each pass."""
+    import ctypes as C
+
+    import torch
+
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import abi, streams
+    tr = streams.make_trace(TRACE_SEED, num_streams=STREAMS, scans_per_stream=scans, threads=16)
+    clouds = [(r.xyz, r.stamps) for r in tr.requests]
+    xyz = torch.from_numpy(np.ascontiguousarray(np.concatenate([c[0] for c in clouds]))).cuda()
+    st = torch.from_numpy(np.ascontiguousarray(np.concatenate([c[1] for c in clouds]))).cuda()
+    off = np.zeros(len(clouds) + 1, np.int64)
+    off[1:] = np.cumsum([len(c[0]) for c in clouds])
+    tp = kds.tree_params(**TREE)
+    R = len(clouds)
+    lib = kds.lib()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times, depth_pts = [], 0
+    for rep in range(3 + max(1, steps)):
+        out = (C.c_void_p * R)()
+        status = (C.c_int32 * R)()
+        torch.cuda.synchronize()
+        e0.record()
+        rc = lib.kds_tree_build_batch(xyz.data_ptr(), st.data_ptr(), off.ctypes.data, R, abi.KDS_MEM_DEVICE,
+                                      C.byref(tp), None, out, status)
+        torch.cuda.synchronize()
+        e1.record()
+        e1.synchronize()
+        if rc != abi.KDS_OK:
+            raise RuntimeError("kds_tree_build_batch: %d" % rc)
+        if rep >= 3:
+            times.append(e0.elapsed_time(e1))
+        depth = 0
+        for i in range(R):
+            if out[i]:
+                depth = max(depth, kds.Tree(out[i]).info.depth)  # the Tree wrapper frees it
+        depth_pts = depth * int(off[-1])
+    ms = float(np.median(times))
+    return {"clouds": R, "points": int(off[-1]), "ms_per_pass_median": ms, "ms_all": times,
+            "point_levels_per_s": depth_pts / (ms * 1e-3),
+            "alg_gbs_48B_per_point_level": 48.0 * depth_pts / (ms * 1e-3) / 1e9}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -551,7 +802,17 @@ def main():
     ap.add_argument("--no-ba", action="store_true", help="skip the batched bundle-adjustment section")
     ap.add_argument("--tracker-only", action="store_true",
                     help="run only the tracker-step leg and print its JSON (for profiling it)")
+    ap.add_argument("--forest-only", action="store_true",
+                    help="run only the served step's build workload (one forest pass of 80 scans) and print its JSON")
     args = ap.parse_args()
+    if args.forest_only:
+        import torch
+
+        import kd_slam2_b200 as kds
+        torch.cuda.set_device(0)
+        kds.init(0)
+        print(json.dumps({"forest_pass": forest_pass(args.steps)}), flush=True)
+        return
     if args.tracker_only:
         # the same device setup as the full run before its legs
         import torch
@@ -703,11 +964,9 @@ def main():
     plain = None
     if not args.no_plain:
         serve_step(dev_inputs, serial=1)  # warm-up: the serial path's aligners grow their workspaces
-        # the serial step's time varies from run to run (210-540 alignments/s seen on one box);
-        # the fastest of three is reported, which keeps served_over_plain conservative
-        p_runs = [serve_step(dev_inputs, serial=1) for _ in range(3)]
+        p_runs = [serve_step(dev_inputs, serial=1) for _ in range(max(5, args.steps))]
         p_all = [float(r[0]) for r in p_runs]
-        p_ms = min(p_all)
+        p_ms = float(np.median(p_all))
         p_res = p_runs[-1][1]
         p_val = n_req / (p_ms / 1e3)
         same = all(np.array_equal(a["X"], b["X"]) and a["result"] == b["result"] for a, b in zip(served, p_res))
@@ -715,7 +974,8 @@ def main():
                                     timeout=600.0)
         latp = np.array([1e3 * (q["t_done"] - q["t_arrival"]) for q in lat_p])
         plain = {"value": p_val, "unit": UNIT, "ms_per_step": p_ms, "ms_per_step_all": p_all,
-                 "reported": "fastest of %d timed steps after 1 warm-up" % len(p_runs),
+                 "reported": "median of %d timed steps after 1 warm-up" % len(p_runs),
+                 "spread": {"min_ms": float(np.min(p_all)), "max_ms": float(np.max(p_all))},
                  "served_over_plain": value / world / p_val,
                  "results_identical_to_served": bool(same),
                  "latency_ms_poisson": {"p50": float(np.percentile(latp, 50)), "p99": float(np.percentile(latp, 99))}}
@@ -746,6 +1006,8 @@ def main():
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_ba:
+        line["single_alignments"] = single_alignments(args.steps, peak, roofline["peak_source"],
+                                                      cpu=world == 1 and not args.no_cpu)
         line["batched_ba"] = batched_ba(args.steps)
         line["scan_input"] = scan_input(args.steps)
         line["tracker_step"] = tracker_step(cpu=world == 1 and not args.no_cpu)

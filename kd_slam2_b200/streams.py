@@ -169,45 +169,3 @@ def serve(trace: Trace, serial: bool = False, tree=None, icp=None, ct=None, inpu
     finally:
         srv.free()
     return results, stats, secs
-
-
-def _forest_main(argv=None):
-    """python -m kd_slam2_b200.streams [--streams S] [--scans K] [--reps R]: builds the
-    request clouds of a trace as one forest pass (kds_tree_build_batch, device inputs)
-    and prints the pass time -- the build workload of the served step, for profiling."""
-    import argparse
-    import ctypes as C
-    import time
-
-    import torch
-
-    from . import abi, lib, tree_params
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--streams", type=int, default=16)
-    ap.add_argument("--scans", type=int, default=5)
-    ap.add_argument("--reps", type=int, default=1)
-    a = ap.parse_args(argv)
-    tr = make_trace(5, num_streams=a.streams, scans_per_stream=a.scans, threads=16)
-    clouds = [(r.xyz, r.stamps) for r in tr.requests]
-    xyz = torch.from_numpy(np.ascontiguousarray(np.concatenate([c[0] for c in clouds]))).cuda()
-    st = torch.from_numpy(np.ascontiguousarray(np.concatenate([c[1] for c in clouds]))).cuda()
-    off = np.zeros(len(clouds) + 1, np.int64)
-    off[1:] = np.cumsum([len(c[0]) for c in clouds])
-    tp = tree_params(leaf_max_points=16)
-    R = len(clouds)
-    for _ in range(a.reps):
-        out = (C.c_void_p * R)()
-        status = (C.c_int32 * R)()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        rc = lib().kds_tree_build_batch(xyz.data_ptr(), st.data_ptr(), off.ctypes.data, R, abi.KDS_MEM_DEVICE,
-                                        C.byref(tp), None, out, status)
-        torch.cuda.synchronize()
-        print("rc %d: %d clouds, %d points, %.2f ms" % (rc, R, off[-1], 1e3 * (time.perf_counter() - t0)))
-        for i in range(R):
-            if out[i]:
-                lib().kds_tree_free(out[i])
-
-
-if __name__ == "__main__":
-    _forest_main()

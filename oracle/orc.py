@@ -79,6 +79,7 @@ def load() -> C.CDLL:
     P = C.c_void_p
     sig = {
         "orc_tree_build": (P, [P, P, C.c_int64, C.POINTER(TreeParams)]),
+        "orc_tree_build_ref32": (P, [P, P, C.c_int64, C.POINTER(TreeParams), C.c_int32]),
         "orc_tree_from_nodes": (P, [P, P, P, P, P, C.c_int64]),
         "orc_tree_num_nodes": (C.c_int64, [P]),
         "orc_tree_num_leaves": (C.c_int64, [P]),
@@ -140,6 +141,17 @@ class OTree:
         st = None if stamps is None else np.ascontiguousarray(stamps, np.float64)
         p = params or tree_params()
         h = lib.orc_tree_build(xyz.ctypes.data, None if st is None else st.ctypes.data, len(xyz), C.byref(p))
+        return OTree(h)
+
+    @staticmethod
+    def build_ref32(xyz, stamps=None, params: TreeParams | None = None, parallel_level: int = -1) -> "OTree":
+        """The reference's float build arithmetic (timed CPU baseline; not bit-comparable)."""
+        lib = load()
+        xyz = np.ascontiguousarray(xyz, np.float32)
+        st = None if stamps is None else np.ascontiguousarray(stamps, np.float64)
+        p = params or tree_params()
+        h = lib.orc_tree_build_ref32(xyz.ctypes.data, None if st is None else st.ctypes.data, len(xyz), C.byref(p),
+                                     int(parallel_level))
         return OTree(h)
 
     @staticmethod

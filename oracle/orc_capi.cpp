@@ -16,6 +16,11 @@ void* orc_tree_build(const float* xyz, const double* stamps, int64_t n, const Tr
   return t;
 }
 
+void* orc_tree_build_ref32(const float* xyz, const double* stamps, int64_t n, const TreeParams* P,
+                           int32_t parallel_level) {
+  return new Tree(build_tree_ref32(xyz, stamps, n, *P, parallel_level));
+}
+
 // Tree from a node array (Node_ fields): used to run the oracle aligner on trees
 // produced elsewhere.  Leaves are the nodes with no children, in array order.
 void* orc_tree_from_nodes(const float* mean, const float* dir, const double* dts_mean, const int32_t* left,

@@ -27,7 +27,9 @@
 //  * A node at level max_level-1 is not split further (the reference recurses
 //    without bound and overflows the stack on a degenerate split).
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
+#include <future>
 #include <limits>
 #include <vector>
 
@@ -428,6 +430,324 @@ Tree build_tree(const float* xyz, const double* st, int64_t n, const TreeParams&
   for (int i = 0; i < cnt; ++i)
     if (T.nodes[i].left < 0 && T.nodes[i].right < 0) T.leaves.push_back(i);
   T.num_unpruned = (int64_t)nn;
+  T.accepted = (int64_t)T.leaves.size() >= (int64_t)P.tree_min_good_leaves;
+  return T;
+}
+
+// ---------------------------------------------------------------------------
+// The reference's own CPU build arithmetic, for the timed CPU baseline (not a parity
+// definition: its float sums make it differ from the canonical build above in the last
+// bits, which moves a split or a leaf decision now and then).  It restates:
+//   Node_ constructor and splitRange       kd/tree/node_impl_.h:12-70 (swap partition,
+//                                          std::async for both children while the
+//                                          node's level < parallel_level >= 0)
+//   LabelPolicyBase_::fillMetadata         kd/tree/label_policy_base_impl_.h:12-97
+//                                          (float StableAdder_ over the packed
+//                                          [xx..zz, x, y, z], double StableAdder_ over
+//                                          (dt, dt^2), mean/cov in float)
+//   SelfAdjointEigenSolver::computeDirect  a closed-form symmetric 3x3 eigen solve in
+//                                          float: the trigonometric roots of the
+//                                          characteristic polynomial (Smith 1961) and
+//                                          eigenvectors as the longest cross product of
+//                                          two rows of A - lambda I
+//   CountLeafPolicy_ / FlatLeafPolicy_     as fill_metadata above, on the float values
+// then the same prune and breadth-first relabel.
+namespace {
+
+struct RefPoint {
+  float x, y, z;
+  double t;
+  int64_t id;
+};
+
+template <class T, int K> struct RefAdder {  // StableAdder_<T[K], 1024, 5>
+  T acc[5][K];
+  int cnt[5];
+  RefAdder() {
+    for (int l = 0; l < 5; ++l) {
+      cnt[l] = 0;
+      for (int k = 0; k < K; ++k) acc[l][k] = T(0);
+    }
+  }
+  void add(const T* v) {
+    T cur[K];
+    for (int k = 0; k < K; ++k) cur[k] = v[k];
+    for (int l = 0; l < 5; ++l) {
+      for (int k = 0; k < K; ++k) acc[l][k] += cur[k];
+      if (++cnt[l] < 1024) break;
+      for (int k = 0; k < K; ++k) { cur[k] = acc[l][k]; acc[l][k] = T(0); }
+      cnt[l] = 0;
+    }
+  }
+  void sum(T* out) const {
+    for (int k = 0; k < K; ++k) out[k] = T(0);
+    for (int l = 0; l < 5; ++l)
+      for (int k = 0; k < K; ++k) out[k] += acc[l][k];
+  }
+};
+
+// eigenvalues ascending, eigenvectors as columns of V
+void eig3_direct(const float A[3][3], float ev[3], float V[3][3]) {
+  const float m = (A[0][0] + A[1][1] + A[2][2]) / 3.0f;
+  float K[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) K[i][j] = A[i][j] - (i == j ? m : 0.0f);
+  float p = 0.0f;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) p += K[i][j] * K[i][j];
+  p = p / 6.0f;
+  if (!(p > 1e-30f)) {
+    for (int i = 0; i < 3; ++i) {
+      ev[i] = m;
+      for (int j = 0; j < 3; ++j) V[i][j] = i == j ? 1.0f : 0.0f;
+    }
+    return;
+  }
+  const float detK = K[0][0] * (K[1][1] * K[2][2] - K[1][2] * K[2][1]) -
+                     K[0][1] * (K[1][0] * K[2][2] - K[1][2] * K[2][0]) +
+                     K[0][2] * (K[1][0] * K[2][1] - K[1][1] * K[2][0]);
+  const float sp = std::sqrt(p);
+  float r = detK / (2.0f * p * sp);
+  r = std::max(-1.0f, std::min(1.0f, r));
+  const float phi = std::acos(r) / 3.0f;
+  float l3 = m + 2.0f * sp * std::cos(phi);
+  float l1 = m + 2.0f * sp * std::cos(phi + 2.0943951f);
+  float l2 = 3.0f * m - l1 - l3;
+  float lam[3] = {l1, l2, l3};
+  std::sort(lam, lam + 3);
+  for (int c = 0; c < 3; ++c) {
+    float B[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) B[i][j] = A[i][j] - (i == j ? lam[c] : 0.0f);
+    float best[3] = {0, 0, 0}, bn = -1.0f;
+    for (int a = 0; a < 3; ++a) {
+      const int b = (a + 1) % 3;
+      const float cx = B[a][1] * B[b][2] - B[a][2] * B[b][1];
+      const float cy = B[a][2] * B[b][0] - B[a][0] * B[b][2];
+      const float cz = B[a][0] * B[b][1] - B[a][1] * B[b][0];
+      const float nn = cx * cx + cy * cy + cz * cz;
+      if (nn > bn) { bn = nn; best[0] = cx; best[1] = cy; best[2] = cz; }
+    }
+    const float inv = bn > 0.0f ? 1.0f / std::sqrt(bn) : 0.0f;
+    for (int i = 0; i < 3; ++i) V[i][c] = bn > 0.0f ? best[i] * inv : (i == c ? 1.0f : 0.0f);
+    ev[c] = lam[c];
+  }
+}
+
+struct RefMeta {
+  bool is_node = false, has_prop = false;
+  float prop[3] = {0, 0, 0};
+  int level = 0;
+  double ts_start = 0.0;
+};
+
+struct RefBuild {
+  RefPoint* pts;
+  Node* nodes;
+  int* levels;
+  std::atomic<int>* idx;
+  int cap;
+  const TreeParams* P;
+  int parallel_level;
+
+  // fillMetadata + the leaf policies on the node's points; returns the node's metadata
+  RefMeta fill(Node& node, const RefMeta* parent) const {
+    RefMeta meta;
+    meta.level = parent ? parent->level + 1 : 0;
+    meta.ts_start = parent ? parent->ts_start : 0.0;
+    const int64_t n = node.end - node.start;
+    for (int i = 0; i < 3; ++i) { node.mean[i] = 0.f; node.dir[i] = 0.f; }
+    node.dts_mean = node.dts_cov = 0.0;
+    bool is_bad = n == 0;
+    float mean[3] = {0, 0, 0}, lam[3] = {0, 0, 0}, e0[3] = {0, 0, 0}, e2[3] = {0, 0, 0};
+    if (n > 0) {
+      if (!parent) {
+        double t0 = std::numeric_limits<double>::max();
+        for (int64_t i = node.start; i < node.end; ++i) t0 = std::min(t0, pts[i].t);
+        meta.ts_start = t0;
+      }
+      const float isize = 1.0f / (float)n;
+      RefAdder<double, 2> ta;
+      RefAdder<float, 9> acc;
+      for (int64_t i = node.start; i < node.end; ++i) {
+        const double dt = pts[i].t - meta.ts_start;
+        const double tv[2] = {dt, dt * dt};
+        ta.add(tv);
+        const float v[3] = {pts[i].x, pts[i].y, pts[i].z};
+        float packed[9];
+        int k = 0;
+        for (int r = 0; r < 3; ++r)
+          for (int c = r; c < 3; ++c) packed[k++] = v[r] * v[c];
+        for (int r = 0; r < 3; ++r) packed[k++] = v[r];
+        acc.add(packed);
+      }
+      double ts2[2];
+      ta.sum(ts2);
+      node.dts_mean = ts2[0] * isize;
+      node.dts_cov = ts2[1] * isize - node.dts_mean * node.dts_mean;
+      float sums[9];
+      acc.sum(sums);
+      float C[3][3];
+      int k = 0;
+      for (int r = 0; r < 3; ++r)
+        for (int c = r; c < 3; ++c, ++k) C[r][c] = C[c][r] = sums[k] * isize;
+      for (int r = 0; r < 3; ++r, ++k) mean[r] = sums[k] * isize;
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) C[r][c] -= mean[r] * mean[c];
+      for (int i = 0; i < 3; ++i) node.mean[i] = mean[i];
+      if (n < 3) {
+        is_bad = true;
+      } else {
+        float V[3][3];
+        eig3_direct(C, lam, V);
+        for (int i = 0; i < 3; ++i) { e0[i] = V[i][0]; e2[i] = V[i][2]; }
+        if (mean[0] * e0[0] + mean[1] * e0[1] + mean[2] * e0[2] > 0.f) for (int i = 0; i < 3; ++i) e0[i] = -e0[i];
+        if (mean[0] * e2[0] + mean[1] * e2[1] + mean[2] * e2[2] > 0.f) for (int i = 0; i < 3; ++i) e2[i] = -e2[i];
+      }
+    }
+    bool is_node = false;
+    if (is_bad) {
+    } else if ((float)n > (float)P->leaf_max_points) {
+      is_node = true;
+      for (int i = 0; i < 3; ++i) node.dir[i] = e2[i];
+    } else {
+      for (int i = 0; i < 3; ++i) node.dir[i] = e0[i];
+    }
+    bool has_prop = false;
+    float prop[3] = {0, 0, 0};
+    if (parent && P->propagate_normal) {
+      has_prop = parent->has_prop;
+      for (int i = 0; i < 3; ++i) prop[i] = parent->prop[i];
+    }
+    auto propagate = [&]() {
+      if (has_prop) {
+        float d[3] = {prop[0], prop[1], prop[2]};
+        if (mean[0] * d[0] + mean[1] * d[1] + mean[2] * d[2] > 0.f) for (int i = 0; i < 3; ++i) d[i] = -d[i];
+        for (int i = 0; i < 3; ++i) node.dir[i] = d[i];
+      }
+    };
+    bool is_flat = false;
+    if (is_bad || (float)n < (float)P->leaf_min_points) {
+      propagate();
+    } else {
+      const float ratio = lam[0] / lam[2];
+      is_flat = ratio < P->leaf_normal_eigenratio &&
+                std::fabs(mean[0] * e0[0] + mean[1] * e0[1] + mean[2] * e0[2]) > P->leaf_min_normal_incidence;
+      if (is_flat) {
+        has_prop = true;
+        for (int i = 0; i < 3; ++i) prop[i] = e0[i];
+      }
+      if (!is_node) {
+        const float density = (float)n / (lam[1] * lam[2]);
+        if (density < P->leaf_density) {
+          is_node = true;
+          for (int i = 0; i < 3; ++i) node.dir[i] = e2[i];
+        } else if (is_flat) {
+          for (int i = 0; i < 3; ++i) node.dir[i] = e0[i];
+        } else {
+          propagate();
+        }
+      }
+    }
+    if (is_node && meta.level >= P->max_level - 1) {
+      is_node = false;
+      for (int i = 0; i < 3; ++i) node.dir[i] = e0[i];
+    }
+    meta.is_node = is_node;
+    meta.has_prop = has_prop;
+    for (int i = 0; i < 3; ++i) meta.prop[i] = prop[i];
+    return meta;
+  }
+
+  int make(int64_t s, int64_t e, const RefMeta* parent) const {
+    const int my = idx->fetch_add(1);
+    if (my >= cap) return -1;
+    Node node;
+    node.start = s;
+    node.end = e;
+    node.left = node.right = -1;
+    const RefMeta meta = fill(node, parent);
+    levels[my] = meta.level;
+    if (meta.is_node) {
+      int64_t a = s, b = e - 1;  // splitRange: swap with the range end
+      while (a <= b) {
+        const RefPoint& p = pts[a];
+        const float d0 = p.x - node.mean[0], d1 = p.y - node.mean[1], d2 = p.z - node.mean[2];
+        if (node.dir[0] * d0 + (node.dir[1] * d1 + node.dir[2] * d2) > 0.0f) {
+          ++a;
+        } else {
+          std::swap(pts[a], pts[b]);
+          --b;
+        }
+      }
+      const int64_t mid = a;
+      if (parallel_level < 0 || meta.level >= parallel_level) {
+        node.left = make(s, mid, &meta);
+        node.right = make(mid, e, &meta);
+      } else {
+        auto hl = std::async(std::launch::async, [&]() { return make(s, mid, &meta); });
+        auto hr = std::async(std::launch::async, [&]() { return make(mid, e, &meta); });
+        node.left = hl.get();
+        node.right = hr.get();
+      }
+    }
+    nodes[my] = node;
+    return my;
+  }
+};
+
+}  // namespace
+
+Tree build_tree_ref32(const float* xyz, const double* st, int64_t n, const TreeParams& P, int parallel_level) {
+  Tree T;
+  T.num_points = n;
+  T.accepted = false;
+  if (n < (int64_t)P.leaf_min_points || n == 0) return T;
+  std::vector<RefPoint> pts(n);
+  for (int64_t i = 0; i < n; ++i) pts[i] = RefPoint{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], st ? st[i] : 0.0, i};
+  const int cap = (int)std::min<int64_t>(4 * n + 64, INT32_MAX / 2);
+  std::vector<Node> nodes(cap);
+  std::vector<int> levels(cap, 0);
+  std::atomic<int> idx(0);
+  RefBuild B{pts.data(), nodes.data(), levels.data(), &idx, cap, &P, parallel_level};
+  B.make(0, n, nullptr);
+  const int nn = std::min(idx.load(), cap);
+  T.perm.resize(n);
+  for (int64_t i = 0; i < n; ++i) T.perm[i] = pts[i].id;
+  // prune (TreeCPU_::prune, kd/tree/tree_cpu_.h:172-196): a node lives if it is a good
+  // leaf or has a living child; then breadth-first relabel from the root
+  std::vector<char> alive(nn, 0);
+  std::vector<int> order;
+  order.reserve(nn);
+  order.push_back(0);
+  for (size_t h = 0; h < order.size(); ++h) {
+    const Node& nd = nodes[order[h]];
+    if (nd.left >= 0) order.push_back(nd.left);
+    if (nd.right >= 0) order.push_back(nd.right);
+  }
+  for (size_t h = order.size(); h-- > 0;) {
+    const int i = order[h];
+    const Node& nd = nodes[i];
+    if (nd.left < 0 && nd.right < 0) alive[i] = good_leaf(nd, P.prune_min_normal_incidence) ? 1 : 0;
+    else alive[i] = ((nd.left >= 0 && alive[nd.left]) || (nd.right >= 0 && alive[nd.right])) ? 1 : 0;
+  }
+  std::vector<int> newidx(nn, -1);
+  int cnt = 0;
+  for (int i : order)
+    if (alive[i]) newidx[i] = cnt++;
+  T.nodes.resize(cnt);
+  T.levels.resize(cnt);
+  for (int i : order) {
+    if (!alive[i]) continue;
+    Node nd = nodes[i];
+    nd.left = (nd.left >= 0 && alive[nd.left]) ? newidx[nd.left] : -1;
+    nd.right = (nd.right >= 0 && alive[nd.right]) ? newidx[nd.right] : -1;
+    T.nodes[newidx[i]] = nd;
+    T.levels[newidx[i]] = levels[i];
+  }
+  for (int i = 0; i < cnt; ++i)
+    if (T.nodes[i].left < 0 && T.nodes[i].right < 0) T.leaves.push_back(i);
+  T.num_unpruned = nn;
   T.accepted = (int64_t)T.leaves.size() >= (int64_t)P.tree_min_good_leaves;
   return T;
 }

@@ -47,6 +47,9 @@ struct Tree {
 };
 
 Tree build_tree(const float* xyz, const double* stamps, int64_t n, const TreeParams& P);
+// The reference's float build arithmetic (StableAdder_ sums, closed-form eigen, swap
+// partition, std::async above parallel_level), for the timed CPU baseline only.
+Tree build_tree_ref32(const float* xyz, const double* stamps, int64_t n, const TreeParams& P, int parallel_level);
 void jacobi3(const double A[3][3], double ev[3], double V[3][3]);
 // floor(v * 2^64) as a 128-bit two's complement integer (hi, lo): the fixed-point
 // grid of the per-node moment sums.

@@ -745,6 +745,64 @@ def tracker_streams(num_streams: int = 32, frames: int = 8):
             "note": "host-timed steps (one frame of every stream), first step excluded"}
 
 
+def served_large_maps(steps: int) -> dict:
+    """The served configuration with each stream's local map at the configuration's
+    ceiling: initial maps of 20 static 128 x 8192 scans (about 14.6M points, 1.2M surfels
+    per stream, 16 resident), the same request mix.  Served steps (saturated, device
+    inputs) after one warm-up, Poisson latency, and the same step with the admission cap
+    (the bytes admitted requests may hold; resident maps are not counted) at a third of
+    the uncapped peak, so that admission throttles the build passes."""
+    import torch
+
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import streams
+    poi = streams.make_trace(TRACE_SEED, num_streams=STREAMS, scans_per_stream=SCANS, rate_hz=RATE_HZ,
+                             map_scans=20, map_layout=(128, 8192, (-22.5, 22.5)), threads=16)
+    sat = streams.saturated(poi)
+    inputs = [(torch.from_numpy(r.xyz).cuda(), torch.from_numpy(r.stamps).cuda()) for r in sat.requests]
+
+    def step(**kw):
+        srv = kds.Server(tree=TREE, icp=ICP, ct=CT, map_every=MAP_EVERY, **kw)
+        try:
+            for st in sat.streams:
+                srv.add_stream(st.map_xyz, st.max_points)
+            tickets = [srv.submit(r.stream, r.kind, x, s_, r.X0, r.v0, r.arrival)
+                       for r, (x, s_) in zip(sat.requests, inputs)]
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            srv.start()
+            srv.drain(900.0)
+            torch.cuda.synchronize()
+            e1.record()
+            e1.synchronize()
+            res = [srv.result(t) for t in tickets]
+            return e0.elapsed_time(e1), res, srv.stats()
+        finally:
+            srv.free()
+
+    step()
+    times = []
+    for _ in range(max(1, min(steps, 3))):
+        ms, res, st = step()
+        times.append(ms)
+    ms = float(np.median(times))
+    resident = int(st["peak_reserved"])
+    cap = int(resident // 3)
+    ms_cap, res_cap, st_cap = step(hbm_cap=cap)
+    same = all(np.array_equal(a["X"], b["X"]) for a, b in zip(res, res_cap))
+    lat_srv, _, _ = streams.serve(poi, tree=TREE, icp=ICP, ct=CT, map_every=MAP_EVERY, timeout=900.0)
+    lat = np.array([1e3 * (q["t_done"] - q["t_arrival"]) for q in lat_srv])
+    return {"initial_map_points": [int(len(s_.map_xyz)) for s_ in sat.streams],
+            "requests": len(sat.requests), "ms_per_step": ms, "alignments_per_s": len(sat.requests) / (ms / 1e3),
+            "latency_ms_poisson": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "peak_reserved_bytes": resident, "map_rebuilds": int(st["map_builds"]),
+            "capped": {"hbm_cap_bytes": cap, "ms_per_step": ms_cap,
+                       "alignments_per_s": len(sat.requests) / (ms_cap / 1e3),
+                       "peak_reserved_bytes": int(st_cap["peak_reserved"]), "build_passes": int(st_cap["build_passes"]),
+                       "results_identical_to_uncapped": bool(same)}}
+
+
 def forest_pass(steps: int, scans: int = 5) -> dict:
     """The build workload of the served step on its own: the first `scans` requests of
     every stream of the trace (80 clouds by default) built as one forest pass
@@ -804,6 +862,8 @@ def main():
                     help="run only the tracker-step leg and print its JSON (for profiling it)")
     ap.add_argument("--forest-only", action="store_true",
                     help="run only the served step's build workload (one forest pass of 80 scans) and print its JSON")
+    ap.add_argument("--large-maps", action="store_true",
+                    help="add the served leg with 1.2M-surfel initial maps per stream (about a minute more)")
     args = ap.parse_args()
     if args.forest_only:
         import torch
@@ -1009,6 +1069,8 @@ def main():
         line["single_alignments"] = single_alignments(args.steps, peak, roofline["peak_source"],
                                                       cpu=world == 1 and not args.no_cpu)
         line["batched_ba"] = batched_ba(args.steps)
+        if args.large_maps:
+            line["served_large_maps"] = served_large_maps(args.steps)
         line["scan_input"] = scan_input(args.steps)
         line["tracker_step"] = tracker_step(cpu=world == 1 and not args.no_cpu)
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -83,10 +83,12 @@ class Trace:
 
 def make_trace(seed: int, num_streams: int = 16, scans_per_stream: int = 20, rate_hz: float = 10.0,
                saturate: bool = False, ct_fraction: float = 0.7, map_scans: int = 5, beam_mix=BEAM_MIX,
-               scene_seed: int = 1005, guess_t: float = 0.1, guess_deg: float = 1.0, threads: int = 8) -> Trace:
+               scene_seed: int = 1005, guess_t: float = 0.1, guess_deg: float = 1.0, threads: int = 8,
+               map_layout=None) -> Trace:
     """A served-registration trace.  saturate=True makes every request arrive at 0
     (submitted round-robin by scan index); otherwise arrivals are Poisson at rate_hz
-    per stream."""
+    per stream.  map_layout = (beams, cols, elevation range) of the initial maps' static
+    scans (default: the stream's own layout)."""
     rng = np.random.default_rng(seed)
     boxes = synth.scene(scene_seed)
     tr = Trace()
@@ -105,8 +107,9 @@ def make_trace(seed: int, num_streams: int = 16, scans_per_stream: int = 20, rat
             X = compose(X, back)
             poses_back.append(X)
         pts = []
+        mb, mc, me = (beams, cols, elev) if map_layout is None else map_layout
         for k, Xm in enumerate(poses_back):
-            xyz, _ = synth.scan(boxes, Xm, None, beams=beams, cols=cols, elev=elev,
+            xyz, _ = synth.scan(boxes, Xm, None, beams=mb, cols=mc, elev=me,
                                 seed=seed * 100003 + s * 1009 + 500 + k, threads=threads)
             pts.append(synth.transform(xyz, Xm))
         tr.streams.append(StreamTrace(beams=beams, max_points=beams * cols,

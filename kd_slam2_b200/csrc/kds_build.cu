@@ -1136,6 +1136,321 @@ __global__ void k_level_advance(LevelState* ls, const int32_t* bsum, int nblocks
   ls->max_next = 0;
 }
 
+// ---- deep levels: whole subtrees in shared memory --------------------------------------
+// Once every node of a level has at most kDeepMax points, each of them is the root of a
+// subtree that one block builds to the end in shared memory: the points are loaded once,
+// and every depth below runs the same steps as the level kernels -- decide (thread per
+// node, from the node's exact sums), children numbered by a block scan, stable ballot
+// partition by whichSide (warp per node) with the smaller child summed on the way (the
+// other = parent - smaller).  The arithmetic and the partition order are those of
+// k_decide / k_small_part, so the nodes are bit-identical to a level-by-level build.
+// Nodes below the roots are written as DeepNode records tagged (subtree, depth, rank);
+// k_deep_place then puts them at their breadth-first positions: depth by depth, subtree
+// by subtree in the roots' order, by rank inside a subtree -- the order in which the
+// level kernels would have numbered them.
+constexpr int kDeepMax = 1024;     // largest subtree root
+constexpr int kDeepThreads = 256;
+constexpr int kDeepWarps = kDeepThreads / 32;
+constexpr int kDeepBlocksPerSM = 2;
+static_assert(kDeepMax <= kBig, "deep subtree roots are summed by k_root_moments");
+
+struct DeepNode {
+  float mean[3], dir[3];
+  double dts_mean, dts_cov;
+  double prop[3];
+  int32_t start, end;     // point offsets inside the subtree
+  int32_t sub;            // subtree ordinal: its root is node lb + sub
+  int32_t depth;          // >= 1: levels below the root
+  int32_t rank;           // breadth-first position among the subtree's nodes of this depth
+  int32_t q;              // split nodes: children ranks 2q, 2q + 1; leaves: -1
+  int32_t parent_rank;    // rank of the parent at depth - 1
+  int32_t has_prop;
+};
+static_assert(sizeof(DeepNode) == 96, "DeepNode layout");
+static_assert(sizeof(DeepNode) <= 11 * sizeof(U128), "a DeepNode fits the sums slot of one node");
+
+struct DeepSmem {
+  float4 pts[2][kDeepMax];      // w = the point's index in load order (as int bits)
+  double st[kDeepMax];          // stamps, load order
+  int32_t gid[kDeepMax];        // global point ids, load order
+  uint32_t range[2][kDeepMax];  // node start | end << 16 (subtree offsets), by depth parity
+  int32_t prank[2][kDeepMax];   // parent's rank, by depth parity
+  int32_t list[kDeepMax];       // q -> rank of the q-th split node of the depth
+  uint8_t split[kDeepMax];
+  int sm[32];
+  int base, nsplit, base_prev;
+};
+
+__global__ void __launch_bounds__(kDeepThreads, kDeepBlocksPerSM)
+    k_deep_build(BNode* nodes, LevelState* ls, PointBufs B, const double* ts0, const U128* mom, BuildParams P,
+                 double* root_frame, DeepNode* dn, int32_t dn_cap, int32_t* dn_count, U128* ring, int32_t* counts,
+                 int32_t dcap) {
+  extern __shared__ __align__(16) unsigned char deep_smem_raw[];
+  DeepSmem& S = *reinterpret_cast<DeepSmem*>(deep_smem_raw);
+  const int lb = ls->lb, le = ls->le, cur0 = ls->cur;
+  const int nroots = le - lb;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  U128* myring = ring + (size_t)blockIdx.x * 2 * kDeepMax * 11;
+  for (int sub = blockIdx.x; sub < nroots; sub += gridDim.x) {
+    const int R = lb + sub;
+    BNode root = nodes[R];
+    const int n = root.end - root.start;
+    const int pbase = root.start;
+    const double t0 = ts0[root.tree];
+    {
+      const float4* pin = B.p[cur0];
+      const double* sin_ = B.s[cur0];
+      const int32_t* iin = B.id[cur0];
+      for (int i = tid; i < n; i += kDeepThreads) {
+        float4 p = pin[pbase + i];
+        p.w = __int_as_float(i);
+        S.pts[0][i] = p;
+        S.st[i] = sin_[pbase + i];
+        S.gid[i] = iin[pbase + i];
+      }
+    }
+    if (tid == 0) {
+      S.range[0][0] = (uint32_t)n << 16;
+      S.prank[0][0] = -1;
+      S.base = 0;
+      S.base_prev = 0;
+    }
+    __syncthreads();
+    int cnt = 1, c = 0;
+    for (int d = 0; cnt > 0; ++d, c ^= 1) {
+      // ---- decide: thread per node of this depth; record slots for the depth's nodes
+      if (d > 0 && tid == 0) {
+        S.base_prev = S.base;
+        const int b = atomicAdd(dn_count, cnt);
+        S.base = b;
+        if (b + cnt > dn_cap) ls->error = 1;
+      }
+      __syncthreads();
+      const int base = S.base, base_prev = S.base_prev;
+      const bool room = d == 0 || base + cnt <= dn_cap;  // depth 0 writes no record
+      const U128* psums = d == 0 ? mom + (size_t)R * 11 : myring + (size_t)(d & 1) * kDeepMax * 11;
+      for (int r = tid; r < cnt && room; r += kDeepThreads) {
+        const uint32_t rg = S.range[c][r];
+        const int st = (int)(rg & 0xffffu), en = (int)(rg >> 16);
+        BNode nd;
+        if (d == 0) {
+          nd = root;
+        } else {
+          memset(&nd, 0, sizeof(nd));
+          nd.level = root.level + d;
+          nd.tree = root.tree;
+          nd.has_parent = 1;
+          const int pr = S.prank[c][r];
+          if (d == 1) {  // the root's decision, written at depth 0
+            for (int k = 0; k < 3; ++k) nd.par_prop[k] = nodes[R].prop[k];
+            nd.par_has = nodes[R].has_prop;
+          } else {
+            const DeepNode& pn = dn[base_prev + pr];
+            nd.par_has = pn.has_prop;
+            for (int k = 0; k < 3; ++k) nd.par_prop[k] = pn.prop[k];
+          }
+        }
+        double Sd[11];
+        const U128* ms = d == 0 ? psums : psums + (size_t)r * 11;
+        for (int k = 0; k < 11; ++k) Sd[k] = fx_to_d(ms[k]);
+        decide(Sd, en - st, nd, P, nd.level == 0 ? root_frame + (size_t)nd.tree * kRootFrame : nullptr);
+        S.split[r] = nd.split ? 1 : 0;
+        if (d == 0) {
+          nodes[R] = nd;  // left / right follow in k_deep_place
+        } else {
+          DeepNode x;
+          for (int k = 0; k < 3; ++k) {
+            x.mean[k] = nd.mean[k];
+            x.dir[k] = nd.dir[k];
+            x.prop[k] = nd.prop[k];
+          }
+          x.dts_mean = nd.dts_mean;
+          x.dts_cov = nd.dts_cov;
+          x.start = st;
+          x.end = en;
+          x.sub = sub;
+          x.depth = d;
+          x.rank = r;
+          x.q = -1;
+          x.parent_rank = S.prank[c][r];
+          x.has_prop = nd.has_prop;
+          dn[base + r] = x;
+        }
+      }
+      __syncthreads();
+      if (!room) break;  // out of record slots: the build reports KDS_ERR_CAPACITY
+      // ---- children numbering: split ranks by a block scan in rank order
+      {
+        int carry = 0;
+        for (int r0 = 0; r0 < cnt; r0 += kDeepThreads) {
+          const int r = r0 + tid;
+          const int f = (r < cnt && S.split[r]) ? 1 : 0;
+          int tot;
+          const int q = block_scan(f, S.sm, &tot) + carry;
+          if (f) {
+            S.list[q] = r;
+            if (d > 0) dn[base + r].q = q;
+          }
+          carry += tot;
+        }
+        if (tid == 0) {
+          S.nsplit = carry;
+          if (carry > 0) {
+            if (d + 1 < dcap) counts[(size_t)(d + 1) * nroots + sub] = 2 * carry;
+            else ls->error = 1;
+          }
+        }
+      }
+      __syncthreads();
+      const int nsplit = S.nsplit;
+      // ---- the leaves' point order, then the partition of the split nodes (warp per node)
+      for (int r = w; r < cnt; r += kDeepWarps) {
+        if (S.split[r]) continue;
+        const uint32_t rg = S.range[c][r];
+        const int st = (int)(rg & 0xffffu), en = (int)(rg >> 16);
+        for (int i = st + lane; i < en; i += 32) B.perm[pbase + i] = S.gid[__float_as_int(S.pts[c][i].w)];
+      }
+      for (int q = w; q < nsplit; q += kDeepWarps) {
+        const int r = S.list[q];
+        const uint32_t rg = S.range[c][r];
+        const int st = (int)(rg & 0xffffu), en = (int)(rg >> 16);
+        float mean[3], dir[3];
+        if (d == 0) {
+          for (int k = 0; k < 3; ++k) { mean[k] = nodes[R].mean[k]; dir[k] = nodes[R].dir[k]; }
+        } else {
+          const DeepNode& x = dn[base + r];
+          for (int k = 0; k < 3; ++k) { mean[k] = x.mean[k]; dir[k] = x.dir[k]; }
+        }
+        int nl = 0;
+        for (int k0 = st; k0 < en; k0 += 32) {
+          const int i = k0 + lane;
+          const bool left = i < en && which_side_f(mean, dir, S.pts[c][i]);
+          nl += __popc(__ballot_sync(0xffffffffu, left));
+        }
+        const int mid = st + nl;
+        const bool small_left = mid - st <= en - mid;
+        Moments MS;
+        for (int k = 0; k < 11; ++k) MS.s[k] = u128_zero();
+        int cl = 0, cr = 0;
+        for (int k0 = st; k0 < en; k0 += 32) {
+          const int i = k0 + lane;
+          const bool valid = i < en;
+          float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (valid) p = S.pts[c][i];
+          const bool left = valid && which_side_f(mean, dir, p);
+          const unsigned bl = __ballot_sync(0xffffffffu, left);
+          const unsigned br = __ballot_sync(0xffffffffu, valid && !left);
+          if (valid) {
+            const int dst = left ? (st + cl + __popc(bl & lt)) : (mid + cr + __popc(br & lt));
+            S.pts[c ^ 1][dst] = p;
+            if (left == small_left) moments_add_point(MS, p, S.st[__float_as_int(p.w)], t0);
+          }
+          cl += __popc(bl);
+          cr += __popc(br);
+        }
+        const U128 qs = warp_sum_moments(MS, lane);
+        if (!(lane & 1) && lane < 22) {
+          const int k = lane >> 1;
+          const U128 ps = d == 0 ? psums[k] : psums[(size_t)r * 11 + k];
+          const U128 other = u128_sub(ps, qs);
+          U128* nxt = myring + (size_t)((d + 1) & 1) * kDeepMax * 11;
+          nxt[(size_t)(2 * q) * 11 + k] = small_left ? qs : other;
+          nxt[(size_t)(2 * q + 1) * 11 + k] = small_left ? other : qs;
+        }
+        if (lane == 0) {
+          S.range[c ^ 1][2 * q] = (uint32_t)st | ((uint32_t)mid << 16);
+          S.range[c ^ 1][2 * q + 1] = (uint32_t)mid | ((uint32_t)en << 16);
+          S.prank[c ^ 1][2 * q] = r;
+          S.prank[c ^ 1][2 * q + 1] = r;
+        }
+      }
+      cnt = 2 * nsplit;
+      if (d + 1 >= dcap) cnt = 0;
+      __syncthreads();
+    }
+    __syncthreads();
+  }
+}
+
+// Deep nodes to their breadth-first positions: node (subtree s, depth d, rank r) goes to
+// le + off[d * nroots + s] + r, where off is the exclusive scan of the per-(depth,
+// subtree) node counts in depth-major order.  The roots get their children's indices.
+__global__ void k_deep_place(BNode* nodes, LevelState* ls, const DeepNode* dn, const int32_t* dn_count,
+                             int32_t dn_cap, const int32_t* off, int32_t dcap, int32_t cap_nodes) {
+  if (ls->error) return;  // the build fails; records may be missing
+  const int lb = ls->lb, le = ls->le;
+  const int nroots = le - lb;
+  const int nd_total = min(*dn_count, dn_cap);
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nroots; i += stride) {
+    BNode& rt = nodes[lb + i];
+    if (rt.split && dcap > 1) {
+      rt.left = le + off[(size_t)1 * nroots + i];
+      rt.right = rt.left + 1;
+    } else {
+      rt.left = rt.right = -1;
+    }
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nd_total; i += stride) {
+    const DeepNode x = dn[i];
+    const int s = x.sub, d = x.depth;
+    const BNode& rt = nodes[lb + s];
+    BNode o;
+    memset(&o, 0, sizeof(o));
+    o.start = rt.start + x.start;
+    o.end = rt.start + x.end;
+    o.level = rt.level + d;
+    o.tree = rt.tree;
+    o.split = x.q >= 0 ? 1 : 0;
+    o.mid = o.end;
+    o.left = o.right = -1;
+    if (x.q >= 0 && d + 1 < dcap) {
+      o.left = le + off[(size_t)(d + 1) * nroots + s] + 2 * x.q;
+      o.right = o.left + 1;
+    }
+    o.has_parent = 1;
+    o.has_prop = x.has_prop;
+    o.parent = d == 1 ? lb + s : le + off[(size_t)(d - 1) * nroots + s] + x.parent_rank;
+    for (int k = 0; k < 3; ++k) {
+      o.mean[k] = x.mean[k];
+      o.dir[k] = x.dir[k];
+      o.prop[k] = x.prop[k];
+    }
+    o.dts_mean = x.dts_mean;
+    o.dts_cov = x.dts_cov;
+    const int g = le + off[(size_t)d * nroots + s] + x.rank;
+    if (g >= cap_nodes) {
+      ls->error = 1;
+      continue;
+    }
+    nodes[g] = o;
+  }
+}
+
+// One thread: the level state after the deep levels (every level done), the begin of
+// each deep level, the depth, and the node capacity check.
+__global__ void k_deep_finish(LevelState* ls, const int32_t* off, const int32_t* total, int32_t dcap,
+                              int32_t cap_nodes, int32_t* level_begin) {
+  if (blockIdx.x != 0 || threadIdx.x != 0 || ls->error) return;
+  const int lb = ls->lb, le = ls->le;
+  const int nroots = le - lb;
+  const int tot = *total;
+  int dmax = 0;  // deepest local depth holding nodes
+  for (int d = 1; d < dcap; ++d) {
+    const int b = off[(size_t)d * nroots];
+    const int e = d + 1 < dcap ? off[(size_t)(d + 1) * nroots] : tot;
+    if (e > b) {
+      dmax = d;
+      if (ls->depth + d < kMaxDepth + 1) level_begin[ls->depth + d] = le + b;
+    }
+  }
+  if (le + tot > cap_nodes) ls->error = 1;
+  ls->depth += dmax + 1;
+  ls->lb = ls->le = le + tot;
+  if (ls->depth < kMaxDepth + 1) level_begin[ls->depth] = ls->lb;
+}
+
 // ---- prune and per-tree compaction -----------------------------------------------------
 // Prune in one launch (alive[] zeroed before): a leaf lives if it passes
 // IsGoodLeafPredicate_ (kd/tree/tree_predicates_.h:18-29, in float), an inner node if
@@ -1385,6 +1700,68 @@ int ws_alloc(BuildWs& w, int64_t n, int R, cudaStream_t s) {
 
 }  // namespace
 
+namespace {
+
+// The deep levels of a build whose current level (h, read at the last sync) has no node
+// above kDeepMax points: k_deep_build, the depth-major scan of the per-(depth, subtree)
+// node counts, k_deep_place, k_deep_finish.  The node records of the deep levels are
+// staged in the unused part of the sums array (slots from le on).
+int deep_pass(BuildWs& w, const BuildParams& P, const LevelState& h, cudaStream_t s) {
+  const int lb = h.lb, le = h.le;
+  const int nroots = le - lb;
+  if (nroots <= 0) return KDS_OK;
+  const int dcap = std::max(1, P.max_level - h.depth);
+  DeepNode* dn = reinterpret_cast<DeepNode*>(w.mom + (size_t)le * 11);
+  const int64_t dn_cap64 = ((w.cap_nodes - le) * (int64_t)(11 * sizeof(U128))) / (int64_t)sizeof(DeepNode);
+  const int32_t dn_cap = (int32_t)std::min<int64_t>(dn_cap64, INT32_MAX);
+  const int grid = std::min(nroots, 148 * kDeepBlocksPerSM);
+  const int64_t ncount = (int64_t)dcap * nroots;
+  if (ncount > INT32_MAX / 2) { set_error("kds_tree_build: too many deep subtrees"); return KDS_ERR_CAPACITY; }
+  const size_t bc = carve_size<int32_t>(ncount), bt = carve_size<int32_t>(ncount / 4096 + 2),
+               br = carve_size<U128>((size_t)grid * 2 * kDeepMax * 11);
+  void* blk = nullptr;
+  cudaError_t e = cudaMallocAsync(&blk, 2 * bc + bt + 3 * 256 + br, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error("cudaMallocAsync for the deep tree levels failed: %s", cudaGetErrorString(e));
+    return KDS_ERR_OOM;
+  }
+  char* p = (char*)blk;
+  int32_t* counts = carve<int32_t>(p, ncount);
+  int32_t* off = carve<int32_t>(p, ncount);
+  int32_t* tiles = carve<int32_t>(p, ncount / 4096 + 2);
+  int32_t* total = carve<int32_t>(p, 1);
+  int32_t* dn_count = carve<int32_t>(p, 1);
+  carve<int32_t>(p, 1);
+  U128* ring = carve<U128>(p, (size_t)grid * 2 * kDeepMax * 11);
+  int rc = KDS_OK;
+  static bool attr_set = false;  // the attribute is a property of the kernel, per process
+  if (!attr_set) {
+    e = cudaFuncSetAttribute((const void*)k_deep_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(DeepSmem));
+    if (e == cudaSuccess) attr_set = true;
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(counts, 0, sizeof(int32_t) * ncount, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dn_count, 0, sizeof(int32_t), s);
+  if (e == cudaSuccess) {
+    k_deep_build<<<grid, kDeepThreads, sizeof(DeepSmem), s>>>(w.nodes, w.ls, w.B, w.ts0, w.mom, P, w.root_frame, dn,
+                                                              dn_cap, dn_count, ring, counts, dcap);
+    count_launch();
+    rc = scan_exclusive(counts, off, (int32_t)ncount, tiles, total, s);
+    const int pg = (int)std::min<int64_t>(nblk(std::max<int64_t>(w.cap_nodes - le, nroots), kThreads), kGridBlocks * 4);
+    k_deep_place<<<pg, kThreads, 0, s>>>(w.nodes, w.ls, dn, dn_count, dn_cap, off, dcap, (int32_t)w.cap_nodes);
+    k_deep_finish<<<1, 32, 0, s>>>(w.ls, off, total, dcap, (int32_t)w.cap_nodes, w.level_begin);
+    count_launch();
+    count_launch();
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(blk, s);
+  if (e != cudaSuccess) return cuda_status(e, "deep tree levels", __FILE__, __LINE__);
+  return rc;
+}
+
+}  // namespace
+
 size_t forest_workspace_bytes(int64_t n, int R) { return ws_bytes(std::max<int64_t>(n, 1), std::max(R, 1)); }
 
 // Builds R trees from R clouds stored back to back (offsets[R+1] on the host).
@@ -1465,8 +1842,28 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   // node-range kernels (k_decide, k_level_children, k_big_plan, k_level_advance) share
   // one block count per level; every kernel's result is independent of its grid.
   int64_t level_nodes = R;
+  hls.lb = 0;
+  hls.le = R;
+  hls.depth = 0;
   for (int round = 0; round < kMaxDepth; ++round) {
-    for (int k = 0; k < kLevelsPerSync; ++k) {
+    if (host_max <= kDeepMax) {
+      // every node of the current level fits one block: the rest of every subtree is
+      // built in shared memory, then the host reads the final level state
+      if (round == 0) {  // the roots' sums (every root has at most kBig points)
+        k_root_moments<<<kGridBlocks, kThreads, 0, s>>>(w.nodes, R, w.B, w.ts0, w.mom);
+        count_launch();
+      }
+      rc = deep_pass(w, P, hls, s);
+      if (rc) return rc;
+      KDS_CK(cudaMemcpyAsync(&hls, w.ls, sizeof(LevelState), cudaMemcpyDeviceToHost, s));
+      KDS_CK(cudaStreamSynchronize(s));
+      if (hls.error == 2) { set_error("kds_tree_build: coordinate >= 32768 m, non-finite stamp or dt >= 65536 s"); return KDS_ERR_RANGE; }
+      if (hls.error == 1) { set_error("kds_tree_build: node capacity exceeded"); return KDS_ERR_CAPACITY; }
+      break;
+    }
+    // sync after every level once the largest node is within a few halvings of kDeepMax
+    const int nlev = host_max > 4 * kDeepMax ? kLevelsPerSync : 1;
+    for (int k = 0; k < nlev; ++k) {
       const bool level0 = round == 0 && k == 0;
       const int64_t nodes_bound = level_nodes << k;
       const int lvl_blocks = (int)std::max<int64_t>(1, std::min<int64_t>(kLevelBlocks, (nodes_bound + kThreads - 1) / kThreads));

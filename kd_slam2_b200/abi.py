@@ -357,6 +357,7 @@ SIGNATURES = {
     "kds_batch_create": (C.c_int, [C.POINTER(_P)]),
     "kds_batch_run": (C.c_int, [_P, C.POINTER(Job), _I32, _I32, _P]),
     "kds_batch_autotune": (C.c_int, [_P, C.POINTER(Job), _I32, _P, C.POINTER(_I32), _P]),
+    "kds_batch_configure": (C.c_int, [_P, C.c_int32]),
     "kds_batch_assemble": (C.c_int, [_P, C.POINTER(Factor), _I32, _I32, C.c_float, _P, C.POINTER(_I32), _P, _P,
                                      _P, _P]),
     "kds_batch_free": (None, [_P]),

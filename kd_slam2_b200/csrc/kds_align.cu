@@ -853,6 +853,155 @@ __global__ void __launch_bounds__(kBlock, 4) k_linearize(const JobIn* __restrict
   settle();
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form of a batch: one launch runs every Gauss-Newton iteration of every job.
+// The work items are (iteration, tile) pairs in iteration-major order, handed out by one
+// atomic counter (queue[0]).  Before an item of iteration i runs, its job's iteration
+// i - 1 must have finished: the last tile of that iteration ran the job's FP64 step and
+// then published ready[job] = i (after a fence).  Items are claimed in order, so every
+// earlier item belongs to a running block and every wait ends; the waits are bounded all
+// the same (an expired wait sets error bit 4 and queue[1], and every later wait gives up
+// at once).  A job that has finished skips its remaining items.  The arithmetic of a
+// tile and of the step is k_linearize's, so each job's result is bit-identical to the
+// per-iteration launches.  A block re-stages the fixed tree's top only when its next tile
+// reads another tree.
+constexpr int kWaitPolls = 1 << 22;
+
+template <int KIND>
+__device__ __forceinline__ void persistent_tile(const JobIn& Jn, const LinDev& L, const CacheF& C, const TileDev& T,
+                                                const DNode* staged, int nst, double* swp, float* sfac, double* P) {
+  constexpr int D = KindDim<KIND>::D;
+  constexpr int M = D * (D + 1) / 2 + D;
+  tile_body<KIND>(Jn, L, C, T, staged, nst, swp, sfac, nullptr, nullptr);
+  __syncthreads();
+  for (int k = threadIdx.x; k < kPStride; k += blockDim.x) {
+    if (k >= M && k < kPStats) continue;
+    double acc = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) acc += swp[w * kPStride + k];
+    P[k] = acc;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock, 4) k_linearize_persistent(const JobIn* __restrict__ jobs, JobState* states,
+                                                                 JobOut* outs, kds_stats* logs, LinDev* lins,
+                                                                 const TileDev* __restrict__ tiles, int num_tiles,
+                                                                 int max_iter, int stage, double* partials,
+                                                                 int32_t* ready, unsigned int* queue, int32_t* err) {
+  __shared__ CacheF sC;
+  __shared__ float sfac[kWarps * 32 * kMaxFS];
+  __shared__ double swp[kWarps * kPStride];
+  __shared__ int s_item, s_skip, s_last, s_fail;
+  __shared__ __align__(8) unsigned long long s_mbar;
+  extern __shared__ float4 sDyn[];
+  const DNode* sN = reinterpret_cast<const DNode*>(sDyn);
+  const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&s_mbar);
+  const DNode* staged_for = nullptr;  // tree whose top is in shared memory
+  int nst = 0;                        // nodes staged (0: read global memory)
+  uint32_t phase = 0;                 // parity of the next mbarrier phase
+  bool copies = false;                // a copy was issued (settle before exit)
+  bool fallback = false;              // a wait gave up: read global memory from here on
+  const int items = max_iter * num_tiles;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_item = (int)atomicAdd(&queue[0], 1u);
+      s_fail = 0;
+    }
+    __syncthreads();
+    const int item = s_item;
+    if (item >= items) break;
+    const int it = item / num_tiles;
+    const int tile = item - it * num_tiles;
+    const TileDev T = tiles[tile];
+    JobState& S = states[T.job];
+    if (threadIdx.x == 0) {
+      int skip = 0;
+      for (int polls = 0;; ++polls) {
+        if (*(volatile int32_t*)&S.done) { skip = 1; break; }
+        if (*(volatile int32_t*)&ready[T.job] >= it) {
+          __threadfence();
+          skip = *(volatile int32_t*)&S.done;  // the step that published may have finished the job
+          break;
+        }
+        if (*(volatile unsigned int*)&queue[1]) { skip = 1; break; }
+        if (polls >= kWaitPolls) {
+          report_error(err, 4);
+          atomicExch(&queue[1], 1u);
+          skip = 1;
+          break;
+        }
+        __nanosleep(128);
+      }
+      s_skip = skip;
+    }
+    __syncthreads();
+    if (s_skip) continue;
+    const JobIn& Jn = jobs[T.job];
+    const LinDev& L = lins[T.lin];
+    const int want = fallback ? 0 : min(stage, L.f_num_nodes);
+    if (want > 0 && (L.fnodes != staged_for || want != nst)) {
+      const uint32_t bytes = (uint32_t)want * (uint32_t)sizeof(DNode);
+      if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(sDyn)),
+                     "l"(L.fnodes), "r"(bytes), "r"(mbar)
+                     : "memory");
+      }
+      copies = true;
+      if (!mbar_wait(mbar, phase, g_wait_spins)) atomicOr(&s_fail, 1);
+      phase ^= 1u;
+      __syncthreads();  // one block-wide outcome
+      if (s_fail) {
+        if (threadIdx.x == 0) report_error(err, 1);
+        fallback = true;  // the copy may still land: never stage again, settle at exit
+        staged_for = nullptr;
+        nst = 0;
+      } else {
+        staged_for = L.fnodes;
+        nst = want;
+      }
+    } else if (want == 0) {
+      nst = 0;
+      staged_for = nullptr;
+    }
+    if (threadIdx.x < (int)(sizeof(CacheF) / 4))
+      reinterpret_cast<float*>(&sC)[threadIdx.x] = reinterpret_cast<const float*>(&L.cache)[threadIdx.x];
+    __syncthreads();
+    double* P = partials + (size_t)tile * kPStride;
+    const int use = (L.fnodes == staged_for) ? nst : 0;
+    if (Jn.kind == 0) persistent_tile<0>(Jn, L, sC, T, sN, use, swp, sfac, P);
+    else if (Jn.kind == 1) persistent_tile<1>(Jn, L, sC, T, sN, use, swp, sfac, P);
+    else persistent_tile<2>(Jn, L, sC, T, sN, use, swp, sfac, P);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned prev = atomicAdd(&S.arrive, 1u);
+      s_last = (prev == (unsigned)(Jn.tile_count - 1)) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      const int Mk = Jn.kind == 0 ? 27 : (Jn.kind == 1 ? 90 : 189);
+      job_tail(Jn, S, outs[T.job], logs ? logs + (size_t)T.job * kMaxLog : nullptr, lins, partials, swp, Mk);
+      if (threadIdx.x < 32) {  // every lane that wrote the job's state makes it visible, then publish
+        __threadfence();
+        __syncwarp();
+        if (threadIdx.x == 0) atomicExch(&ready[T.job], it + 1);
+      }
+    }
+  }
+  if (threadIdx.x == 0 && copies) {
+    // the last copy's phase: wait (bounded) until it has landed before the block exits
+    if (!mbar_wait(mbar, phase ^ 1u)) report_error(err, 2);
+  }
+}
+
 // Resets control state, seeds state from the job inputs and writes the first caches.
 __device__ void init_job(int j, const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins) {
   const JobIn& Jn = jobs[j];
@@ -887,9 +1036,11 @@ __device__ void init_job(int j, const JobIn* jobs, JobState* states, JobOut* out
 }
 
 __global__ void k_init_jobs(const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins, int num_jobs,
-                            int32_t* err) {
+                            int32_t* err, int32_t* ready = nullptr, unsigned int* queue = nullptr) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j == 0 && err) *err = 0;
+  if (j == 0 && queue) { queue[0] = 0u; queue[1] = 0u; }
+  if (j < num_jobs && ready) ready[j] = 0;
   if (j >= num_jobs) return;
   init_job(j, jobs, states, outs, lins);
 }
@@ -965,7 +1116,7 @@ int Runner::reserve(int nj, int nl, int nt) {
   cap_tiles = std::max({nt, ot + ot / 2, 1});
   size_t bytes = sizeof(JobIn) * cap_jobs + sizeof(JobState) * cap_jobs + sizeof(JobOut) * cap_jobs +
                  sizeof(kds_stats) * kMaxLog * cap_jobs + sizeof(LinDev) * cap_lins + sizeof(TileDev) * cap_tiles +
-                 sizeof(double) * kPStride * cap_tiles + 9 * 256;
+                 sizeof(double) * kPStride * cap_tiles + sizeof(int32_t) * cap_jobs + 11 * 256;
   cudaError_t e = cudaMalloc(&block, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -988,6 +1139,8 @@ int Runner::reserve(int nj, int nl, int nt) {
   d_tiles = (TileDev*)carve(sizeof(TileDev) * cap_tiles);
   d_partials = (double*)carve(sizeof(double) * kPStride * cap_tiles);
   d_err = (int32_t*)carve(sizeof(int32_t));
+  d_ready = (int32_t*)carve(sizeof(int32_t) * cap_jobs);
+  d_queue = (unsigned int*)carve(2 * sizeof(unsigned int));
   return KDS_OK;
 }
 
@@ -1095,8 +1248,55 @@ double Runner::profile_mean_ms(int* launches) const {
   return n ? sum / n : 0.0;
 }
 
+// Blocks of the persistent kernel: every SM full at its occupancy for `smem` bytes of
+// dynamic shared memory, at most one block per work item.
+static int persistent_grid(size_t smem, int64_t items) {
+  static int nsm = 0;
+  if (nsm == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
+      nsm = 148;
+  }
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_linearize_persistent, kBlock, smem) != cudaSuccess ||
+      per < 1) {
+    cudaGetLastError();
+    per = 1;
+  }
+  return (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)nsm * per));
+}
+
 int Runner::enqueue(cudaStream_t s, int32_t* dbg_match, int32_t* dbg_status) {
   if (num_jobs == 0) return KDS_OK;
+  if (persistent && !dbg_match) {
+    k_init_jobs<<<(num_jobs + 127) / 128, 128, 0, s>>>(d_jobs, d_states, d_outs, d_lins, num_jobs, d_err, d_ready,
+                                                       d_queue);
+    ::kds::count_launch();
+    const int L = max_launches();
+    prof_launches = profiling ? 1 : 0;
+    if (profiling) {
+      int rc = ensure_events(2);
+      if (rc) return rc;
+    }
+    const size_t stage_bytes = (size_t)stage_nodes * sizeof(DNode);
+    if (!persistent_attr_set) {
+      KDS_CK(cudaFuncSetAttribute((const void*)k_linearize_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  200 * 1024));
+      persistent_attr_set = true;
+    }
+    if (num_tiles > 0 && L > 0) {
+      const int grid = persistent_grid(stage_bytes, (int64_t)num_tiles * L);
+      if (profiling) KDS_CK(cudaEventRecordWithFlags(prof_ev[0], s, cudaEventRecordExternal));
+      k_linearize_persistent<<<grid, kBlock, stage_bytes, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
+                                                               num_tiles, L, stage_nodes, d_partials, d_ready,
+                                                               d_queue, d_err);
+      ::kds::count_launch();
+      if (profiling) KDS_CK(cudaEventRecordWithFlags(prof_ev[1], s, cudaEventRecordExternal));
+    }
+    KDS_CK(cudaGetLastError());
+    return KDS_OK;
+  }
   k_init_jobs<<<(num_jobs + 127) / 128, 128, 0, s>>>(d_jobs, d_states, d_outs, d_lins, num_jobs, d_err);
   ::kds::count_launch();
   int L = max_launches();
@@ -1152,6 +1352,7 @@ int Runner::run(cudaStream_t s, bool use_graph, int32_t* dbg_match, int32_t* dbg
   key.push_back(profiling ? 1 : 0);
   key.push_back(stage_nodes);
   key.push_back(order_by_size);
+  key.push_back(persistent);
   if (key != graph_key) {
     // capture only a shape that repeats: a one-off shape (every call of a stream of
     // different scans) costs less launched directly than captured and instantiated

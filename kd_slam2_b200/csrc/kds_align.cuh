@@ -105,6 +105,8 @@ struct Runner {
   TileDev* d_tiles = nullptr;
   double* d_partials = nullptr;  // scratch: one kPStride partial per tile
   int32_t* d_err = nullptr;      // error bits of the last launch sequence (zeroed by k_init_jobs)
+  int32_t* d_ready = nullptr;    // persistent form: per job, the next iteration that may start
+  unsigned int* d_queue = nullptr;  // persistent form: [0] next work item, [1] abort
   std::vector<JobIn> h_jobs;
   std::vector<LinDev> h_lins;
   std::vector<TileDev> h_tiles;
@@ -118,7 +120,11 @@ struct Runner {
   int stage_nodes = 2047;
   // tiles of larger jobs first (1) or in job order (0); tuned by kds_batch_autotune
   int order_by_size = 0;
+  // 1: every iteration of every job in one persistent launch over a device work queue
+  // (k_linearize_persistent); 0: one k_linearize launch per iteration and kind
+  int persistent = 0;
   bool smem_attr_set = false;
+  bool persistent_attr_set = false;
   // optional event pair per linearization launch (measurement only)
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;

@@ -789,6 +789,13 @@ static int batch_inputs(kds_job* jobs, int32_t num_jobs, std::vector<JobIn>& J, 
 // Candidate launch configurations of the autotuner: (tree-top nodes staged per block,
 // tiles of larger jobs first).
 static const int kTuneStage[3] = {0, 1023, 2047};
+// config = stage index + 3 * order_by_size + 6 * persistent
+static const int kTuneConfigs = 12;
+static void apply_config(Runner& R, int c) {
+  R.stage_nodes = kTuneStage[c % 3];
+  R.order_by_size = (c / 3) % 2;
+  R.persistent = c / 6;
+}
 
 int kds_batch_autotune(kds_batch* B, kds_job* jobs, int32_t num_jobs, void* stream, int32_t* chosen,
                        double* ms_out) {
@@ -803,9 +810,8 @@ int kds_batch_autotune(kds_batch* B, kds_job* jobs, int32_t num_jobs, void* stre
   KDS_CK(cudaEventCreate(&e1));
   int best = -1;
   double best_ms = 1e300;
-  for (int c = 0; c < 6 && rc == KDS_OK; ++c) {
-    B->runner.stage_nodes = kTuneStage[c % 3];
-    B->runner.order_by_size = c / 3;
+  for (int c = 0; c < kTuneConfigs && rc == KDS_OK; ++c) {
+    apply_config(B->runner, c);
     double sum = 0.0;
     for (int rep = 0; rep < 5 && rc == KDS_OK; ++rep) {  // two warm-ups (direct, graph capture), three timed
       rc = B->runner.setup(J, lins, s);
@@ -828,9 +834,17 @@ int kds_batch_autotune(kds_batch* B, kds_job* jobs, int32_t num_jobs, void* stre
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
-  B->runner.stage_nodes = kTuneStage[best % 3];
-  B->runner.order_by_size = best / 3;
+  apply_config(B->runner, best);
   if (chosen) *chosen = best;
+  return KDS_OK;
+}
+
+int kds_batch_configure(kds_batch* B, int32_t config) {
+  if (!B || config < 0 || config >= kTuneConfigs) {
+    set_error("kds_batch_configure: config must be in [0, %d)", kTuneConfigs);
+    return KDS_ERR_INVALID_ARG;
+  }
+  apply_config(B->runner, config);
   return KDS_OK;
 }
 

@@ -2,8 +2,9 @@
 
 * Every pair of the batch -- rigid and CT-ICP, uneven sizes, one graph-captured launch
   sequence -- gives the result of its own kds_aligner_compute, bit for bit.
-* The autotuner's configurations (tree-top staging, job order) change the launch shape
-  only: results are identical under the chosen one and under every other one.
+* The autotuner's configurations (tree-top staging, job order, per-iteration launches
+  or one persistent launch over a device work queue) change the launch shape only:
+  results are identical under the chosen one and under every other one.
 """
 import numpy as np
 import pytest
@@ -64,9 +65,24 @@ def test_autotune_keeps_results(workload):
     ref = outputs(kds.Batch().run(jobs))
     b = kds.Batch()
     chosen, ms = b.autotune(jobs)
-    assert 0 <= chosen < 6 and np.all(ms > 0)
+    assert 0 <= chosen < 12 and np.all(ms > 0)
     same(ref, outputs(b.run(jobs)))
     same(ref, outputs(b.run(jobs)))  # graph replay
+
+
+@pytest.mark.parametrize("config", list(range(12)))
+def test_every_configuration_gives_identical_results(workload, config):
+    """Each launch configuration -- the persistent one included, whose blocks wait for a
+    job's previous iteration on the device -- gives every job bit-identical results, run
+    directly and replayed from its graph."""
+    from kd_slam2_b200 import ba
+    wl, trees = workload
+    jobs = ba.jobs(wl, trees, ICP, CT)
+    ref = outputs(kds.Batch().run(jobs, use_graph=False))
+    b = kds.Batch()
+    b.configure(config)
+    for _ in range(3):  # direct, graph capture, graph replay
+        same(ref, outputs(b.run(jobs, use_graph=True)))
 
 
 def test_autotune_as_first_use_of_the_library(tmp_path):

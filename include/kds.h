@@ -365,16 +365,18 @@ int kds_batch_run(kds_batch* b, kds_job* jobs, int32_t num_jobs, int32_t use_gra
 /* Launch-shape autotuner for a job set (no reference counterpart): times the batched
  * launches for each candidate configuration -- tree-top nodes staged in shared memory
  * per block (0, 1023, 2047) x tiles of the larger jobs first or in job order x the
- * form: one linearization launch per iteration and kind (graph-captured), or one
- * persistent launch that runs every iteration of every job from a device work queue --
- * keeps the fastest in the batch handle for the following kds_batch_run calls, and
- * reports its index (config = stage index + 3 * order + 6 * persistent) and the mean
- * milliseconds of all twelve (ms_out: 12 doubles, may be NULL).  The jobs are read, not
- * modified; results do not depend on the configuration. */
+ * form: (0) one linearization launch per iteration and kind (graph-captured), one tile
+ * of 128 moving surfels per block; (1) one persistent launch that runs every iteration
+ * of every job from a device work queue; (2) as (0) with two tiles of a job per block,
+ * each thread keeping two descents in flight -- keeps the fastest in the batch handle
+ * for the following kds_batch_run calls, and reports its index (config = stage index +
+ * 3 * order + 6 * form) and the mean milliseconds of all eighteen (ms_out: 18 doubles,
+ * may be NULL).  The jobs are read, not modified; results do not depend on the
+ * configuration. */
 int kds_batch_autotune(kds_batch* b, kds_job* jobs, int32_t num_jobs, void* stream, int32_t* chosen,
                        double* ms_out);
 /* Sets the batch's launch configuration directly (an index as kds_batch_autotune reports
- * it, 0..11); KDS_ERR_INVALID_ARG otherwise. */
+ * it, 0..17); KDS_ERR_INVALID_ARG otherwise. */
 int kds_batch_configure(kds_batch* b, int32_t config);
 
 /* One multi-view bundle-adjustment factor over a job of the last kds_batch_run.

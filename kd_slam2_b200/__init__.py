@@ -592,13 +592,13 @@ class Batch:
         """Chooses the launch configuration for this job set; returns (index, ms per config)."""
         arr = (L.Job * len(jobs))(*jobs)
         chosen = C.c_int32()
-        ms = np.zeros(12)
+        ms = np.zeros(18)
         _check(_lib.kds_batch_autotune(self._h, arr, len(jobs), stream, C.byref(chosen), ms.ctypes.data),
                "kds_batch_autotune")
         return chosen.value, ms
 
     def configure(self, config: int) -> None:
-        """Launch configuration by index (stage + 3 * order + 6 * persistent), as autotune reports it."""
+        """Launch configuration by index (stage + 3 * order + 6 * form), as autotune reports it."""
         _check(_lib.kds_batch_configure(self._h, int(config)), "kds_batch_configure")
 
     def run(self, jobs, use_graph: bool = True, stream=None):

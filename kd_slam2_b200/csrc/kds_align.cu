@@ -156,24 +156,24 @@ template <> struct KindDim<0> { static constexpr int D = 6; };
 template <> struct KindDim<1> { static constexpr int D = 12; };
 template <> struct KindDim<2> { static constexpr int D = 18; };
 
+// The query of one moving leaf: optional CT warp (applyVelocities) and the moving-to-
+// fixed transform Xmf.
 template <int KIND>
-__device__ __forceinline__ void leaf_term(const CacheF& C, const DNode* F, int fnn, const float* fdts,
-                                          const DNode* staged, int nstaged, float4 md,
-                                          float4 nr, const ParamsF& P, bool stats_mode, int& status, int& match,
-                                          float& e_out, float& gamma_out, float* J) {
-  constexpr int D = KindDim<KIND>::D;
-#pragma unroll
-  for (int i = 0; i < D; ++i) J[i] = 0.f;
-  e_out = 0.f;
-  gamma_out = 0.f;
-  F3 m = f3(md.x, md.y, md.z), n = f3(nr.x, nr.y, nr.z);
-  float dt = md.w;
-  F3 mw = m, nw = n;
-  if (KIND != 0) warp_x(C.v, dt, m, n, mw, nw);
-  F3 q = apply_iso_x(C.Xmf, mw);
-  // greedy descent (kd/icp/icp_impl_.h:116-121): no backtracking
-  int idx = fnn > 0 ? 0 : -1;
-  DNode nd;
+__device__ __forceinline__ void leaf_query(const CacheF& C, float4 md, float4 nr, F3& m, F3& n, F3& mw, F3& nw,
+                                           F3& q) {
+  m = f3(md.x, md.y, md.z);
+  n = f3(nr.x, nr.y, nr.z);
+  mw = m;
+  nw = n;
+  if (KIND != 0) warp_x(C.v, md.w, m, n, mw, nw);
+  q = apply_iso_x(C.Xmf, mw);
+}
+
+// Greedy descent (kd/icp/icp_impl_.h:116-121): no backtracking.  idx = the leaf reached,
+// or -1 where the descent steps into a pruned child; nd = its record.
+__device__ __forceinline__ void descend(const DNode* F, int fnn, const DNode* staged, int nstaged, F3 q, int& idx,
+                                        DNode& nd) {
+  idx = fnn > 0 ? 0 : -1;
   while (idx >= 0) {
     nd = (idx < nstaged) ? staged[idx] : load_node(F + idx);
     int l = node_left(nd), r = node_right(nd);
@@ -181,6 +181,50 @@ __device__ __forceinline__ void leaf_term(const CacheF& C, const DNode* F, int f
     bool side = dot3x(node_dir(nd), sub3x(q, node_mean(nd))) > 0.0f;
     idx = side ? l : r;
   }
+}
+
+// Two descents through the same tree in lockstep: both chains' node loads are issued
+// before either is used, so a thread keeps two dependent load chains in flight.  Each
+// chain takes exactly the steps of descend().
+__device__ __forceinline__ void descend2(const DNode* F, int fnn, const DNode* staged, int nstaged, bool va, F3 qa,
+                                         int& ia, DNode& na, bool vb, F3 qb, int& ib, DNode& nb) {
+  ia = (va && fnn > 0) ? 0 : -1;
+  ib = (vb && fnn > 0) ? 0 : -1;
+  bool ra = ia >= 0, rb = ib >= 0;  // still descending
+  while (ra || rb) {
+    if (ra) na = (ia < nstaged) ? staged[ia] : load_node(F + ia);
+    if (rb) nb = (ib < nstaged) ? staged[ib] : load_node(F + ib);
+    if (ra) {
+      const int l = node_left(na), r = node_right(na);
+      if (l < 0 && r < 0) {
+        ra = false;
+      } else {
+        ia = dot3x(node_dir(na), sub3x(qa, node_mean(na))) > 0.0f ? l : r;
+        ra = ia >= 0;
+      }
+    }
+    if (rb) {
+      const int l = node_left(nb), r = node_right(nb);
+      if (l < 0 && r < 0) {
+        rb = false;
+      } else {
+        ib = dot3x(node_dir(nb), sub3x(qb, node_mean(nb))) > 0.0f ? l : r;
+        rb = ib >= 0;
+      }
+    }
+  }
+}
+
+// Gates, error, Jacobian and robust weight of one leaf whose descent ended at idx / nd.
+template <int KIND>
+__device__ __forceinline__ void leaf_math(const CacheF& C, F3 m, F3 n, float dt, F3 mw, F3 nw, int idx,
+                                          const DNode& nd, const float* fdts, const ParamsF& P, bool stats_mode,
+                                          int& status, int& match, float& e_out, float& gamma_out, float* J) {
+  constexpr int D = KindDim<KIND>::D;
+#pragma unroll
+  for (int i = 0; i < D; ++i) J[i] = 0.f;
+  e_out = 0.f;
+  gamma_out = 0.f;
   match = idx;
   if (idx < 0) { status = ST_BAD; return; }
   F3 pf = node_mean(nd), nf = node_dir(nd);
@@ -214,6 +258,19 @@ __device__ __forceinline__ void leaf_term(const CacheF& C, const DNode* F, int f
   gamma_out = gamma;
 }
 
+template <int KIND>
+__device__ __forceinline__ void leaf_term(const CacheF& C, const DNode* F, int fnn, const float* fdts,
+                                          const DNode* staged, int nstaged, float4 md,
+                                          float4 nr, const ParamsF& P, bool stats_mode, int& status, int& match,
+                                          float& e_out, float& gamma_out, float* J) {
+  F3 m, n, mw, nw, q;
+  leaf_query<KIND>(C, md, nr, m, n, mw, nw, q);
+  int idx;
+  DNode nd;
+  descend(F, fnn, staged, nstaged, q, idx, nd);
+  leaf_math<KIND>(C, m, n, md.w, mw, nw, idx, nd, fdts, P, stats_mode, status, match, e_out, gamma_out, J);
+}
+
 // entry k of the packed D(D+1)/2 + D vector -> (row, col); col == D means "e"
 __device__ __forceinline__ void entry_rc(int D, int k, int& r, int& c) {
   int T = D * (D + 1) / 2;
@@ -228,27 +285,15 @@ constexpr int kBlock = 128;
 constexpr int kWarps = kBlock / 32;
 constexpr int kMaxFS = 21;  // factor row stride (D + 2, padded to odd)
 
+// One warp's share of a tile partial from its 32 leaves' terms (leaf = lane): stats by
+// ballots, chi2 sums by xor butterfly, and gamma J^T J, gamma J^T e as float Kahan sums
+// over the lanes (lane k owns packed entries k, k + 32, ...) stored as s - comp in FP64.
 template <int KIND>
-__device__ __forceinline__ void tile_body(const JobIn& Jn, const LinDev& L, const CacheF& C, const TileDev& T,
-                                          const DNode* staged, int nstaged,
-                                          double* wpart /* [kWarps][kPStride] */, float* fac /* [kWarps][32][kMaxFS] */,
-                                          int32_t* dbg_match, int32_t* dbg_status) {
+__device__ __forceinline__ void tile_reduce(int status, float e, float gamma, const float* J, double* wpart,
+                                            float* fac) {
   constexpr int D = KindDim<KIND>::D;
   constexpr int M = D * (D + 1) / 2 + D;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int i = T.leaf_begin + threadIdx.x;
-  int status = ST_NONE, match = -1;
-  float e = 0.f, gamma = 0.f;
-  float J[D];
-#pragma unroll
-  for (int k = 0; k < D; ++k) J[k] = 0.f;
-  if (i < T.leaf_end) {
-    float4 md = __ldg(Jn.m_md + i);
-    float4 nr = __ldg(Jn.m_nrm + i);
-    leaf_term<KIND>(C, L.fnodes, L.f_num_nodes, L.fdts, staged, nstaged, md, nr, Jn.P, Jn.stats_mode != 0, status,
-                    match, e, gamma, J);
-    if (dbg_match) { dbg_match[i] = match; dbg_status[i] = status; }
-  }
   bool contrib = status == ST_INLIER || status == ST_OUTLIER;
   float* row = fac + (w * 32 + lane) * kMaxFS;
 #pragma unroll
@@ -296,6 +341,79 @@ __device__ __forceinline__ void tile_body(const JobIn& Jn, const LinDev& L, cons
     wp[kPStats + 4] = c_fn;
     wp[kPStats + 5] = chi2;
     wp[kPStats + 6] = chi2k;
+  }
+  __syncwarp();  // the warp's rows may be rewritten after this
+}
+
+template <int KIND>
+__device__ __forceinline__ void tile_body(const JobIn& Jn, const LinDev& L, const CacheF& C, const TileDev& T,
+                                          const DNode* staged, int nstaged,
+                                          double* wpart /* [kWarps][kPStride] */, float* fac /* [kWarps][32][kMaxFS] */,
+                                          int32_t* dbg_match, int32_t* dbg_status) {
+  constexpr int D = KindDim<KIND>::D;
+  const int i = T.leaf_begin + threadIdx.x;
+  int status = ST_NONE, match = -1;
+  float e = 0.f, gamma = 0.f;
+  float J[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) J[k] = 0.f;
+  if (i < T.leaf_end) {
+    float4 md = __ldg(Jn.m_md + i);
+    float4 nr = __ldg(Jn.m_nrm + i);
+    leaf_term<KIND>(C, L.fnodes, L.f_num_nodes, L.fdts, staged, nstaged, md, nr, Jn.P, Jn.stats_mode != 0, status,
+                    match, e, gamma, J);
+    if (dbg_match) { dbg_match[i] = match; dbg_status[i] = status; }
+  }
+  tile_reduce<KIND>(status, e, gamma, J, wpart, fac);
+}
+
+// Two tiles of one (job, fixed entry) per block: thread t takes leaf t of both, runs the
+// two descents in lockstep, then reduces tile A and tile B one after the other with
+// tile_body's arithmetic, so each tile's partial is bit-identical to one-tile blocks.
+template <int KIND>
+__device__ __forceinline__ void tile_body_pair(const JobIn& Jn, const LinDev& L, const CacheF& C, const TileDev& TA,
+                                               const TileDev& TB, bool has_b, const DNode* staged, int nstaged,
+                                               double* wpa, double* wpb, float* fac, int32_t* dbg_match,
+                                               int32_t* dbg_status) {
+  constexpr int D = KindDim<KIND>::D;
+  const int ia = TA.leaf_begin + threadIdx.x, ib = TB.leaf_begin + threadIdx.x;
+  const bool va = ia < TA.leaf_end, vb = has_b && ib < TB.leaf_end;
+  F3 ma, na, mwa, nwa, qa, mb, nb, mwb, nwb, qb;
+  float dta = 0.f, dtb = 0.f;
+  if (va) {
+    const float4 md = __ldg(Jn.m_md + ia), nr = __ldg(Jn.m_nrm + ia);
+    leaf_query<KIND>(C, md, nr, ma, na, mwa, nwa, qa);
+    dta = md.w;
+  }
+  if (vb) {
+    const float4 md = __ldg(Jn.m_md + ib), nr = __ldg(Jn.m_nrm + ib);
+    leaf_query<KIND>(C, md, nr, mb, nb, mwb, nwb, qb);
+    dtb = md.w;
+  }
+  int xa, xb;
+  DNode nda, ndb;
+  descend2(L.fnodes, L.f_num_nodes, staged, nstaged, va, qa, xa, nda, vb, qb, xb, ndb);
+  {
+    int status = ST_NONE, match = -1;
+    float e = 0.f, gamma = 0.f, J[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) J[k] = 0.f;
+    if (va) {
+      leaf_math<KIND>(C, ma, na, dta, mwa, nwa, xa, nda, L.fdts, Jn.P, Jn.stats_mode != 0, status, match, e, gamma, J);
+      if (dbg_match) { dbg_match[ia] = match; dbg_status[ia] = status; }
+    }
+    tile_reduce<KIND>(status, e, gamma, J, wpa, fac);
+  }
+  {
+    int status = ST_NONE, match = -1;
+    float e = 0.f, gamma = 0.f, J[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) J[k] = 0.f;
+    if (vb) {
+      leaf_math<KIND>(C, mb, nb, dtb, mwb, nwb, xb, ndb, L.fdts, Jn.P, Jn.stats_mode != 0, status, match, e, gamma, J);
+      if (dbg_match) { dbg_match[ib] = match; dbg_status[ib] = status; }
+    }
+    tile_reduce<KIND>(status, e, gamma, J, wpb, fac);
   }
 }
 
@@ -853,6 +971,85 @@ __global__ void __launch_bounds__(kBlock, 4) k_linearize(const JobIn* __restrict
   settle();
 }
 
+// One Gauss-Newton iteration with two tiles per block: the block list pairs consecutive
+// tiles of the same (job, fixed entry) (the second index is -1 for a job's odd last
+// tile).  Each thread keeps two descents in flight; the partials, the arrival count and
+// the job's step are those of k_linearize.
+template <int KIND>
+__global__ void __launch_bounds__(kBlock, 4) k_linearize_pair(const JobIn* __restrict__ jobs, JobState* states,
+                                                           JobOut* outs, kds_stats* logs, LinDev* lins,
+                                                           const TileDev* __restrict__ tiles,
+                                                           const int2* __restrict__ pairs, int pair0, int stage,
+                                                           double* partials, int32_t* dbg_match, int32_t* dbg_status,
+                                                           int32_t* err) {
+  constexpr int D = KindDim<KIND>::D;
+  constexpr int M = D * (D + 1) / 2 + D;
+  __shared__ CacheF sC;
+  __shared__ float sfac[kWarps * 32 * kMaxFS];
+  __shared__ double swp[2][kWarps * kPStride];
+  __shared__ int s_last;
+  __shared__ __align__(8) unsigned long long s_mbar;
+  const int2 pr = pairs[pair0 + blockIdx.x];
+  const TileDev TA = tiles[pr.x];
+  const bool has_b = pr.y >= 0;
+  const TileDev TB = has_b ? tiles[pr.y] : TA;
+  JobState& S = states[TA.job];
+  if (*(volatile int32_t*)&S.done) return;
+  const JobIn& Jn = jobs[TA.job];
+  const LinDev& L = lins[TA.lin];
+  extern __shared__ float4 sDyn[];
+  const DNode* sN = reinterpret_cast<const DNode*>(sDyn);
+  int nst = min(stage, L.f_num_nodes);
+  const uint32_t bytes = (uint32_t)nst * (uint32_t)sizeof(DNode);
+  const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&s_mbar);
+  if (threadIdx.x == 0 && bytes > 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(sDyn)),
+                 "l"(L.fnodes), "r"(bytes), "r"(mbar)
+                 : "memory");
+  }
+  if (threadIdx.x < (int)(sizeof(CacheF) / 4))
+    reinterpret_cast<float*>(&sC)[threadIdx.x] = reinterpret_cast<const float*>(&L.cache)[threadIdx.x];
+  __syncthreads();
+  if (bytes > 0 && !mbar_wait(mbar, 0u, g_wait_spins)) {
+    report_error(err, 1);  // read the whole tree from global memory
+    nst = 0;
+  }
+  auto settle = [&]() {
+    if (threadIdx.x == 0 && bytes > 0 && !mbar_wait(mbar, 0u)) report_error(err, 2);
+  };
+  tile_body_pair<KIND>(Jn, L, sC, TA, TB, has_b, sN, nst, swp[0], swp[1], sfac, dbg_match, dbg_status);
+  __syncthreads();
+  for (int h = 0; h < (has_b ? 2 : 1); ++h) {
+    double* P = partials + (size_t)(h ? pr.y : pr.x) * kPStride;
+    for (int k = threadIdx.x; k < kPStride; k += blockDim.x) {
+      if (k >= M && k < kPStats) continue;
+      double acc = 0.0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) acc += swp[h][w * kPStride + k];
+      P[k] = acc;
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned nt = has_b ? 2u : 1u;
+    unsigned prev = atomicAdd(&S.arrive, nt);
+    s_last = (prev + nt == (unsigned)Jn.tile_count) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_last) {
+    settle();
+    return;
+  }
+  __threadfence();
+  job_tail(Jn, S, outs[TA.job], logs ? logs + (size_t)TA.job * kMaxLog : nullptr, lins, partials, swp[0], M);
+  settle();
+}
+
 // ---------------------------------------------------------------------------
 // Persistent form of a batch: one launch runs every Gauss-Newton iteration of every job.
 // The work items are (iteration, tile) pairs in iteration-major order, handed out by one
@@ -1116,7 +1313,8 @@ int Runner::reserve(int nj, int nl, int nt) {
   cap_tiles = std::max({nt, ot + ot / 2, 1});
   size_t bytes = sizeof(JobIn) * cap_jobs + sizeof(JobState) * cap_jobs + sizeof(JobOut) * cap_jobs +
                  sizeof(kds_stats) * kMaxLog * cap_jobs + sizeof(LinDev) * cap_lins + sizeof(TileDev) * cap_tiles +
-                 sizeof(double) * kPStride * cap_tiles + sizeof(int32_t) * cap_jobs + 11 * 256;
+                 sizeof(double) * kPStride * cap_tiles + sizeof(int32_t) * cap_jobs + sizeof(int2) * cap_tiles +
+                 12 * 256;
   cudaError_t e = cudaMalloc(&block, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -1141,6 +1339,7 @@ int Runner::reserve(int nj, int nl, int nt) {
   d_err = (int32_t*)carve(sizeof(int32_t));
   d_ready = (int32_t*)carve(sizeof(int32_t) * cap_jobs);
   d_queue = (unsigned int*)carve(2 * sizeof(unsigned int));
+  d_pairs = (int2*)carve(sizeof(int2) * cap_tiles);
   return KDS_OK;
 }
 
@@ -1191,14 +1390,28 @@ int Runner::setup(const std::vector<JobIn>& jobs_in, const std::vector<LinDev>& 
     }
     kind_count[kind] = (int)h_tiles.size() - kind_begin[kind];
   }
+  // blocks of two consecutive tiles of one (job, fixed entry), per kind
+  h_pairs.clear();
+  for (int kind = 0; kind < 3; ++kind) {
+    kind_pair_begin[kind] = (int)h_pairs.size();
+    const int e = kind_begin[kind] + kind_count[kind];
+    for (int t = kind_begin[kind]; t < e;) {
+      const bool two = t + 1 < e && h_tiles[t + 1].job == h_tiles[t].job && h_tiles[t + 1].lin == h_tiles[t].lin;
+      h_pairs.push_back(make_int2(t, two ? t + 1 : -1));
+      t += two ? 2 : 1;
+    }
+    kind_pair_count[kind] = (int)h_pairs.size() - kind_pair_begin[kind];
+  }
   int rc = reserve((int)h_jobs.size(), (int)h_lins.size(), (int)h_tiles.size());
   if (rc) return rc;
   num_jobs = (int)h_jobs.size();
   num_tiles = (int)h_tiles.size();
   KDS_CK(cudaMemcpyAsync(d_jobs, h_jobs.data(), sizeof(JobIn) * h_jobs.size(), cudaMemcpyHostToDevice, s));
   KDS_CK(cudaMemcpyAsync(d_lins, h_lins.data(), sizeof(LinDev) * h_lins.size(), cudaMemcpyHostToDevice, s));
-  if (num_tiles)
+  if (num_tiles) {
     KDS_CK(cudaMemcpyAsync(d_tiles, h_tiles.data(), sizeof(TileDev) * h_tiles.size(), cudaMemcpyHostToDevice, s));
+    KDS_CK(cudaMemcpyAsync(d_pairs, h_pairs.data(), sizeof(int2) * h_pairs.size(), cudaMemcpyHostToDevice, s));
+  }
   return KDS_OK;
 }
 
@@ -1310,17 +1523,31 @@ int Runner::enqueue(cudaStream_t s, int32_t* dbg_match, int32_t* dbg_status) {
   const int stage = stage_nodes;
   const size_t stage_bytes = (size_t)stage * sizeof(DNode);
   if (stage_bytes > 0 && !smem_attr_set) {  // static + dynamic shared memory can pass 48 KB
-    for (int k = 0; k < 3; ++k) {
-      const void* f = k == 0 ? (const void*)k_linearize<0> : (k == 1 ? (const void*)k_linearize<1> : (const void*)k_linearize<2>);
-      KDS_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    }
+    const void* fs[6] = {(const void*)k_linearize<0>, (const void*)k_linearize<1>, (const void*)k_linearize<2>,
+                         (const void*)k_linearize_pair<0>, (const void*)k_linearize_pair<1>,
+                         (const void*)k_linearize_pair<2>};
+    for (int k = 0; k < 6; ++k) KDS_CK(cudaFuncSetAttribute(fs[k], cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     smem_attr_set = true;
   }
   for (int i = 0; i < L; ++i) {
     for (int kind = 0; kind < 3; ++kind) {
       if (!kind_count[kind]) continue;
       if (profiling) KDS_CK(cudaEventRecordWithFlags(prof_ev[ev++], s, cudaEventRecordExternal));
-      if (kind == 0)
+      if (pair_tiles) {
+        const int nb = kind_pair_count[kind], p0 = kind_pair_begin[kind];
+        if (kind == 0)
+          k_linearize_pair<0><<<nb, kBlock, stage_bytes, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
+                                                              d_pairs, p0, stage, d_partials, dbg_match, dbg_status,
+                                                              d_err);
+        else if (kind == 1)
+          k_linearize_pair<1><<<nb, kBlock, stage_bytes, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
+                                                              d_pairs, p0, stage, d_partials, dbg_match, dbg_status,
+                                                              d_err);
+        else
+          k_linearize_pair<2><<<nb, kBlock, stage_bytes, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
+                                                              d_pairs, p0, stage, d_partials, dbg_match, dbg_status,
+                                                              d_err);
+      } else if (kind == 0)
         k_linearize<0><<<kind_count[0], kBlock, stage_bytes, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins,
                                                                      d_tiles, kind_begin[0], stage, d_partials,
                                                                      dbg_match, dbg_status, d_err);
@@ -1353,6 +1580,7 @@ int Runner::run(cudaStream_t s, bool use_graph, int32_t* dbg_match, int32_t* dbg
   key.push_back(stage_nodes);
   key.push_back(order_by_size);
   key.push_back(persistent);
+  key.push_back(pair_tiles);
   if (key != graph_key) {
     // capture only a shape that repeats: a one-off shape (every call of a stream of
     // different scans) costs less launched directly than captured and instantiated

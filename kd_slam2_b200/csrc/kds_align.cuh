@@ -107,9 +107,12 @@ struct Runner {
   int32_t* d_err = nullptr;      // error bits of the last launch sequence (zeroed by k_init_jobs)
   int32_t* d_ready = nullptr;    // persistent form: per job, the next iteration that may start
   unsigned int* d_queue = nullptr;  // persistent form: [0] next work item, [1] abort
+  int2* d_pairs = nullptr;          // two-tile blocks: (tile, tile or -1), grouped by kind
   std::vector<JobIn> h_jobs;
   std::vector<LinDev> h_lins;
   std::vector<TileDev> h_tiles;
+  std::vector<int2> h_pairs;
+  int kind_pair_begin[3] = {0, 0, 0}, kind_pair_count[3] = {0, 0, 0};
   int num_jobs = 0, num_tiles = 0;
   int kind_begin[3] = {0, 0, 0}, kind_count[3] = {0, 0, 0};
   cudaGraph_t graph = nullptr;
@@ -123,6 +126,9 @@ struct Runner {
   // 1: every iteration of every job in one persistent launch over a device work queue
   // (k_linearize_persistent); 0: one k_linearize launch per iteration and kind
   int persistent = 0;
+  // 1: two tiles of one (job, fixed entry) per block, two descents in flight per thread
+  // (k_linearize_pair); ignored by the persistent form
+  int pair_tiles = 0;
   bool smem_attr_set = false;
   bool persistent_attr_set = false;
   // optional event pair per linearization launch (measurement only)

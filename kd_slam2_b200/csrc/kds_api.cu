@@ -789,12 +789,15 @@ static int batch_inputs(kds_job* jobs, int32_t num_jobs, std::vector<JobIn>& J, 
 // Candidate launch configurations of the autotuner: (tree-top nodes staged per block,
 // tiles of larger jobs first).
 static const int kTuneStage[3] = {0, 1023, 2047};
-// config = stage index + 3 * order_by_size + 6 * persistent
-static const int kTuneConfigs = 12;
+// config = stage index + 3 * order_by_size + 6 * form; form 0: one launch per iteration
+// and kind, one tile per block; 1: persistent; 2: one launch per iteration and kind, two
+// tiles per block
+static const int kTuneConfigs = 18;
 static void apply_config(Runner& R, int c) {
   R.stage_nodes = kTuneStage[c % 3];
   R.order_by_size = (c / 3) % 2;
-  R.persistent = c / 6;
+  R.persistent = (c / 6) == 1 ? 1 : 0;
+  R.pair_tiles = (c / 6) == 2 ? 1 : 0;
 }
 
 int kds_batch_autotune(kds_batch* B, kds_job* jobs, int32_t num_jobs, void* stream, int32_t* chosen,

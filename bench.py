@@ -414,6 +414,9 @@ def batched_ba(steps: int):
         "batched_over_plain": (len(jobs) / (batch_ms / 1e3)) * plain_s, "plain_sample": len(sample),
         "results_identical_to_plain": bool(same), "autotune_config": int(chosen),
         "autotune_ms": [float(x) for x in tune_ms],
+        "autotune_best_ms_by_form": {name: float(np.min(tune_ms[6 * f:6 * f + 6])) for f, name in
+                                     enumerate(("launch_per_iteration", "persistent", "two_tiles_per_block"))},
+        "autotune_note": "config = staged tree-top nodes index (0, 1023, 2047) + 3 x (larger jobs first) + 6 x form",
         "median_t_err_vs_truth_m": float(np.median(errs[:, 0])), "median_r_err_vs_truth_rad": float(np.median(errs[:, 1])),
         "pose_vs_oracle": ba_pose,
         "factor_step": {"factors": len(factors), "variables": nv, "blocks": int(len(brc)),

@@ -49,10 +49,10 @@ TREE = dict(leaf_max_points=16)
 ICP = dict(max_error=0.5, max_iterations=10)
 CT = dict(max_error=0.5, max_iterations=15, velocity_damping=10.0)
 MAP_EVERY = 5
-# DRAM bytes per point per level of a forest build pass: dram__bytes_read.sum +
-# dram__bytes_write.sum over all kernels of one ncu-captured pass of 80 scans of this trace
-# (5.54M points, 20 levels, 6.30 GB); a step's build traffic scales with its points x levels.
-BUILD_TRAFFIC_PER_POINT_LEVEL = 56.9
+# DRAM bytes per point of a forest build pass: dram__bytes_read.sum + dram__bytes_write.sum
+# over all kernels of one ncu-captured pass of the trace's first 80 scans (bench.py
+# --forest-only); a step's build traffic scales with its points.  None: not captured.
+BUILD_TRAFFIC_PER_POINT = None
 
 
 def pose_err(A, B):
@@ -521,7 +521,10 @@ def single_alignments(steps: int, peak: float, peak_source: str, cpu: bool = Tru
         rm = orc.align(kind, orc.MODE_MIXED, Om, Os, P, X0, v0=v0)
         r64 = orc.align(kind, orc.MODE_FP64, Om, Os, P, X0, v0=v0)
         npts = len(wl["xyz"])
-        pl = M.info.depth * len(wl["map_xyz"])
+        inf = M.info
+        pl = inf.depth * len(wl["map_xyz"])
+        map_alg = 48.0 * inf.global_levels * len(wl["map_xyz"]) + (
+            32.0 * len(wl["map_xyz"]) if inf.global_levels < inf.depth else 0.0)
         line = {
             "scan_points": npts, "scan_leaves": int(leaves), "map_points": int(len(wl["map_xyz"])),
             "map_leaves": int(M.num_leaves), "map_depth": int(M.info.depth), "iterations": int(wl["params"]["max_iterations"]),
@@ -529,9 +532,11 @@ def single_alignments(steps: int, peak: float, peak_source: str, cpu: bool = Tru
             "e2e": {"ms_per_alignment": ms_e2e, "alignments_per_s": 1e3 / ms_e2e,
                     "h2d_bytes": int(npts * 20), "note": "scan points and stamps from page-locked host memory"},
             "map_build_ms": map_ms, "map_build_point_levels_per_s": pl / (map_ms * 1e-3),
-            "map_build_roofline": {"achieved": 48.0 * pl / (map_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
-                                   "frac": 48.0 * pl / (map_ms * 1e-3) / 1e9 / peak, "peak_source": peak_source,
-                                   "model": "48 B per point per level"},
+            "map_levels_level_by_level": int(inf.global_levels),
+            "map_build_roofline": {"achieved": map_alg / (map_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                                   "frac": map_alg / (map_ms * 1e-3) / 1e9 / peak, "peak_source": peak_source,
+                                   "model": "48 B per point per level built level by level + 32 B per point "
+                                            "for the shared-memory subtree pass"},
             "roofline_linearize": {"achieved": lin_ach, "peak": peak, "unit": "GB/s",
                                    "frac": lin_ach / peak if lin_ach else None, "peak_source": peak_source,
                                    "mean_launch_ms": lin_ms, "launches": launches, "touched_fixed_nodes": int(touched),
@@ -841,15 +846,17 @@ def forest_pass(steps: int, scans: int = 5) -> dict:
             raise RuntimeError("kds_tree_build_batch: %d" % rc)
         if rep >= 3:
             times.append(e0.elapsed_time(e1))
-        depth = 0
+        depth = glob = 0
         for i in range(R):
             if out[i]:
-                depth = max(depth, kds.Tree(out[i]).info.depth)  # the Tree wrapper frees it
-        depth_pts = depth * int(off[-1])
+                inf = kds.Tree(out[i]).info  # the Tree wrapper frees it
+                depth, glob = max(depth, inf.depth), max(glob, inf.global_levels)
+        npts = int(off[-1])
     ms = float(np.median(times))
-    return {"clouds": R, "points": int(off[-1]), "ms_per_pass_median": ms, "ms_all": times,
-            "point_levels_per_s": depth_pts / (ms * 1e-3),
-            "alg_gbs_48B_per_point_level": 48.0 * depth_pts / (ms * 1e-3) / 1e9}
+    alg = 48.0 * glob * npts + (32.0 * npts if glob < depth else 0.0)
+    return {"clouds": R, "points": npts, "levels": depth, "levels_level_by_level": glob,
+            "ms_per_pass_median": ms, "ms_all": times, "point_levels_per_s": depth * npts / (ms * 1e-3),
+            "alg_bytes": alg, "alg_gbs": alg / (ms * 1e-3) / 1e9}
 
 
 def main():
@@ -995,19 +1002,26 @@ def main():
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = pst["alg_bytes"] / (pst["lin_ms"] * 1e-3) / 1e9 if pst["lin_ms"] > 0 else None
     # the dominant kernels of the step are the tree-build passes; the linearization launches second
-    build_alg = 48.0 * pst["build_point_levels"]
+    # per point and level built level by level: a 16 B point record read twice and written once
+    # (48 B); the shared-memory subtree pass that finishes the deep levels: 28 B of point record
+    # read once + 4 B of point order written (32 B per point)
+    deep = pst["build_global_point_levels"] < pst["build_point_levels"]
+    build_alg = 48.0 * pst["build_global_point_levels"] + (32.0 * pst["build_points"] if deep else 0.0)
     build_ach = build_alg / (pst["build_ms"] * 1e-3) / 1e9 if pst["build_ms"] > 0 else None
     roofline = {"bound": "hbm", "kernel": "tree-build passes (k_small_part, k_decide, k_big_*, level kernels): "
                                           "forest builds of request and map trees",
                 "achieved": build_ach, "peak": peak, "unit": "GB/s",
                 "frac": build_ach / peak if build_ach else None,
-                "traffic": BUILD_TRAFFIC_PER_POINT_LEVEL * pst["build_point_levels"],
-                "traffic_source": "per point-level DRAM bytes of an ncu capture of an 80-scan forest pass, "
-                                  "scaled by the step's points x levels",
+                "traffic": BUILD_TRAFFIC_PER_POINT * pst["build_points"] if BUILD_TRAFFIC_PER_POINT else None,
+                "traffic_source": "DRAM bytes per point of an ncu capture of an 80-scan forest pass (all its "
+                                  "kernels), scaled by the step's points",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "alg_bytes_per_step": build_alg, "build_ms_per_step": pst["build_ms"],
-                "model": "48 B per point per level (a 16 B point record read twice and written once); "
-                         "points x levels summed over the step's build passes / their wall time"}
+                "model": "48 B per point per level built level by level (a 16 B point record read twice and "
+                         "written once) + 32 B per point for the shared-memory subtree pass of the deep levels; "
+                         "summed over the step's build passes / their wall time",
+                "point_levels": pst["build_point_levels"],
+                "point_levels_level_by_level": pst["build_global_point_levels"]}
     ticks = max(1, pst["lin_ticks"])
     roofline_lin = {"bound": "hbm", "kernel": "k_linearize<0>/<1> (fused ICP / CT-ICP linearization + GN step)",
                     "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -89,6 +89,9 @@ typedef struct {
   double ts_start; /* Tree_::_ts_start */
   int32_t accepted;
   int32_t depth;
+  int32_t global_levels; /* levels the build ran level by level; the levels below, in subtrees of at
+                            most 1,024 points, were finished in shared memory (== depth if none) */
+  int32_t pad_;
 } kds_tree_info;
 
 /* Replaces TreeGenerator_::makeTree (kd/tree/tree_generator_impl_.h:7-19) and the
@@ -564,6 +567,8 @@ typedef struct {
   double build_ms;         /* wall time of the tree-build passes (requests and map rebuilds) */
   int64_t build_points;    /* points those passes built */
   double build_point_levels; /* sum over the passes of points x levels */
+  double build_global_point_levels; /* sum over the passes of points x levels built level by level
+                                       (the levels below ran in shared-memory subtrees) */
 } kds_server_stats;
 
 void kds_server_params_default(kds_server_params* p);

@@ -65,6 +65,8 @@ class TreeInfo(C.Structure):
         ("ts_start", C.c_double),
         ("accepted", C.c_int32),
         ("depth", C.c_int32),
+        ("global_levels", C.c_int32),
+        ("pad_", C.c_int32),
     ]
 
 
@@ -242,6 +244,7 @@ class ServerStats(C.Structure):
         ("build_ms", C.c_double),
         ("build_points", C.c_int64),
         ("build_point_levels", C.c_double),
+        ("build_global_point_levels", C.c_double),
     ]
 
     def as_dict(self) -> dict:

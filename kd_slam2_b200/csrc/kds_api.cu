@@ -230,6 +230,8 @@ int kds_tree_get_info(const kds_tree* t, kds_tree_info* info) {
   info->ts_start = t->d.ts_start;
   info->accepted = t->d.accepted;
   info->depth = t->d.depth;
+  info->global_levels = t->d.global_levels;
+  info->pad_ = 0;
   return KDS_OK;
 }
 

@@ -1842,6 +1842,7 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   // node-range kernels (k_decide, k_level_children, k_big_plan, k_level_advance) share
   // one block count per level; every kernel's result is independent of its grid.
   int64_t level_nodes = R;
+  int32_t global_levels = -1;  // levels built level by level; -1: no shared-memory pass
   hls.lb = 0;
   hls.le = R;
   hls.depth = 0;
@@ -1853,6 +1854,7 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
         k_root_moments<<<kGridBlocks, kThreads, 0, s>>>(w.nodes, R, w.B, w.ts0, w.mom);
         count_launch();
       }
+      global_levels = hls.depth;
       rc = deep_pass(w, P, hls, s);
       if (rc) return rc;
       KDS_CK(cudaMemcpyAsync(&hls, w.ls, sizeof(LevelState), cudaMemcpyDeviceToHost, s));
@@ -1955,6 +1957,7 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
     t->d.num_unpruned = tu[r];
     t->d.ts_start = ts0[r];
     t->d.depth = depth;
+    t->d.global_levels = global_levels >= 0 ? global_levels : depth;
     const double* f = &rf[(size_t)kRootFrame * r];
     for (int i = 0; i < 3; ++i) {
       t->root_eigenvalues[i] = (float)f[i];

@@ -46,6 +46,7 @@ struct TreeDev {
   double ts_start = 0.0;
   int32_t depth = 0;
   int32_t accepted = 1;
+  int32_t global_levels = 0;  // levels built level by level (the rest in shared-memory subtrees)
   DNode* nodes = nullptr;         // [num_nodes]
   float* dts_f = nullptr;         // [num_nodes] (float)dts_mean
   double* dts_mean = nullptr;     // [num_nodes]

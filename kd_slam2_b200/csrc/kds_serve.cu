@@ -264,6 +264,7 @@ struct kds_server {
   int tick_n[2] = {0, 0};
   int64_t build_points = 0;   // points built (requests and maps)
   double build_point_levels = 0.0;  // sum over passes of points x levels
+  double build_global_point_levels = 0.0;  // the same for the levels built level by level
 };
 
 namespace {
@@ -496,10 +497,14 @@ void build_loop(kds_server* s) {
       s->build_ms += 1e3 * seconds_since(pass_t0);
       s->build_points += N;
       {
-        int depth = 0;  // levels of the pass (the same for every tree it built)
+        int depth = 0, glob = 0;  // levels of the pass (the same for every tree it built)
         for (auto* t : trees)
-          if (t) depth = std::max(depth, (int)t->d.depth);
+          if (t) {
+            depth = std::max(depth, (int)t->d.depth);
+            glob = std::max(glob, (int)t->d.global_levels);
+          }
         s->build_point_levels += (double)N * depth;
+        s->build_global_point_levels += (double)N * glob;
       }
       {
         const double t1 = seconds_since(s->t0);
@@ -1223,6 +1228,7 @@ int kds_server_get_stats(kds_server* s, kds_server_stats* st) {
   st->build_ms = s->build_ms;
   st->build_points = s->build_points;
   st->build_point_levels = s->build_point_levels;
+  st->build_global_point_levels = s->build_global_point_levels;
   return KDS_OK;
 }
 

@@ -872,9 +872,26 @@ def main():
                     help="run only the tracker-step leg and print its JSON (for profiling it)")
     ap.add_argument("--forest-only", action="store_true",
                     help="run only the served step's build workload (one forest pass of 80 scans) and print its JSON")
+    ap.add_argument("--single-only", action="store_true",
+                    help="run only the single-alignment legs (16 x 1024 ICP, 64 x 1024 CT-ICP vs 1.2M surfels)")
     ap.add_argument("--large-maps", action="store_true",
                     help="add the served leg with 1.2M-surfel initial maps per stream (about a minute more)")
     args = ap.parse_args()
+    if args.single_only:
+        import torch
+
+        import kd_slam2_b200 as kds
+        torch.cuda.set_device(0)
+        kds.init(0)
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        print(json.dumps({"single_alignments": single_alignments(
+            args.steps, float(peaks.get("hbm_gbs", 6650.0)), "measured" if "hbm_gbs" in peaks else "fallback",
+            cpu=not args.no_cpu)}), flush=True)
+        return
     if args.forest_only:
         import torch
 

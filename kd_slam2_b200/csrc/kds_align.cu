@@ -1461,6 +1461,16 @@ double Runner::profile_mean_ms(int* launches) const {
   return n ? sum / n : 0.0;
 }
 
+// A profiling event on s: inside a stream capture it becomes an external event node of
+// the graph (recorded at every replay); outside one it is a plain record.
+static cudaError_t record_profile_event(cudaEvent_t e, cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaError_t r = cudaStreamIsCapturing(s, &cs);
+  if (r != cudaSuccess) return r;
+  return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal)
+                                             : cudaEventRecord(e, s);
+}
+
 // Blocks of the persistent kernel: every SM full at its occupancy for `smem` bytes of
 // dynamic shared memory, at most one block per work item.
 static int persistent_grid(size_t smem, int64_t items) {
@@ -1500,12 +1510,12 @@ int Runner::enqueue(cudaStream_t s, int32_t* dbg_match, int32_t* dbg_status) {
     }
     if (num_tiles > 0 && L > 0) {
       const int grid = persistent_grid(stage_bytes, (int64_t)num_tiles * L);
-      if (profiling) KDS_CK(cudaEventRecordWithFlags(prof_ev[0], s, cudaEventRecordExternal));
+      if (profiling) KDS_CK(record_profile_event(prof_ev[0], s));
       k_linearize_persistent<<<grid, kBlock, stage_bytes, s>>>(d_jobs, d_states, d_outs, d_logs, d_lins, d_tiles,
                                                                num_tiles, L, stage_nodes, d_partials, d_ready,
                                                                d_queue, d_err);
       ::kds::count_launch();
-      if (profiling) KDS_CK(cudaEventRecordWithFlags(prof_ev[1], s, cudaEventRecordExternal));
+      if (profiling) KDS_CK(record_profile_event(prof_ev[1], s));
     }
     KDS_CK(cudaGetLastError());
     return KDS_OK;
@@ -1532,7 +1542,7 @@ int Runner::enqueue(cudaStream_t s, int32_t* dbg_match, int32_t* dbg_status) {
   for (int i = 0; i < L; ++i) {
     for (int kind = 0; kind < 3; ++kind) {
       if (!kind_count[kind]) continue;
-      if (profiling) KDS_CK(cudaEventRecordWithFlags(prof_ev[ev++], s, cudaEventRecordExternal));
+      if (profiling) KDS_CK(record_profile_event(prof_ev[ev++], s));
       if (pair_tiles) {
         const int nb = kind_pair_count[kind], p0 = kind_pair_begin[kind];
         if (kind == 0)
@@ -1560,7 +1570,7 @@ int Runner::enqueue(cudaStream_t s, int32_t* dbg_match, int32_t* dbg_status) {
                                                                      d_tiles, kind_begin[2], stage, d_partials,
                                                                      dbg_match, dbg_status, d_err);
       ::kds::count_launch();
-      if (profiling) KDS_CK(cudaEventRecordWithFlags(prof_ev[ev++], s, cudaEventRecordExternal));
+      if (profiling) KDS_CK(record_profile_event(prof_ev[ev++], s));
     }
   }
   KDS_CK(cudaGetLastError());

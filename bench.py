@@ -565,6 +565,86 @@ def single_alignments(steps: int, peak: float, peak_source: str, cpu: bool = Tru
     return out
 
 
+def _precision_worker(args):
+    """One perturbation of the precision leg on the oracle: the product-semantics run (recorded),
+    its FP64 replay and the free FP64 run (spawned process)."""
+    path, X0, v0, params = args
+    import sys
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    from oracle import orc
+    g = globals()
+    if g.get("_prec_path") != path:
+        d = np.load(path)
+        g["_prec_M"] = orc.OTree.from_nodes(d["mean"], d["dir"], d["dts_mean"], d["left"], d["right"])
+        g["_prec_T"] = orc.OTree.build(d["xyz"], d["st"], orc.tree_params(**TREE))
+        g["_prec_path"] = path
+    P = orc.align_params(**params)
+    M, T = g["_prec_M"], g["_prec_T"]
+    rec = orc.align_recorded(orc.KIND_CT, M, T, P, X0, v0=v0)
+    Xr, _ = orc.align_replay64(orc.KIND_CT, M, T, P, X0, rec["match"], rec["status"], v0=v0)
+    r64 = orc.align(orc.KIND_CT, orc.MODE_FP64, M, T, P, X0, v0=v0)
+    return rec["X"], Xr, r64["X"]
+
+
+def precision_leg(steps: int, perturbations: int = 16) -> dict:
+    """The precision configuration on a sample: the 128 x 2048 scan against the 4.2M-surfel map,
+    seeded perturbations of 0-0.5 m / 0-5 deg aligned in one batch (CUDA events around the
+    batch, device-resident trees), each pose against the oracle: bit-identity with the
+    product-semantics run, the arithmetic error against the FP64 replay of the same
+    correspondences, and the distance to the free all-FP64 run (branch divergence included)."""
+    import multiprocessing as mp
+    import tempfile
+
+    import torch
+
+    import kd_slam2_b200 as kds
+    from kd_slam2_b200 import scans
+    from kd_slam2_b200.abi import KDS_CTICP
+    wl = scans.ct_128x2048_4m_map(perturbations=perturbations)
+    gen = kds.TreeGeneratorB2003D(**wl["tree"])
+    M = gen.make_tree(torch.from_numpy(wl["map_xyz"]).cuda(), device=True)
+    T = gen.make_tree(wl["xyz"], wl["st"])
+    params = kds.aligner_params(**wl["params"])
+    jobs = [kds.make_job(KDS_CTICP, M, T, params, X=X0, v=wl["v0"]) for X0 in wl["X0s"]]
+    b = kds.Batch()
+    b.run(jobs)
+    b.run(jobs)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times = []
+    for _ in range(max(1, steps)):
+        torch.cuda.synchronize()
+        e0.record()
+        res = b.run(jobs)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    me = M.export()
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "prec.npz")
+        np.savez(path, mean=me["mean"], dir=me["dir"], dts_mean=me["dts_mean"], left=me["left"], right=me["right"],
+                 xyz=wl["xyz"], st=wl["st"])
+        with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+            ref = pool.map(_precision_worker, [(path, X0, wl["v0"], wl["params"]) for X0 in wl["X0s"]], chunksize=1)
+    same, arith, fp64 = 0, [], []
+    for j, (Xm, Xr, X64) in zip(res, ref):
+        X = np.array(j.X[:]).reshape(3, 4)
+        same += int(np.array_equal(X, Xm))
+        arith.append(max(pose_err(X, Xr)))
+        fp64.append(max(pose_err(X, X64)))
+    arith, fp64 = np.array(arith), np.array(fp64)
+    ms = float(np.median(times))
+    return {"scan_points": int(len(wl["xyz"])), "scan_leaves": int(T.num_leaves), "map_points": int(len(wl["map_xyz"])),
+            "map_leaves": int(M.num_leaves), "perturbations": len(jobs), "batch_ms": ms,
+            "alignments_per_s": len(jobs) / (ms / 1e3),
+            "bit_identical_to_product_semantics_oracle": same,
+            "arithmetic_error_vs_fp64_replay": {"max": float(arith.max()), "median": float(np.median(arith)),
+                                                "within_1e-5": int(np.sum(arith <= 1e-5))},
+            "vs_free_fp64": {"max": float(fp64.max()), "median": float(np.median(fp64)),
+                             "within_1e-5": int(np.sum(fp64 <= 1e-5))},
+            "note": "errors are max(translation m, rotation rad) per perturbation"}
+
+
 def scan_input(steps: int):
     """The scan input stage and the tree wire format on full-size sweeps: toPointsVector +
     Voxelizer_::voxelize on the device (kds_points_voxelize, device-resident inputs) over
@@ -1103,6 +1183,7 @@ def main():
         line["single_alignments"] = single_alignments(args.steps, peak, roofline["peak_source"],
                                                       cpu=world == 1 and not args.no_cpu)
         line["batched_ba"] = batched_ba(args.steps)
+        line["precision"] = precision_leg(args.steps) if world == 1 and not args.no_cpu else None
         if args.large_maps:
             line["served_large_maps"] = served_large_maps(args.steps)
         line["scan_input"] = scan_input(args.steps)

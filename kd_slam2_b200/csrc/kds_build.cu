@@ -1138,21 +1138,24 @@ __global__ void k_level_advance(LevelState* ls, const int32_t* bsum, int nblocks
 
 // ---- deep levels: whole subtrees in shared memory --------------------------------------
 // Once every node of a level has at most kDeepMax points, each of them is the root of a
-// subtree that one block builds to the end in shared memory: the points are loaded once,
-// and every depth below runs the same steps as the level kernels -- decide (thread per
-// node, from the node's exact sums), children numbered by a block scan, stable ballot
-// partition by whichSide (warp per node) with the smaller child summed on the way (the
-// other = parent - smaller).  The arithmetic and the partition order are those of
-// k_decide / k_small_part, so the nodes are bit-identical to a level-by-level build.
-// Nodes below the roots are written as DeepNode records tagged (subtree, depth, rank);
-// k_deep_place then puts them at their breadth-first positions: depth by depth, subtree
-// by subtree in the roots' order, by rank inside a subtree -- the order in which the
-// level kernels would have numbered them.
-constexpr int kDeepMax = 1024;     // largest subtree root
-constexpr int kDeepThreads = 256;
-constexpr int kDeepWarps = kDeepThreads / 32;
-constexpr int kDeepBlocksPerSM = 2;
+// subtree that one warp builds to the end in its own slice of shared memory: the points
+// are loaded once, and every depth below runs the same steps as the level kernels --
+// decide (lane per node, from the node's exact sums), children numbered by a warp scan,
+// stable ballot partition by whichSide (the warp per node) with the smaller child summed
+// on the way (the other = parent - smaller).  The arithmetic and the partition order are
+// those of k_decide / k_small_part, so the nodes are bit-identical to a level-by-level
+// build.  The warps of a block share nothing and never wait for each other.  Nodes below
+// the roots are written as DeepNode records tagged (subtree, depth, rank); k_deep_place
+// then puts them at their breadth-first positions: depth by depth, subtree by subtree in
+// the roots' order, by rank inside a subtree -- the order in which the level kernels
+// would have numbered them.
+constexpr int kDeepMax = 256;      // largest subtree root (points)
+constexpr int kDeepNodes = 192;    // nodes of one depth: at most 2 x (kDeepMax / 3) split children
+constexpr int kDeepWarpsPerBlock = 4;
+constexpr int kDeepThreads = 32 * kDeepWarpsPerBlock;
+constexpr int kDeepBlocksPerSM = 4;
 static_assert(kDeepMax <= kBig, "deep subtree roots are summed by k_root_moments");
+static_assert(2 * (kDeepMax / 3) <= kDeepNodes, "node capacity of one depth");
 
 struct DeepNode {
   float mean[3], dir[3];
@@ -1169,16 +1172,12 @@ struct DeepNode {
 static_assert(sizeof(DeepNode) == 96, "DeepNode layout");
 static_assert(sizeof(DeepNode) <= 11 * sizeof(U128), "a DeepNode fits the sums slot of one node");
 
-struct DeepSmem {
-  float4 pts[2][kDeepMax];      // w = the point's index in load order (as int bits)
-  double st[kDeepMax];          // stamps, load order
-  int32_t gid[kDeepMax];        // global point ids, load order
-  uint32_t range[2][kDeepMax];  // node start | end << 16 (subtree offsets), by depth parity
-  int32_t prank[2][kDeepMax];   // parent's rank, by depth parity
-  int32_t list[kDeepMax];       // q -> rank of the q-th split node of the depth
-  uint8_t split[kDeepMax];
-  int sm[32];
-  int base, nsplit, base_prev;
+struct DeepWarpSmem {                // one warp's slice
+  float4 pts[2][kDeepMax];           // w = the point's offset in the subtree's input order (int bits)
+  uint32_t range[2][kDeepNodes];     // node start | end << 16 (subtree offsets), by depth parity
+  int32_t prank[2][kDeepNodes];      // parent's rank, by depth parity
+  int32_t list[kDeepNodes];          // q -> rank of the q-th split node of the depth
+  uint8_t split[kDeepNodes];
 };
 
 __global__ void __launch_bounds__(kDeepThreads, kDeepBlocksPerSM)
@@ -1186,51 +1185,47 @@ __global__ void __launch_bounds__(kDeepThreads, kDeepBlocksPerSM)
                  double* root_frame, DeepNode* dn, int32_t dn_cap, int32_t* dn_count, U128* ring, int32_t* counts,
                  int32_t dcap) {
   extern __shared__ __align__(16) unsigned char deep_smem_raw[];
-  DeepSmem& S = *reinterpret_cast<DeepSmem*>(deep_smem_raw);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  DeepWarpSmem& S = reinterpret_cast<DeepWarpSmem*>(deep_smem_raw)[wib];
   const int lb = ls->lb, le = ls->le, cur0 = ls->cur;
   const int nroots = le - lb;
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const unsigned lt = (1u << lane) - 1u;
-  U128* myring = ring + (size_t)blockIdx.x * 2 * kDeepMax * 11;
-  for (int sub = blockIdx.x; sub < nroots; sub += gridDim.x) {
+  const unsigned full = 0xffffffffu, lt = (1u << lane) - 1u;
+  const int gw = blockIdx.x * kDeepWarpsPerBlock + wib, nw = gridDim.x * kDeepWarpsPerBlock;
+  U128* myring = ring + (size_t)gw * 2 * kDeepNodes * 11;
+  const float4* pin = B.p[cur0];
+  const double* sin_ = B.s[cur0];
+  const int32_t* iin = B.id[cur0];
+  for (int sub = gw; sub < nroots; sub += nw) {
     const int R = lb + sub;
-    BNode root = nodes[R];
+    const BNode root = nodes[R];
     const int n = root.end - root.start;
     const int pbase = root.start;
     const double t0 = ts0[root.tree];
-    {
-      const float4* pin = B.p[cur0];
-      const double* sin_ = B.s[cur0];
-      const int32_t* iin = B.id[cur0];
-      for (int i = tid; i < n; i += kDeepThreads) {
-        float4 p = pin[pbase + i];
-        p.w = __int_as_float(i);
-        S.pts[0][i] = p;
-        S.st[i] = sin_[pbase + i];
-        S.gid[i] = iin[pbase + i];
-      }
+    for (int i = lane; i < n; i += 32) {
+      float4 p = pin[pbase + i];
+      p.w = __int_as_float(i);
+      S.pts[0][i] = p;
     }
-    if (tid == 0) {
+    if (lane == 0) {
       S.range[0][0] = (uint32_t)n << 16;
       S.prank[0][0] = -1;
-      S.base = 0;
-      S.base_prev = 0;
     }
-    __syncthreads();
-    int cnt = 1, c = 0;
+    __syncwarp();
+    int cnt = 1, c = 0, base = 0, base_prev = 0;
     for (int d = 0; cnt > 0; ++d, c ^= 1) {
-      // ---- decide: thread per node of this depth; record slots for the depth's nodes
-      if (d > 0 && tid == 0) {
-        S.base_prev = S.base;
-        const int b = atomicAdd(dn_count, cnt);
-        S.base = b;
-        if (b + cnt > dn_cap) ls->error = 1;
+      // ---- decide: lane per node of this depth; record slots for the depth's nodes
+      if (d > 0) {
+        base_prev = base;
+        int b = 0;
+        if (lane == 0) b = atomicAdd(dn_count, cnt);
+        base = __shfl_sync(full, b, 0);
+        if (base + cnt > dn_cap) {
+          if (lane == 0) ls->error = 1;  // out of record slots: the build reports KDS_ERR_CAPACITY
+          break;
+        }
       }
-      __syncthreads();
-      const int base = S.base, base_prev = S.base_prev;
-      const bool room = d == 0 || base + cnt <= dn_cap;  // depth 0 writes no record
-      const U128* psums = d == 0 ? mom + (size_t)R * 11 : myring + (size_t)(d & 1) * kDeepMax * 11;
-      for (int r = tid; r < cnt && room; r += kDeepThreads) {
+      const U128* psums = d == 0 ? mom + (size_t)R * 11 : myring + (size_t)(d & 1) * kDeepNodes * 11;
+      for (int r = lane; r < cnt; r += 32) {
         const uint32_t rg = S.range[c][r];
         const int st = (int)(rg & 0xffffu), en = (int)(rg >> 16);
         BNode nd;
@@ -1241,12 +1236,11 @@ __global__ void __launch_bounds__(kDeepThreads, kDeepBlocksPerSM)
           nd.level = root.level + d;
           nd.tree = root.tree;
           nd.has_parent = 1;
-          const int pr = S.prank[c][r];
           if (d == 1) {  // the root's decision, written at depth 0
             for (int k = 0; k < 3; ++k) nd.par_prop[k] = nodes[R].prop[k];
             nd.par_has = nodes[R].has_prop;
           } else {
-            const DeepNode& pn = dn[base_prev + pr];
+            const DeepNode& pn = dn[base_prev + S.prank[c][r]];
             nd.par_has = pn.has_prop;
             for (int k = 0; k < 3; ++k) nd.par_prop[k] = pn.prop[k];
           }
@@ -1278,40 +1272,38 @@ __global__ void __launch_bounds__(kDeepThreads, kDeepBlocksPerSM)
           dn[base + r] = x;
         }
       }
-      __syncthreads();
-      if (!room) break;  // out of record slots: the build reports KDS_ERR_CAPACITY
-      // ---- children numbering: split ranks by a block scan in rank order
-      {
-        int carry = 0;
-        for (int r0 = 0; r0 < cnt; r0 += kDeepThreads) {
-          const int r = r0 + tid;
-          const int f = (r < cnt && S.split[r]) ? 1 : 0;
-          int tot;
-          const int q = block_scan(f, S.sm, &tot) + carry;
-          if (f) {
-            S.list[q] = r;
-            if (d > 0) dn[base + r].q = q;
-          }
-          carry += tot;
+      __syncwarp();
+      // ---- children numbering: split ranks by a warp scan in rank order
+      int nsplit = 0;
+      for (int r0 = 0; r0 < cnt; r0 += 32) {
+        const int r = r0 + lane;
+        const bool f = r < cnt && S.split[r];
+        const unsigned bf = __ballot_sync(full, f);
+        if (f) {
+          const int q = nsplit + __popc(bf & lt);
+          S.list[q] = r;
+          if (d > 0) dn[base + r].q = q;
         }
-        if (tid == 0) {
-          S.nsplit = carry;
-          if (carry > 0) {
-            if (d + 1 < dcap) counts[(size_t)(d + 1) * nroots + sub] = 2 * carry;
-            else ls->error = 1;
-          }
-        }
+        nsplit += __popc(bf);
       }
-      __syncthreads();
-      const int nsplit = S.nsplit;
-      // ---- the leaves' point order, then the partition of the split nodes (warp per node)
-      for (int r = w; r < cnt; r += kDeepWarps) {
+      if (2 * nsplit > kDeepNodes) {  // cannot happen (split nodes hold >= 3 points); refuse rather than overrun
+        if (lane == 0) ls->error = 1;
+        break;
+      }
+      if (nsplit > 0 && lane == 0) {
+        if (d + 1 < dcap) counts[(size_t)(d + 1) * nroots + sub] = 2 * nsplit;
+        else ls->error = 1;
+      }
+      __syncwarp();
+      // ---- the leaves' point order (lane per leaf)
+      for (int r = lane; r < cnt; r += 32) {
         if (S.split[r]) continue;
         const uint32_t rg = S.range[c][r];
         const int st = (int)(rg & 0xffffu), en = (int)(rg >> 16);
-        for (int i = st + lane; i < en; i += 32) B.perm[pbase + i] = S.gid[__float_as_int(S.pts[c][i].w)];
+        for (int i = st; i < en; ++i) B.perm[pbase + i] = iin[pbase + __float_as_int(S.pts[c][i].w)];
       }
-      for (int q = w; q < nsplit; q += kDeepWarps) {
+      // ---- partition of the split nodes, the warp per node
+      for (int q = 0; q < nsplit; ++q) {
         const int r = S.list[q];
         const uint32_t rg = S.range[c][r];
         const int st = (int)(rg & 0xffffu), en = (int)(rg >> 16);
@@ -1326,7 +1318,7 @@ __global__ void __launch_bounds__(kDeepThreads, kDeepBlocksPerSM)
         for (int k0 = st; k0 < en; k0 += 32) {
           const int i = k0 + lane;
           const bool left = i < en && which_side_f(mean, dir, S.pts[c][i]);
-          nl += __popc(__ballot_sync(0xffffffffu, left));
+          nl += __popc(__ballot_sync(full, left));
         }
         const int mid = st + nl;
         const bool small_left = mid - st <= en - mid;
@@ -1339,12 +1331,12 @@ __global__ void __launch_bounds__(kDeepThreads, kDeepBlocksPerSM)
           float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
           if (valid) p = S.pts[c][i];
           const bool left = valid && which_side_f(mean, dir, p);
-          const unsigned bl = __ballot_sync(0xffffffffu, left);
-          const unsigned br = __ballot_sync(0xffffffffu, valid && !left);
+          const unsigned bl = __ballot_sync(full, left);
+          const unsigned br = __ballot_sync(full, valid && !left);
           if (valid) {
             const int dst = left ? (st + cl + __popc(bl & lt)) : (mid + cr + __popc(br & lt));
             S.pts[c ^ 1][dst] = p;
-            if (left == small_left) moments_add_point(MS, p, S.st[__float_as_int(p.w)], t0);
+            if (left == small_left) moments_add_point(MS, p, sin_[pbase + __float_as_int(p.w)], t0);
           }
           cl += __popc(bl);
           cr += __popc(br);
@@ -1354,7 +1346,7 @@ __global__ void __launch_bounds__(kDeepThreads, kDeepBlocksPerSM)
           const int k = lane >> 1;
           const U128 ps = d == 0 ? psums[k] : psums[(size_t)r * 11 + k];
           const U128 other = u128_sub(ps, qs);
-          U128* nxt = myring + (size_t)((d + 1) & 1) * kDeepMax * 11;
+          U128* nxt = myring + (size_t)((d + 1) & 1) * kDeepNodes * 11;
           nxt[(size_t)(2 * q) * 11 + k] = small_left ? qs : other;
           nxt[(size_t)(2 * q + 1) * 11 + k] = small_left ? other : qs;
         }
@@ -1367,9 +1359,9 @@ __global__ void __launch_bounds__(kDeepThreads, kDeepBlocksPerSM)
       }
       cnt = 2 * nsplit;
       if (d + 1 >= dcap) cnt = 0;
-      __syncthreads();
+      __syncwarp();
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
@@ -1714,11 +1706,13 @@ int deep_pass(BuildWs& w, const BuildParams& P, const LevelState& h, cudaStream_
   DeepNode* dn = reinterpret_cast<DeepNode*>(w.mom + (size_t)le * 11);
   const int64_t dn_cap64 = ((w.cap_nodes - le) * (int64_t)(11 * sizeof(U128))) / (int64_t)sizeof(DeepNode);
   const int32_t dn_cap = (int32_t)std::min<int64_t>(dn_cap64, INT32_MAX);
-  const int grid = std::min(nroots, 148 * kDeepBlocksPerSM);
+  const int grid = (int)std::min<int64_t>((nroots + kDeepWarpsPerBlock - 1) / kDeepWarpsPerBlock,
+                                          148 * kDeepBlocksPerSM);
+  const int64_t nwarps = (int64_t)grid * kDeepWarpsPerBlock;
   const int64_t ncount = (int64_t)dcap * nroots;
   if (ncount > INT32_MAX / 2) { set_error("kds_tree_build: too many deep subtrees"); return KDS_ERR_CAPACITY; }
   const size_t bc = carve_size<int32_t>(ncount), bt = carve_size<int32_t>(ncount / 4096 + 2),
-               br = carve_size<U128>((size_t)grid * 2 * kDeepMax * 11);
+               br = carve_size<U128>((size_t)nwarps * 2 * kDeepNodes * 11);
   void* blk = nullptr;
   cudaError_t e = cudaMallocAsync(&blk, 2 * bc + bt + 3 * 256 + br, s);
   if (e != cudaSuccess) {
@@ -1733,18 +1727,18 @@ int deep_pass(BuildWs& w, const BuildParams& P, const LevelState& h, cudaStream_
   int32_t* total = carve<int32_t>(p, 1);
   int32_t* dn_count = carve<int32_t>(p, 1);
   carve<int32_t>(p, 1);
-  U128* ring = carve<U128>(p, (size_t)grid * 2 * kDeepMax * 11);
+  U128* ring = carve<U128>(p, (size_t)nwarps * 2 * kDeepNodes * 11);
   int rc = KDS_OK;
   static bool attr_set = false;  // the attribute is a property of the kernel, per process
   if (!attr_set) {
     e = cudaFuncSetAttribute((const void*)k_deep_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(DeepSmem));
+                             (int)(sizeof(DeepWarpSmem) * kDeepWarpsPerBlock));
     if (e == cudaSuccess) attr_set = true;
   }
   if (e == cudaSuccess) e = cudaMemsetAsync(counts, 0, sizeof(int32_t) * ncount, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(dn_count, 0, sizeof(int32_t), s);
   if (e == cudaSuccess) {
-    k_deep_build<<<grid, kDeepThreads, sizeof(DeepSmem), s>>>(w.nodes, w.ls, w.B, w.ts0, w.mom, P, w.root_frame, dn,
+    k_deep_build<<<grid, kDeepThreads, sizeof(DeepWarpSmem) * kDeepWarpsPerBlock, s>>>(w.nodes, w.ls, w.B, w.ts0, w.mom, P, w.root_frame, dn,
                                                               dn_cap, dn_count, ring, counts, dcap);
     count_launch();
     rc = scan_exclusive(counts, off, (int32_t)ncount, tiles, total, s);

@@ -1150,6 +1150,12 @@ __global__ void k_level_advance(LevelState* ls, const int32_t* bsum, int nblocks
 // the roots' order, by rank inside a subtree -- the order in which the level kernels
 // would have numbered them.
 constexpr int kDeepMax = 256;      // largest subtree root (points)
+// The subtree pass runs only while the level has at most this many nodes: it finishes a
+// few thousand subtrees in about one subtree's latency, which beats the level kernels'
+// launches for single trees and small batches; for large forests (hundreds of thousands
+// of tiny subtrees, where a warp's decide runs on a few lanes) the level kernels, with a
+// thread per node of the whole level, are faster.
+constexpr int kDeepMaxRoots = 8192;
 constexpr int kDeepNodes = 192;    // nodes of one depth: at most 2 x (kDeepMax / 3) split children
 constexpr int kDeepWarpsPerBlock = 4;
 constexpr int kDeepThreads = 32 * kDeepWarpsPerBlock;
@@ -1841,7 +1847,7 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   hls.le = R;
   hls.depth = 0;
   for (int round = 0; round < kMaxDepth; ++round) {
-    if (host_max <= kDeepMax) {
+    if (host_max <= kDeepMax && level_nodes <= kDeepMaxRoots) {
       // every node of the current level fits one block: the rest of every subtree is
       // built in shared memory, then the host reads the final level state
       if (round == 0) {  // the roots' sums (every root has at most kBig points)
@@ -1857,8 +1863,9 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
       if (hls.error == 1) { set_error("kds_tree_build: node capacity exceeded"); return KDS_ERR_CAPACITY; }
       break;
     }
-    // sync after every level once the largest node is within a few halvings of kDeepMax
-    const int nlev = host_max > 4 * kDeepMax ? kLevelsPerSync : 1;
+    // sync after every level once the subtree pass is within reach: the largest node within
+    // a few halvings of kDeepMax and the level small enough (nodes at most double per level)
+    const int nlev = (host_max <= 4 * kDeepMax && level_nodes * 4 <= kDeepMaxRoots) ? 1 : kLevelsPerSync;
     for (int k = 0; k < nlev; ++k) {
       const bool level0 = round == 0 && k == 0;
       const int64_t nodes_bound = level_nodes << k;

@@ -479,16 +479,14 @@ __device__ __forceinline__ void level_range(const LevelState* ls, int& b, int& e
 // ---------------------------------------------------------------------------
 // Kernels
 
-__global__ void k_ingest(const float* xyz, const double* st, int64_t n, float4* pts, double* sts, int32_t* ids,
-                         LevelState* ls) {
+__global__ void k_ingest(const float* xyz, const double* st, int64_t n, float4* pts, double* sts, LevelState* ls) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
     double s = st ? st[i] : 0.0;
     bool ok = fabsf(x) < 32768.f && fabsf(y) < 32768.f && fabsf(z) < 32768.f && isfinite(s);
     if (!ok) ls->error = 2;
-    pts[i] = make_float4(x, y, z, 0.f);
+    pts[i] = make_float4(x, y, z, __int_as_float((int32_t)i));
     sts[i] = s;
-    ids[i] = (int32_t)i;
   }
 }
 
@@ -547,10 +545,12 @@ __global__ void k_init_roots(BNode* nodes, const int64_t* off, int R, LevelState
   }
 }
 
+// A point moves through the levels as one 16 B record (x, y, z, w = its input index as int
+// bits), double-buffered by level parity; its stamp stays in input order and is read by
+// index where a sum needs it.
 struct PointBufs {
   float4* p[2];
-  double* s[2];
-  int32_t* id[2];
+  double* st;     // stamps, input order
   int32_t* perm;  // final point order (global indices)
 };
 
@@ -591,7 +591,12 @@ __device__ __forceinline__ U128 warp_moments(const float4* p, const double* st, 
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int i = k0 + u * 32 + lane;
-      if (i < e) { pv[u] = p[i]; sv[u] = st[i]; }
+      if (i < e) pv[u] = p[i];
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = k0 + u * 32 + lane;
+      if (i < e) sv[u] = st[__float_as_int(pv[u].w)];
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -610,7 +615,7 @@ __global__ void __launch_bounds__(kThreads) k_root_moments(const BNode* nodes, i
   for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < R; r += nw) {
     const int s = nodes[r].start, e = nodes[r].end;
     if (e - s > kBig) continue;
-    const U128 q = warp_moments(B.p[0], B.s[0], s, e, ts0[nodes[r].tree], lane);
+    const U128 q = warp_moments(B.p[0], B.st, s, e, ts0[nodes[r].tree], lane);
     if (!(lane & 1) && lane < 22) mom[(size_t)r * 11 + (lane >> 1)] = q;
   }
 }
@@ -664,11 +669,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelS
                                                          const double* ts0, U128* mom) {
   const int lb = ls->lb, le = ls->le, cur = ls->cur;
   const float4* pin = B.p[cur];
-  const double* sin_ = B.s[cur];
-  const int32_t* iin = B.id[cur];
+  const double* sts = B.st;
   float4* pout = B.p[cur ^ 1];
-  double* sout = B.s[cur ^ 1];
-  int32_t* iout = B.id[cur ^ 1];
   const int lane = threadIdx.x & 31;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int wslot = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // consecutive nodes on different SMs
@@ -697,7 +699,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelS
     fetch(ni + nwarps);  // the next node's record and sums are in flight meanwhile
     if (e - s > kBig) continue;
     if (!split) {
-      for (int i = s + lane; i < e; i += 32) B.perm[i] = iin[i];
+      for (int i = s + lane; i < e; i += 32) B.perm[i] = __float_as_int(pin[i].w);
       if (lane == 0) nodes[ni].mid = e;
       continue;
     }
@@ -705,16 +707,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelS
     const bool one = K <= kUnroll;  // the whole node fits one round of loads: keep it
     unsigned bits = 0u;
     float4 pv[kUnroll];
-    double sv[kUnroll];
-    int iv[kUnroll];
     for (int k0 = 0; k0 < K; k0 += kUnroll) {
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) {
         int i = s + ((k0 + u) << 5) + lane;
-        if (i < e) {
-          pv[u] = pin[i];
-          if (one) { sv[u] = sin_[i]; iv[u] = iin[i]; }
-        }
+        if (i < e) pv[u] = pin[i];
       }
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) {
@@ -736,11 +733,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelS
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) {
         int i = s + ((k0 + u) << 5) + lane;
-        if (i < e && !one) {
-          pv[u] = pin[i];
-          sv[u] = sin_[i];
-          iv[u] = iin[i];
-        }
+        if (i < e && !one) pv[u] = pin[i];
       }
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) {
@@ -752,9 +745,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelS
         if (valid) {
           int dst = left ? (s + cl + __popc(bl & lt)) : (s + nl + cr + __popc(br & lt));
           pout[dst] = pv[u];
-          sout[dst] = sv[u];
-          iout[dst] = iv[u];
-          if (left == small_left) moments_add_point(MS, pv[u], sv[u], t0);
+          if (left == small_left) moments_add_point(MS, pv[u], sts[__float_as_int(pv[u].w)], t0);
         }
         cl += __popc(bl);
         cr += __popc(br);
@@ -897,13 +888,16 @@ __global__ void __launch_bounds__(kThreads) k_big_moments(const Chunk* chunks, c
   __shared__ U128 sm[kThreads / 32][11];
   const int nc = ls->num_chunks, cur = ls->cur;
   const float4* pts = B.p[cur];
-  const double* st = B.s[cur];
+  const double* st = B.st;
   for (int ci = blockIdx.x; ci < nc; ci += gridDim.x) {
     Chunk c = chunks[ci];
     double t0 = ts0[nodes[c.node].tree];
     Moments M;
     for (int k = 0; k < 11; ++k) M.s[k] = u128_zero();
-    for (int i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) moments_add_point(M, pts[i], st[i], t0);
+    for (int i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) {
+      const float4 pp = pts[i];
+      moments_add_point(M, pp, st[__float_as_int(pp.w)], t0);
+    }
     block_add_moments(M, sm, acc + (size_t)c.big * 11);
   }
 }
@@ -982,11 +976,8 @@ __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, c
   __shared__ int swl[2][kWarpsB];  // left counts of the chunk's warps, by chunk parity
   const int nc = ls->num_chunks, cur = ls->cur;
   const float4* pin = B.p[cur];
-  const double* sin_ = B.s[cur];
-  const int32_t* iin = B.id[cur];
+  const double* sts = B.st;
   float4* pout = B.p[cur ^ 1];
-  double* sout = B.s[cur ^ 1];
-  int32_t* iout = B.id[cur ^ 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   int par = 0;
@@ -994,21 +985,19 @@ __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, c
     const Chunk c = chunks[ci];
     const BNode& nd = nodes[c.node];
     if (!nd.split) {
-      for (int i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) B.perm[i] = iin[i];
+      for (int i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) B.perm[i] = __float_as_int(pin[i].w);
       continue;  // uniform per block
     }
     const float mean[3] = {nd.mean[0], nd.mean[1], nd.mean[2]};
     const float dir[3] = {nd.dir[0], nd.dir[1], nd.dir[2]};
     const int wb = c.begin + w * 32 * kPer;  // this warp's first point
     float4 pv[kPer];
-    double sv[kPer];
-    int iv[kPer];
     unsigned bl[kPer], bv[kPer];
     int nl = 0;
 #pragma unroll
     for (int u = 0; u < kPer; ++u) {
       const int i = wb + u * 32 + lane;
-      if (i < c.end) { pv[u] = pin[i]; sv[u] = sin_[i]; iv[u] = iin[i]; }
+      if (i < c.end) pv[u] = pin[i];
     }
 #pragma unroll
     for (int u = 0; u < kPer; ++u) {
@@ -1036,9 +1025,7 @@ __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, c
         const bool left = (bl[u] >> lane) & 1u;
         const int dst = left ? lo + __popc(bl[u] & lt) : ro + __popc(br & lt);
         pout[dst] = pv[u];
-        sout[dst] = sv[u];
-        iout[dst] = iv[u];
-        if (left == small_left) moments_add_point(M, pv[u], sv[u], t0);
+        if (left == small_left) moments_add_point(M, pv[u], sts[__float_as_int(pv[u].w)], t0);
       }
       lo += __popc(bl[u]);
       ro += __popc(br);
@@ -1179,7 +1166,7 @@ static_assert(sizeof(DeepNode) == 96, "DeepNode layout");
 static_assert(sizeof(DeepNode) <= 11 * sizeof(U128), "a DeepNode fits the sums slot of one node");
 
 struct DeepWarpSmem {                // one warp's slice
-  float4 pts[2][kDeepMax];           // w = the point's offset in the subtree's input order (int bits)
+  float4 pts[2][kDeepMax];           // the 16 B point records (w = input index)
   uint32_t range[2][kDeepNodes];     // node start | end << 16 (subtree offsets), by depth parity
   int32_t prank[2][kDeepNodes];      // parent's rank, by depth parity
   int32_t list[kDeepNodes];          // q -> rank of the q-th split node of the depth
@@ -1199,19 +1186,14 @@ __global__ void __launch_bounds__(kDeepThreads, kDeepBlocksPerSM)
   const int gw = blockIdx.x * kDeepWarpsPerBlock + wib, nw = gridDim.x * kDeepWarpsPerBlock;
   U128* myring = ring + (size_t)gw * 2 * kDeepNodes * 11;
   const float4* pin = B.p[cur0];
-  const double* sin_ = B.s[cur0];
-  const int32_t* iin = B.id[cur0];
+  const double* sts = B.st;
   for (int sub = gw; sub < nroots; sub += nw) {
     const int R = lb + sub;
     const BNode root = nodes[R];
     const int n = root.end - root.start;
     const int pbase = root.start;
     const double t0 = ts0[root.tree];
-    for (int i = lane; i < n; i += 32) {
-      float4 p = pin[pbase + i];
-      p.w = __int_as_float(i);
-      S.pts[0][i] = p;
-    }
+    for (int i = lane; i < n; i += 32) S.pts[0][i] = pin[pbase + i];
     if (lane == 0) {
       S.range[0][0] = (uint32_t)n << 16;
       S.prank[0][0] = -1;
@@ -1306,7 +1288,7 @@ __global__ void __launch_bounds__(kDeepThreads, kDeepBlocksPerSM)
         if (S.split[r]) continue;
         const uint32_t rg = S.range[c][r];
         const int st = (int)(rg & 0xffffu), en = (int)(rg >> 16);
-        for (int i = st; i < en; ++i) B.perm[pbase + i] = iin[pbase + __float_as_int(S.pts[c][i].w)];
+        for (int i = st; i < en; ++i) B.perm[pbase + i] = __float_as_int(S.pts[c][i].w);
       }
       // ---- partition of the split nodes, the warp per node
       for (int q = 0; q < nsplit; ++q) {
@@ -1342,7 +1324,7 @@ __global__ void __launch_bounds__(kDeepThreads, kDeepBlocksPerSM)
           if (valid) {
             const int dst = left ? (st + cl + __popc(bl & lt)) : (mid + cr + __popc(br & lt));
             S.pts[c ^ 1][dst] = p;
-            if (left == small_left) moments_add_point(MS, p, sin_[pbase + __float_as_int(p.w)], t0);
+            if (left == small_left) moments_add_point(MS, p, sts[__float_as_int(p.w)], t0);
           }
           cl += __popc(bl);
           cr += __popc(br);
@@ -1627,7 +1609,7 @@ size_t ws_bytes(int64_t n, int R) {
   const int64_t chunk_cap = n / kChunk + n / kBig + 16;
   const int64_t ntiles = cn / 4096 + 2;
   const int64_t G = (int64_t)(kMaxDepth + 2) * R;
-  return 2 * carve_size<float4>(n) + 2 * carve_size<double>(n) + 3 * carve_size<int32_t>(n) +
+  return 2 * carve_size<float4>(n) + carve_size<double>(n) + carve_size<int32_t>(n) +
          carve_size<BNode>(cn) + 4 * carve_size<int32_t>(cn) + carve_size<int32_t>(ntiles) +
          carve_size<Chunk>(chunk_cap) + 4 * carve_size<int32_t>(chunk_cap) +
          2 * carve_size<U128>((size_t)11 * (n / kBig + 2)) + carve_size<U128>((size_t)11 * cn) + 2 * carve_size<double>(R) +
@@ -1655,10 +1637,7 @@ int ws_alloc(BuildWs& w, int64_t n, int R, cudaStream_t s) {
   char* p = (char*)w.block;
   w.B.p[0] = carve<float4>(p, n);
   w.B.p[1] = carve<float4>(p, n);
-  w.B.s[0] = carve<double>(p, n);
-  w.B.s[1] = carve<double>(p, n);
-  w.B.id[0] = carve<int32_t>(p, n);
-  w.B.id[1] = carve<int32_t>(p, n);
+  w.B.st = carve<double>(p, n);
   w.B.perm = carve<int32_t>(p, n);
   w.nodes = carve<BNode>(p, cn);
   w.alive = carve<int32_t>(p, cn);
@@ -1820,13 +1799,13 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   }
   KDS_CK(cudaMemsetAsync(w.ls, 0, sizeof(LevelState), s));
   KDS_CK(cudaMemcpyAsync(w.off, off.data(), sizeof(int64_t) * (R + 1), cudaMemcpyHostToDevice, s));
-  k_ingest<<<nblk(N, kThreads), kThreads, 0, s>>>(d_xyz, d_st, N, w.B.p[0], w.B.s[0], w.B.id[0], w.ls);
+  k_ingest<<<nblk(N, kThreads), kThreads, 0, s>>>(d_xyz, d_st, N, w.B.p[0], w.B.st, w.ls);
   count_launch();
   {
     KDS_CK(cudaMemsetAsync(w.tsmin, 0xff, sizeof(unsigned long long) * R, s));
     dim3 g((unsigned)std::min<int64_t>(std::max<int64_t>((max_size + kThreads - 1) / kThreads, 1), 64), (unsigned)R);
-    k_tree_min<<<g, kThreads, 0, s>>>(w.B.s[0], w.off, w.tsmin);
-    k_tree_check<<<g, kThreads, 0, s>>>(w.B.s[0], w.off, w.tsmin, w.ts0, w.ls);
+    k_tree_min<<<g, kThreads, 0, s>>>(w.B.st, w.off, w.tsmin);
+    k_tree_check<<<g, kThreads, 0, s>>>(w.B.st, w.off, w.tsmin, w.ts0, w.ls);
     count_launch();
     count_launch();
   }

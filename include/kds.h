@@ -529,6 +529,9 @@ typedef struct {
   kds_tree_params tree;     /* scans and maps */
   kds_aligner_params icp;   /* KDS_ICP requests */
   kds_aligner_params ct;    /* KDS_CTICP requests */
+  int32_t build_threads;    /* build threads, each with its own stream: 1 or 2 (2); passes of
+                               the two run at the same time on the device */
+  int32_t pad_;
 } kds_server_params;
 
 typedef struct {

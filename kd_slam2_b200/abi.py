@@ -192,6 +192,8 @@ class ServerParams(C.Structure):
         ("tree", TreeParams),
         ("icp", AlignerParams),
         ("ct", AlignerParams),
+        ("build_threads", C.c_int32),
+        ("pad_", C.c_int32),
     ]
 
 

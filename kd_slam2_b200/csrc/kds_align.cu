@@ -1474,13 +1474,10 @@ static cudaError_t record_profile_event(cudaEvent_t e, cudaStream_t s) {
 // Blocks of the persistent kernel: every SM full at its occupancy for `smem` bytes of
 // dynamic shared memory, at most one block per work item.
 static int persistent_grid(size_t smem, int64_t items) {
-  static int nsm = 0;
-  if (nsm == 0) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
-      nsm = 148;
-  }
+  int nsm = 0, dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
+    nsm = 148;
   int per = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_linearize_persistent, kBlock, smem) != cudaSuccess ||
       per < 1) {

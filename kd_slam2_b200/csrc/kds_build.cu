@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstddef>
 #include <cstring>
@@ -1714,11 +1715,11 @@ int deep_pass(BuildWs& w, const BuildParams& P, const LevelState& h, cudaStream_
   carve<int32_t>(p, 1);
   U128* ring = carve<U128>(p, (size_t)nwarps * 2 * kDeepNodes * 11);
   int rc = KDS_OK;
-  static bool attr_set = false;  // the attribute is a property of the kernel, per process
-  if (!attr_set) {
+  static std::atomic<bool> attr_set{false};  // a property of the kernel, per process (builds may run on two threads)
+  if (!attr_set.load()) {
     e = cudaFuncSetAttribute((const void*)k_deep_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(DeepWarpSmem) * kDeepWarpsPerBlock));
-    if (e == cudaSuccess) attr_set = true;
+    if (e == cudaSuccess) attr_set.store(true);
   }
   if (e == cudaSuccess) e = cudaMemsetAsync(counts, 0, sizeof(int32_t) * ncount, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(dn_count, 0, sizeof(int32_t), s);

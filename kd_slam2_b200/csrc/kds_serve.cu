@@ -215,7 +215,8 @@ struct kds_server {
   bool started = false, stopping = false;
   int device = 0;
   cudaStream_t sA = nullptr, sB = nullptr;  // Gauss-Newton (high priority), builds
-  std::thread th_build, th_gn;
+  cudaStream_t sB2 = nullptr;               // the second build thread's stream
+  std::thread th_build, th_build2, th_gn;
   int thread_error = KDS_OK;
   char thread_error_text[256] = {0};
 
@@ -354,8 +355,7 @@ int finish_request(kds_server* s, Request* r, cudaStream_t stream, const float* 
 // One build thread: each pass takes the pending map rebuilds first (they unblock whole
 // windows), then admits arrived requests.  (Two build passes running concurrently on
 // separate streams each take the whole GPU and slowed each other down.)
-void build_loop(kds_server* s) {
-  const cudaStream_t bst = s->sB;
+void build_loop(kds_server* s, cudaStream_t bst) {
   cudaSetDevice(s->device);
   std::vector<Request*> batch;
   std::vector<MapTask> maps;
@@ -975,6 +975,7 @@ void kds_server_params_default(kds_server_params* p) {
   p->max_build_points = 16 << 20;
   p->max_tiles = 32768;
   p->iters_per_tick = 3;
+  p->build_threads = 2;
   kds_tree_params_default(&p->tree);
   kds_aligner_params_default(&p->icp);
   kds_aligner_params_default(&p->ct);
@@ -982,7 +983,7 @@ void kds_server_params_default(kds_server_params* p) {
 
 int kds_server_create(const kds_server_params* params, kds_server** out) {
   if (!params || !out || params->max_slots <= 0 || params->map_every <= 0 || params->max_build_trees <= 0 ||
-      params->max_tiles <= 0 || params->iters_per_tick <= 0) {
+      params->max_tiles <= 0 || params->iters_per_tick <= 0 || params->build_threads > 2) {
     set_error("kds_server_create: bad parameters");
     return KDS_ERR_INVALID_ARG;
   }
@@ -996,6 +997,7 @@ int kds_server_create(const kds_server_params* params, kds_server** out) {
   KDS_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
   KDS_CK(cudaStreamCreateWithPriority(&s->sA, cudaStreamNonBlocking, hi));
   KDS_CK(cudaStreamCreateWithPriority(&s->sB, cudaStreamNonBlocking, lo));
+  KDS_CK(cudaStreamCreateWithPriority(&s->sB2, cudaStreamNonBlocking, lo));
   size_t fr = 0, tot = 0;
   KDS_CK(cudaMemGetInfo(&fr, &tot));
   const int64_t avail = (int64_t)(fr * 0.9);
@@ -1154,7 +1156,8 @@ int kds_server_start(kds_server* s) {
   if (s->P.serial) {
     s->th_build = std::thread(serial_loop, s);
   } else {
-    s->th_build = std::thread(build_loop, s);
+    s->th_build = std::thread(build_loop, s, s->sB);
+    if (s->P.build_threads > 1) s->th_build2 = std::thread(build_loop, s, s->sB2);
     s->th_gn = std::thread(gn_loop, s);
   }
   return KDS_OK;
@@ -1242,9 +1245,11 @@ void kds_server_free(kds_server* s) {
     s->cv_done.notify_all();
   }
   if (s->th_build.joinable()) s->th_build.join();
+  if (s->th_build2.joinable()) s->th_build2.join();
   if (s->th_gn.joinable()) s->th_gn.join();
   cudaStreamSynchronize(s->sA);
   cudaStreamSynchronize(s->sB);
+  cudaStreamSynchronize(s->sB2);
   for (auto& r : s->reqs) {
     if (r->tree) kds_tree_free(r->tree);
     if (r->batch && r->batch->block) {
@@ -1259,6 +1264,7 @@ void kds_server_free(kds_server* s) {
   }
   cudaStreamSynchronize(s->sA);
   cudaStreamSynchronize(s->sB);
+  cudaStreamSynchronize(s->sB2);
   cudaFree(s->d_jobs);
   cudaFree(s->d_states);
   cudaFree(s->d_outs);
@@ -1279,6 +1285,7 @@ void kds_server_free(kds_server* s) {
   }
   cudaStreamDestroy(s->sA);
   cudaStreamDestroy(s->sB);
+  cudaStreamDestroy(s->sB2);
   cudaGetLastError();
   delete s;
 }

@@ -572,6 +572,8 @@ typedef struct {
   double build_point_levels; /* sum over the passes of points x levels */
   double build_global_point_levels; /* sum over the passes of points x levels built level by level
                                        (the levels below ran in shared-memory subtrees) */
+  double build_busy_ms;     /* wall time during which at least one build pass ran (passes of the
+                               two build threads overlap) */
 } kds_server_stats;
 
 void kds_server_params_default(kds_server_params* p);

@@ -247,6 +247,7 @@ class ServerStats(C.Structure):
         ("build_points", C.c_int64),
         ("build_point_levels", C.c_double),
         ("build_global_point_levels", C.c_double),
+        ("build_busy_ms", C.c_double),
     ]
 
     def as_dict(self) -> dict:

@@ -259,7 +259,10 @@ struct kds_server {
   int64_t ticks = 0, build_passes = 0, map_builds = 0, built_trees = 0;
   double sum_active = 0.0, lin_ms = 0.0, alg_bytes = 0.0;
   int64_t lin_launches = 0, leaf_iterations = 0, h2d_bytes = 0, d2h_bytes = 0;
-  double build_ms = 0.0;      // wall time of the build passes
+  double build_ms = 0.0;      // wall time of the build passes (summed over passes)
+  double build_busy_ms = 0.0;  // wall time during which at least one build pass ran
+  int32_t passes_running = 0;
+  double busy_since = 0.0;
   // timeline: kind (0 build pass, 1 tick), count (points / registrations), begin, end [s]
   std::vector<std::array<double, 4>> trace;
   double tick_t0[2] = {0.0, 0.0};
@@ -422,6 +425,7 @@ void build_loop(kds_server* s, cudaStream_t bst) {
         }
         if (!batch.empty() || !maps.empty()) {
           if (!batch.empty()) ++s->request_passes;
+          if (s->passes_running++ == 0) s->busy_since = seconds_since(s->t0);
           transient = batch.empty() ? 0 : (int64_t)forest_workspace_bytes(rpts, (int)batch.size());
           s->reserved += transient;
           s->peak_reserved = std::max(s->peak_reserved, s->reserved);
@@ -505,6 +509,7 @@ void build_loop(kds_server* s, cudaStream_t bst) {
       s->h2d_bytes += h2d;
       ++s->build_passes;
       s->build_ms += 1e3 * seconds_since(pass_t0);
+      if (--s->passes_running == 0) s->build_busy_ms += 1e3 * (seconds_since(s->t0) - s->busy_since);
       s->build_points += N;
       {
         int depth = 0, glob = 0;  // levels of the pass (the same for every tree it built)
@@ -1239,6 +1244,7 @@ int kds_server_get_stats(kds_server* s, kds_server_stats* st) {
   st->h2d_bytes = s->h2d_bytes;
   st->d2h_bytes = s->d2h_bytes;
   st->build_ms = s->build_ms;
+  st->build_busy_ms = s->build_busy_ms;
   st->build_points = s->build_points;
   st->build_point_levels = s->build_point_levels;
   st->build_global_point_levels = s->build_global_point_levels;

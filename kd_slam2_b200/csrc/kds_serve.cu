@@ -227,7 +227,6 @@ struct kds_server {
   std::deque<MapTask> map_tasks;
   int64_t completed = 0;
   int64_t reserved = 0, peak_reserved = 0, cap = 0;
-  int32_t request_passes = 0;  // build passes with requests on the device now (at most one)
   float* zero_stamps = nullptr;  // serial mode: zero stamps for map builds
   int64_t zero_cap = 0;
 
@@ -381,12 +380,8 @@ void build_loop(kds_server* s, cudaStream_t bst) {
         for (auto& m : maps) pts += m.points;
         int64_t rpts = 0;  // request points of the pass
         double next_arrival = -1.0;
-        // One request pass at a time: a second thread builds map rebuilds beside it (they
-        // are on the critical path of the next window), not more request trees, which
-        // would slow the current window's trees that its ticks wait for.
-        const bool may_admit = s->request_passes == 0;
         auto it = s->pending.begin();
-        while (may_admit && it != s->pending.end() && (int)(batch.size() + maps.size()) < s->P.max_build_trees) {
+        while (it != s->pending.end() && (int)(batch.size() + maps.size()) < s->P.max_build_trees) {
           Request* r = *it;
           if (r->in.arrival > now) {
             next_arrival = r->in.arrival;
@@ -424,7 +419,6 @@ void build_loop(kds_server* s, cudaStream_t bst) {
           rpts += r->in.n;
         }
         if (!batch.empty() || !maps.empty()) {
-          if (!batch.empty()) ++s->request_passes;
           if (s->passes_running++ == 0) s->busy_since = seconds_since(s->t0);
           transient = batch.empty() ? 0 : (int64_t)forest_workspace_bytes(rpts, (int)batch.size());
           s->reserved += transient;
@@ -434,7 +428,7 @@ void build_loop(kds_server* s, cudaStream_t bst) {
         // a request refused above can complete a window and queue its map rebuild (its
         // notification came while this thread held the lock): take it before waiting
         if (!s->map_tasks.empty()) continue;
-        if (next_arrival > 0.0 && may_admit)
+        if (next_arrival > 0.0)
           s->cv_build.wait_for(lk, std::chrono::duration<double>(std::max(0.0, next_arrival - now)));
         else
           s->cv_build.wait(lk);
@@ -502,10 +496,6 @@ void build_loop(kds_server* s, cudaStream_t bst) {
     {
       std::lock_guard<std::mutex> g(s->mu);
       s->reserved -= transient;
-      if (!batch.empty()) {
-        --s->request_passes;
-        s->cv_build.notify_all();  // the other thread may admit requests now
-      }
       s->h2d_bytes += h2d;
       ++s->build_passes;
       s->build_ms += 1e3 * seconds_since(pass_t0);

@@ -529,8 +529,11 @@ typedef struct {
   kds_tree_params tree;     /* scans and maps */
   kds_aligner_params icp;   /* KDS_ICP requests */
   kds_aligner_params ct;    /* KDS_CTICP requests */
-  int32_t build_threads;    /* build threads, each with its own stream: 1 or 2 (2); passes of
-                               the two run at the same time on the device */
+  int32_t build_threads;    /* build threads, each with its own stream: 1 or 2 (2).  With 2, one
+                               builds the map rebuilds and the requests whose map is installed
+                               (a stream one priority below the Gauss-Newton one), the other
+                               the requests whose map is not there yet (lowest priority, while
+                               the reservations stay under a quarter of the cap) */
   int32_t pad_;
 } kds_server_params;
 
@@ -574,6 +577,8 @@ typedef struct {
                                        (the levels below ran in shared-memory subtrees) */
   double build_busy_ms;     /* wall time during which at least one build pass ran (passes of the
                                two build threads overlap) */
+  int64_t build_released_ahead; /* trees built ahead of their map and released to make room
+                                   under the cap (rebuilt later; two build threads only) */
 } kds_server_stats;
 
 void kds_server_params_default(kds_server_params* p);

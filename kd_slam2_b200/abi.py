@@ -248,6 +248,7 @@ class ServerStats(C.Structure):
         ("build_point_levels", C.c_double),
         ("build_global_point_levels", C.c_double),
         ("build_busy_ms", C.c_double),
+        ("build_released_ahead", C.c_int64),
     ]
 
     def as_dict(self) -> dict:

@@ -7,10 +7,12 @@
 // kd/icp/tree_aligner_base_.h:100-115) on a moving tree from
 // TreeGenerator_::makeTree (kd/tree/tree_generator_impl_.h:7-19).
 //
-// Two host threads drive two CUDA streams:
-//  * the build thread admits arrived requests in arrival order while their estimated
+// Host threads drive their own CUDA streams:
+//  * a build thread admits arrived requests in arrival order while their estimated
 //    device memory fits under the cap, copies their points to the device and builds
-//    all their moving trees -- and any pending map rebuilds -- in one forest pass;
+//    all their moving trees -- and any pending map rebuilds -- in one forest pass (with
+//    two build threads, one builds what can register next and the other builds ahead;
+//    see build_loop);
 //  * the Gauss-Newton thread runs ticks.  One tick = one k_linearize launch per kind
 //    over the tiles of every active job, followed by a compact result copy.  Requests
 //    whose trees are built join at the next tick when a slot, tile space and their
@@ -261,6 +263,7 @@ struct kds_server {
   double build_ms = 0.0;      // wall time of the build passes (summed over passes)
   double build_busy_ms = 0.0;  // wall time during which at least one build pass ran
   int32_t passes_running = 0;
+  int64_t released_ahead = 0;  // trees built ahead and released to make room
   double busy_since = 0.0;
   // timeline: kind (0 build pass, 1 tick), count (points / registrations), begin, end [s]
   std::vector<std::array<double, 4>> trace;
@@ -354,11 +357,50 @@ int finish_request(kds_server* s, Request* r, cudaStream_t stream, const float* 
 }
 
 // ---------------------------------------------------------------------------
-// Build thread (served mode)
-// One build thread: each pass takes the pending map rebuilds first (they unblock whole
-// windows), then admits arrived requests.  (Two build passes running concurrently on
-// separate streams each take the whole GPU and slowed each other down.)
-void build_loop(kds_server* s, cudaStream_t bst) {
+// Build threads (served mode)
+// With one build thread each pass takes the pending map rebuilds first (they unblock whole
+// windows), then admits arrived requests in arrival order.  With two, the work is split by
+// what it unblocks:
+//  * the first thread (stream above the second in priority) takes the map rebuilds and the
+//    requests whose map version is installed: everything that can register as soon as it
+//    is built;
+//  * the second takes the requests whose map is not there yet and builds their trees
+//    ahead, at the lowest priority, in the time the first leaves.  It admits only while
+//    the reservations stay under a quarter of the cap; when the first thread cannot fit a
+//    request it releases the trees built ahead (they are rebuilt later), so a request that
+//    fits under the cap alone is never held back by work that waits for it.
+
+// Releases the trees built ahead (requests whose map version is not installed) and puts
+// their requests back into the pending queue in arrival order.  Called with the lock held.
+bool release_ahead(kds_server* s) {
+  bool any = false;
+  for (auto it = s->ready.begin(); it != s->ready.end();) {
+    Request* r = *it;
+    if (s->streams[r->in.stream].installed >= r->window) { ++it; continue; }
+    if (r->tree) kds_tree_free(r->tree);
+    r->tree = nullptr;
+    if (r->batch && --r->batch->refs == 0 && r->batch->block) {
+      cudaFreeAsync(r->batch->block, s->sB2);
+      r->batch->block = nullptr;
+    }
+    r->batch.reset();
+    s->reserved -= r->reserved;
+    r->reserved = 0;
+    r->built = false;
+    it = s->ready.erase(it);
+    auto pos = std::find_if(s->pending.begin(), s->pending.end(), [&](const Request* q) {
+      return q->in.arrival > r->in.arrival || (q->in.arrival == r->in.arrival && q->ticket > r->ticket);
+    });
+    s->pending.insert(pos, r);
+    ++s->released_ahead;
+    any = true;
+  }
+  return any;
+}
+
+void build_loop(kds_server* s, cudaStream_t bst, int role) {
+  const bool split = s->P.build_threads > 1;  // roles as above; role 0 takes everything otherwise
+  const bool ahead = split && role == 1;
   cudaSetDevice(s->device);
   std::vector<Request*> batch;
   std::vector<MapTask> maps;
@@ -372,7 +414,7 @@ void build_loop(kds_server* s, cudaStream_t bst) {
         if (s->stopping) return;
         const double now = seconds_since(s->t0);
         // map rebuilds first; they are not held under the cap
-        while (!s->map_tasks.empty() && (int)maps.size() < s->P.max_build_trees) {
+        while (!ahead && !s->map_tasks.empty() && (int)maps.size() < s->P.max_build_trees) {
           maps.push_back(s->map_tasks.front());
           s->map_tasks.pop_front();
         }
@@ -380,6 +422,7 @@ void build_loop(kds_server* s, cudaStream_t bst) {
         for (auto& m : maps) pts += m.points;
         int64_t rpts = 0;  // request points of the pass
         double next_arrival = -1.0;
+        bool released = false;
         auto it = s->pending.begin();
         while (it != s->pending.end() && (int)(batch.size() + maps.size()) < s->P.max_build_trees) {
           Request* r = *it;
@@ -387,12 +430,22 @@ void build_loop(kds_server* s, cudaStream_t bst) {
             next_arrival = r->in.arrival;
             break;
           }
+          if (split && (s->streams[r->in.stream].installed < r->window) != ahead) {
+            ++it;
+            continue;
+          }
           if (!batch.empty() && pts + r->in.n > s->P.max_build_points) break;
           const int64_t need = request_persistent_bytes(r->in);
           const int64_t ws = (int64_t)forest_workspace_bytes(rpts + r->in.n, (int)batch.size() + 1);
-          if (s->reserved + need + ws > s->cap) {
-            if (s->reserved == 0 && batch.empty()) {
-              // can never fit: refused at admission, finishes with its initial guess
+          if (s->reserved + need + ws > (ahead ? s->cap / 4 : s->cap)) {
+            if (ahead) break;
+            if (split && !released && release_ahead(s)) {
+              released = true;  // the queue changed: scan again (admitted requests left it)
+              it = s->pending.begin();
+              continue;
+            }
+            if (batch.empty() && need + (int64_t)forest_workspace_bytes(r->in.n, 1) > s->cap) {
+              // can never fit, even alone: refused at admission, finishes with its initial guess
               it = s->pending.erase(it);
               r->res.status = KDS_ERR_ADMISSION;
               memcpy(r->res.X, r->in.X0, sizeof(r->res.X));
@@ -427,7 +480,7 @@ void build_loop(kds_server* s, cudaStream_t bst) {
         }
         // a request refused above can complete a window and queue its map rebuild (its
         // notification came while this thread held the lock): take it before waiting
-        if (!s->map_tasks.empty()) continue;
+        if (!ahead && !s->map_tasks.empty()) continue;
         if (next_arrival > 0.0)
           s->cv_build.wait_for(lk, std::chrono::duration<double>(std::max(0.0, next_arrival - now)));
         else
@@ -554,6 +607,7 @@ void build_loop(kds_server* s, cudaStream_t bst) {
         B->block = nullptr;
       }
       s->cv_gn.notify_all();
+      if (split) s->cv_build.notify_all();  // installed maps make queued requests the other role's
     }
   }
 }
@@ -1001,7 +1055,9 @@ int kds_server_create(const kds_server_params* params, kds_server** out) {
   int lo = 0, hi = 0;
   KDS_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
   KDS_CK(cudaStreamCreateWithPriority(&s->sA, cudaStreamNonBlocking, hi));
-  KDS_CK(cudaStreamCreateWithPriority(&s->sB, cudaStreamNonBlocking, lo));
+  // builds that unblock registrations one step below the Gauss-Newton stream (where the
+  // range has room), builds ahead at the lowest priority
+  KDS_CK(cudaStreamCreateWithPriority(&s->sB, cudaStreamNonBlocking, lo - hi >= 2 ? hi + 1 : lo));
   KDS_CK(cudaStreamCreateWithPriority(&s->sB2, cudaStreamNonBlocking, lo));
   size_t fr = 0, tot = 0;
   KDS_CK(cudaMemGetInfo(&fr, &tot));
@@ -1161,8 +1217,8 @@ int kds_server_start(kds_server* s) {
   if (s->P.serial) {
     s->th_build = std::thread(serial_loop, s);
   } else {
-    s->th_build = std::thread(build_loop, s, s->sB);
-    if (s->P.build_threads > 1) s->th_build2 = std::thread(build_loop, s, s->sB2);
+    s->th_build = std::thread(build_loop, s, s->sB, 0);
+    if (s->P.build_threads > 1) s->th_build2 = std::thread(build_loop, s, s->sB2, 1);
     s->th_gn = std::thread(gn_loop, s);
   }
   return KDS_OK;
@@ -1235,6 +1291,7 @@ int kds_server_get_stats(kds_server* s, kds_server_stats* st) {
   st->d2h_bytes = s->d2h_bytes;
   st->build_ms = s->build_ms;
   st->build_busy_ms = s->build_busy_ms;
+  st->build_released_ahead = s->released_ahead;
   st->build_points = s->build_points;
   st->build_point_levels = s->build_point_levels;
   st->build_global_point_levels = s->build_global_point_levels;

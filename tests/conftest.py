@@ -57,8 +57,9 @@ def pose_err(A, B):
     A = np.asarray(A, np.float64).reshape(3, 4)
     B = np.asarray(B, np.float64).reshape(3, 4)
     dR = A[:, :3].T @ B[:, :3]
-    c = np.clip((np.trace(dR) - 1) / 2, -1, 1)
-    return float(np.linalg.norm(A[:, 3] - B[:, 3])), float(np.arccos(c))
+    # atan2 of the skew part and the trace: arccos of the trace alone bottoms out near 3e-8 rad
+    w = 0.5 * np.array([dR[2, 1] - dR[1, 2], dR[0, 2] - dR[2, 0], dR[1, 0] - dR[0, 1]])
+    return float(np.linalg.norm(A[:, 3] - B[:, 3])), float(np.arctan2(np.linalg.norm(w), (np.trace(dR) - 1) / 2))
 
 
 def assert_same_tree(O, G):

@@ -8,8 +8,8 @@
 * Requests aligned against the initial map agree with the oracle in the product's
   semantics within 1e-5 m / 1e-5 rad, and with the all-FP64 oracle within 1e-4.
 * Admission by device memory: under a small cap every request still finishes, the
-  reserved bytes never exceed the cap, the results do not change; a request that can
-  never fit is refused with KDS_ERR_ADMISSION.
+  reserved bytes never exceed the cap, the results do not change, with one build thread
+  or two; a request that can never fit is refused with KDS_ERR_ADMISSION.
 """
 import numpy as np
 import pytest
@@ -116,6 +116,23 @@ def test_admission_under_a_small_cap(trace):
     assert st["hbm_cap"] == cap
     assert 0 < st["peak_reserved"] <= cap
     same_results(served, capped)
+
+
+@pytest.mark.parametrize("factor", [1100, 1600, 3200])
+def test_build_threads_and_caps_do_not_change_results(trace, factor):
+    """One build thread, or two (one building what can register next, the other building
+    ahead of the maps and giving its trees back when the first cannot fit a request):
+    the same results under caps from about one to four of the largest requests."""
+    served, _, _ = run(trace, build_threads=1)
+    biggest = max(len(r.xyz) for r in trace.requests)
+    cap = int(biggest * factor)
+    for threads in (1, 2):
+        capped, st, _ = run(trace, hbm_cap=cap, build_threads=threads)
+        assert st["completed"] == len(trace.requests)
+        assert 0 < st["peak_reserved"] <= cap
+        if threads == 1:
+            assert st["build_released_ahead"] == 0
+        same_results(served, capped)
 
 
 def test_request_that_never_fits_is_refused(trace):

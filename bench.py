@@ -1175,9 +1175,10 @@ def main():
         "plain": plain,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(e2e_stats["h2d_bytes"]),
                 "d2h_bytes_per_step": int(e2e_stats["d2h_bytes"]), "results_identical_to_device_inputs":
-                    bool(same_host_dev)},
+                    bool(same_host_dev), "ms_per_step_all": [float(x) for x in e2e_times]},
         "gpu_launches": int(launches),
-        "served": {"ticks": st0["ticks"], "mean_registrations_per_tick": st0["mean_active"],
+        "served": {"ms_per_step_all": [float(x) for x in times],
+                   "ticks": st0["ticks"], "mean_registrations_per_tick": st0["mean_active"],
                    "build_passes": st0["build_passes"], "trees_built": st0["built_trees"],
                    "map_rebuilds": st0["map_builds"], "build_pass_ms": st0["build_ms"],
                    "build_points": st0["build_points"], "peak_reserved_bytes": st0["peak_reserved"],

@@ -530,10 +530,9 @@ typedef struct {
   kds_aligner_params icp;   /* KDS_ICP requests */
   kds_aligner_params ct;    /* KDS_CTICP requests */
   int32_t build_threads;    /* build threads, each with its own stream: 1 or 2 (2).  With 2, one
-                               builds the map rebuilds and the requests whose map is installed
-                               (a stream one priority below the Gauss-Newton one), the other
-                               the requests whose map is not there yet (lowest priority, while
-                               the reservations stay under a quarter of the cap) */
+                               builds the map rebuilds and the requests whose map is installed,
+                               the other the requests whose map is not there yet (while the
+                               reservations stay under a quarter of the cap) */
   int32_t pad_;
 } kds_server_params;
 

@@ -1682,6 +1682,9 @@ int linearize_smem_setup() {
   KDS_CK(cudaFuncSetAttribute((const void*)k_linearize<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   KDS_CK(cudaFuncSetAttribute((const void*)k_linearize<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   KDS_CK(cudaFuncSetAttribute((const void*)k_linearize<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  KDS_CK(cudaFuncSetAttribute((const void*)k_linearize_pair<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  KDS_CK(cudaFuncSetAttribute((const void*)k_linearize_pair<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  KDS_CK(cudaFuncSetAttribute((const void*)k_linearize_pair<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   return KDS_OK;
 }
 
@@ -1707,6 +1710,24 @@ int launch_linearize(int kind, int ntiles, const JobIn* jobs, JobState* states, 
   else
     k_linearize<2><<<ntiles, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, 0, kServeStage,
                                                        partials, nullptr, nullptr, nullptr);
+  count_launch();
+  KDS_CK(cudaGetLastError());
+  return KDS_OK;
+}
+
+int launch_linearize_pairs(int kind, int npairs, const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins,
+                           const TileDev* tiles, const int2* pairs, double* partials, cudaStream_t s) {
+  if (npairs <= 0) return KDS_OK;
+  const size_t stage_bytes = (size_t)kServeStage * sizeof(DNode);
+  if (kind == 0)
+    k_linearize_pair<0><<<npairs, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, pairs, 0,
+                                                            kServeStage, partials, nullptr, nullptr, nullptr);
+  else if (kind == 1)
+    k_linearize_pair<1><<<npairs, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, pairs, 0,
+                                                            kServeStage, partials, nullptr, nullptr, nullptr);
+  else
+    k_linearize_pair<2><<<npairs, kBlock, stage_bytes, s>>>(jobs, states, outs, nullptr, lins, tiles, pairs, 0,
+                                                            kServeStage, partials, nullptr, nullptr, nullptr);
   count_launch();
   KDS_CK(cudaGetLastError());
   return KDS_OK;

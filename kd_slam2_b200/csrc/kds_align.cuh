@@ -170,12 +170,16 @@ struct SlotResult {
 };
 constexpr int kStageNodes = 2047;  // most fixed-tree nodes any launch stages in shared memory
 constexpr int kServeStage = 1023;  // nodes the served loop stages (a smaller stage leaves room for more blocks)
-constexpr int kTileSurfels = 128;  // moving surfels per tile = threads per k_linearize block  // fixed-tree nodes each block stages in shared memory
+constexpr int kTileSurfels = 128;  // moving surfels per tile = threads per k_linearize block
 // Copies n admitted job records into their slots and initialises those jobs.
 int launch_admit_slots(const int32_t* d_slots, int n, const JobIn* new_jobs, const LinDev* new_lins, JobIn* jobs,
                        JobState* states, JobOut* outs, LinDev* lins, cudaStream_t s);
 int launch_linearize(int kind, int ntiles, const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins,
                      const TileDev* tiles, double* partials, cudaStream_t s);
+// Two tiles of one (job, fixed entry) per block (k_linearize_pair): pairs[i] = (tile,
+// second tile or -1).
+int launch_linearize_pairs(int kind, int npairs, const JobIn* jobs, JobState* states, JobOut* outs, LinDev* lins,
+                           const TileDev* tiles, const int2* pairs, double* partials, cudaStream_t s);
 int launch_collect(int n, const JobState* states, const JobOut* outs, const unsigned long long* touched,
                    SlotResult* res, cudaStream_t s);
 // Counts the distinct fixed nodes that the descents of job `slot` visit at its current

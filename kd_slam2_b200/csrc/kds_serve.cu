@@ -13,8 +13,9 @@
 //    all their moving trees -- and any pending map rebuilds -- in one forest pass (with
 //    two build threads, one builds what can register next and the other builds ahead;
 //    see build_loop);
-//  * the Gauss-Newton thread runs ticks.  One tick = one k_linearize launch per kind
-//    over the tiles of every active job, followed by a compact result copy.  Requests
+//  * the Gauss-Newton thread runs ticks.  One tick = one k_linearize_pair launch per
+//    kind over the tiles of every active job (two tiles of one job per block), followed
+//    by a compact result copy.  Requests
 //    whose trees are built join at the next tick when a slot, tile space and their
 //    map version are available; finished jobs leave at the tick after they finish.
 //    Ticks are double buffered: tick t+1 is queued before the results of tick t are
@@ -239,6 +240,7 @@ struct kds_server {
   JobOut* d_outs = nullptr;
   LinDev* d_lins = nullptr;
   TileDev* d_tiles[2] = {nullptr, nullptr};
+  int2* d_pairs[2] = {nullptr, nullptr};  // blocks of two tiles of one job, per kind
   double* d_partials[2] = {nullptr, nullptr};
   SlotResult* d_res = nullptr;
   void* d_stage = nullptr;  // admitted job records (2 tick buffers)
@@ -361,11 +363,10 @@ int finish_request(kds_server* s, Request* r, cudaStream_t stream, const float* 
 // With one build thread each pass takes the pending map rebuilds first (they unblock whole
 // windows), then admits arrived requests in arrival order.  With two, the work is split by
 // what it unblocks:
-//  * the first thread (stream above the second in priority) takes the map rebuilds and the
-//    requests whose map version is installed: everything that can register as soon as it
-//    is built;
+//  * the first thread takes the map rebuilds and the requests whose map version is
+//    installed: everything that can register as soon as it is built;
 //  * the second takes the requests whose map is not there yet and builds their trees
-//    ahead, at the lowest priority, in the time the first leaves.  It admits only while
+//    ahead, beside the first.  It admits only while
 //    the reservations stay under a quarter of the cap; when the first thread cannot fit a
 //    request it releases the trees built ahead (they are rebuilt later), so a request that
 //    fits under the cap alone is never held back by work that waits for it.
@@ -617,7 +618,21 @@ void build_loop(kds_server* s, cudaStream_t bst, int role) {
 size_t stage_bytes(const kds_server* s) {
   const size_t recs = ((size_t)s->S * (sizeof(int32_t) + sizeof(JobIn) + sizeof(LinDev)) + 3 * 256 + 255) &
                       ~(size_t)255;
-  return recs + sizeof(TileDev) * (size_t)(s->arena[0].cap + s->arena[1].cap) + 256;
+  return recs + (sizeof(TileDev) + sizeof(int2)) * (size_t)(s->arena[0].cap + s->arena[1].cap) + 512;
+}
+
+// Blocks of two consecutive tiles of one job (the pair form of k_linearize: two descents
+// in flight per thread, the tree top staged once per two tiles); the sentinel's free tiles
+// get no block.  Returns the number of pairs written to out.
+int make_pairs(const TileDev* tiles, int hw, int sentinel, int2* out) {
+  int n = 0;
+  for (int t = 0; t < hw;) {
+    if (tiles[t].job == sentinel) { ++t; continue; }
+    const bool two = t + 1 < hw && tiles[t + 1].job == tiles[t].job && tiles[t + 1].lin == tiles[t].lin;
+    out[n++] = make_int2(t, two ? t + 1 : -1);
+    t += two ? 2 : 1;
+  }
+  return n;
 }
 
 void release_slot(kds_server* s, Request* r) {
@@ -772,6 +787,9 @@ void gn_loop(kds_server* s) {
       const int hw0 = s->arena[0].hw, hw1 = s->arena[1].hw;
       if (hw0) memcpy(h_t0, s->h_tiles[0].data(), sizeof(TileDev) * hw0);
       if (hw1) memcpy(h_t1, s->h_tiles[1].data(), sizeof(TileDev) * hw1);
+      int2* h_p0 = (int2*)(h_t1 + s->arena[1].cap);
+      int2* h_p1 = h_p0 + s->arena[0].cap;
+      const int np0 = make_pairs(h_t0, hw0, s->S, h_p0), np1 = make_pairs(h_t1, hw1, s->S, h_p1);
       char* d = (char*)s->d_stage + (size_t)buf * stage_bytes(s);
       cudaStream_t A = s->sA;
       cudaError_t e = cudaSuccess;
@@ -780,6 +798,10 @@ void gn_loop(kds_server* s) {
         e = cudaMemcpyAsync(s->d_tiles[0], h_t0, sizeof(TileDev) * hw0, cudaMemcpyHostToDevice, A);
       if (e == cudaSuccess && hw1)
         e = cudaMemcpyAsync(s->d_tiles[1], h_t1, sizeof(TileDev) * hw1, cudaMemcpyHostToDevice, A);
+      if (e == cudaSuccess && np0)
+        e = cudaMemcpyAsync(s->d_pairs[0], h_p0, sizeof(int2) * np0, cudaMemcpyHostToDevice, A);
+      if (e == cudaSuccess && np1)
+        e = cudaMemcpyAsync(s->d_pairs[1], h_p1, sizeof(int2) * np1, cudaMemcpyHostToDevice, A);
       if (e != cudaSuccess) rc = cuda_status(e, "served tick upload", __FILE__, __LINE__);
       if (!rc && na > 0) {
         const int32_t* d_slots = (const int32_t*)d;
@@ -802,11 +824,11 @@ void gn_loop(kds_server* s) {
       if (!rc && !active_cur.empty()) {
         if (s->P.profile) cudaEventRecord(s->ev_lin[buf][0], A);
         for (int it = 0; it < s->P.iters_per_tick && !rc; ++it) {
-          rc = launch_linearize(0, hw0, s->d_jobs, s->d_states, s->d_outs, s->d_lins, s->d_tiles[0],
-                                s->d_partials[0], A);
+          rc = launch_linearize_pairs(0, np0, s->d_jobs, s->d_states, s->d_outs, s->d_lins, s->d_tiles[0],
+                                      s->d_pairs[0], s->d_partials[0], A);
           if (!rc)
-            rc = launch_linearize(1, hw1, s->d_jobs, s->d_states, s->d_outs, s->d_lins, s->d_tiles[1],
-                                  s->d_partials[1], A);
+            rc = launch_linearize_pairs(1, np1, s->d_jobs, s->d_states, s->d_outs, s->d_lins, s->d_tiles[1],
+                                        s->d_pairs[1], s->d_partials[1], A);
         }
         if (s->P.profile) cudaEventRecord(s->ev_lin[buf][1], A);
         int nslots = 0;
@@ -1055,9 +1077,10 @@ int kds_server_create(const kds_server_params* params, kds_server** out) {
   int lo = 0, hi = 0;
   KDS_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
   KDS_CK(cudaStreamCreateWithPriority(&s->sA, cudaStreamNonBlocking, hi));
-  // builds that unblock registrations one step below the Gauss-Newton stream (where the
-  // range has room), builds ahead at the lowest priority
-  KDS_CK(cudaStreamCreateWithPriority(&s->sB, cudaStreamNonBlocking, lo - hi >= 2 ? hi + 1 : lo));
+  // both build streams at the lowest priority: a build stream above the other made the
+  // two passes preempt each other's blocks (two overlapped passes took 35-55 ms instead of
+  // 8-13 ms in some steps)
+  KDS_CK(cudaStreamCreateWithPriority(&s->sB, cudaStreamNonBlocking, lo));
   KDS_CK(cudaStreamCreateWithPriority(&s->sB2, cudaStreamNonBlocking, lo));
   size_t fr = 0, tot = 0;
   KDS_CK(cudaMemGetInfo(&fr, &tot));
@@ -1082,6 +1105,7 @@ int kds_server_create(const kds_server_params* params, kds_server** out) {
       KDS_CK(cudaMemcpy(s->d_tiles[k], s->h_tiles[k].data(), sizeof(TileDev) * params->max_tiles,
                         cudaMemcpyHostToDevice));
       KDS_CK(cudaMalloc(&s->d_partials[k], sizeof(double) * kPStride * params->max_tiles));
+      KDS_CK(cudaMalloc(&s->d_pairs[k], sizeof(int2) * params->max_tiles));
       KDS_CK(cudaMallocHost(&s->h_stage[k], stage_bytes(s.get())));
       KDS_CK(cudaMallocHost(&s->h_res[k], sizeof(SlotResult) * S1));
       KDS_CK(cudaEventCreateWithFlags(&s->ev_tick[k], cudaEventDisableTiming));
@@ -1339,6 +1363,7 @@ void kds_server_free(kds_server* s) {
   cudaFree(s->zero_stamps);
   for (int k = 0; k < 2; ++k) {
     cudaFree(s->d_tiles[k]);
+    cudaFree(s->d_pairs[k]);
     cudaFree(s->d_partials[k]);
     if (s->h_stage[k]) cudaFreeHost(s->h_stage[k]);
     if (s->h_res[k]) cudaFreeHost(s->h_res[k]);

@@ -529,10 +529,12 @@ typedef struct {
   kds_tree_params tree;     /* scans and maps */
   kds_aligner_params icp;   /* KDS_ICP requests */
   kds_aligner_params ct;    /* KDS_CTICP requests */
-  int32_t build_threads;    /* build threads, each with its own stream: 1 or 2 (2).  With 2, one
+  int32_t build_threads;    /* build threads, each with its own stream: 1 or 2 (1).  With 2, one
                                builds the map rebuilds and the requests whose map is installed,
                                the other the requests whose map is not there yet (while the
-                               reservations stay under a quarter of the cap) */
+                               reservations stay under a quarter of the cap): typical steps
+                               are shorter, but while the two passes overlap some steps
+                               stall for tens to hundreds of milliseconds */
   int32_t pad_;
 } kds_server_params;
 

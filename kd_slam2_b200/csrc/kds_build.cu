@@ -1746,6 +1746,37 @@ size_t forest_workspace_bytes(int64_t n, int R) { return ws_bytes(std::max<int64
 
 // Builds R trees from R clouds stored back to back (offsets[R+1] on the host).
 // out[r] = NULL and status[r] = KDS_ERR_TREE_REJECTED where makeTree returns nullptr.
+// Page-locked staging for the build's small device-to-host reads (the level state at each
+// host check, the per-tree counts at the end) instead of pageable host memory: one block
+// per host thread, grown on demand, released when the thread exits.
+struct PinnedStage {
+  void* p = nullptr;
+  size_t cap = 0;
+  ~PinnedStage() {
+    if (p) cudaFreeHost(p);
+  }
+  void* get(size_t bytes) {
+    if (bytes > cap) {
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+      cap = 0;
+      const size_t c = std::max<size_t>(bytes, 64 * 1024);
+      if (cudaMallocHost(&p, c) != cudaSuccess) {
+        cudaGetLastError();
+        p = nullptr;
+        return nullptr;
+      }
+      cap = c;
+    }
+    return p;
+  }
+};
+
+void* pinned_stage(size_t bytes) {
+  thread_local PinnedStage st;
+  return st.get(bytes);
+}
+
 int tree_build_forest(const float* xyz, const double* stamps, const int64_t* offsets, int32_t R, int32_t mem,
                       const kds_tree_params* prm, cudaStream_t s, kds_tree** out, int32_t* status) {
   for (int r = 0; r < R; ++r) { out[r] = nullptr; status[r] = KDS_ERR_TREE_REJECTED; }
@@ -1814,7 +1845,14 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   count_launch();
   KDS_CK(cudaGetLastError());
 
-  LevelState hls;
+  // pinned: [level state | per-tree nodes, leaves, unpruned nodes | ts0 | root frames]
+  const size_t st_ls = (sizeof(LevelState) + 255) & ~(size_t)255;
+  const size_t st_cnt = ((size_t)12 * R + 255) & ~(size_t)255;
+  char* stage = (char*)pinned_stage(st_ls + st_cnt + sizeof(double) * (size_t)(1 + kRootFrame) * R);
+  if (!stage) { set_error("kds_tree_build: page-locked staging of the level state failed"); return KDS_ERR_OOM; }
+  LevelState& hls = *reinterpret_cast<LevelState*>(stage);
+  int32_t* h_cnt = reinterpret_cast<int32_t*>(stage + st_ls);
+  double* h_dbl = reinterpret_cast<double*>(stage + st_ls + st_cnt);
   int32_t host_max = max_size;
   const int cb = std::min<int>(w.chunk_cap, kGridBlocks * 2);
   // Grids of the level kernels sized to the level: a level has at most twice the nodes
@@ -1914,14 +1952,14 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   if (rc) return rc;
   k_group_tables<<<1, 1024, 0, s>>>(depth, R, w.cnt, w.lcnt, w.gp, w.lgp, w.to, w.lto, w.tot_nodes, w.tot_leaves);
   count_launch();
-  std::vector<int32_t> tn(R), tl(R), tu(R);
-  std::vector<double> ts0(R), rf((size_t)kRootFrame * R);
-  KDS_CK(cudaMemcpyAsync(tn.data(), w.tot_nodes, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, s));
-  KDS_CK(cudaMemcpyAsync(tl.data(), w.tot_leaves, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, s));
-  KDS_CK(cudaMemcpyAsync(tu.data(), w.ucnt, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, s));
-  KDS_CK(cudaMemcpyAsync(ts0.data(), w.ts0, sizeof(double) * R, cudaMemcpyDeviceToHost, s));
-  KDS_CK(cudaMemcpyAsync(rf.data(), w.root_frame, sizeof(double) * kRootFrame * R, cudaMemcpyDeviceToHost, s));
+  KDS_CK(cudaMemcpyAsync(h_cnt, w.tot_nodes, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, s));
+  KDS_CK(cudaMemcpyAsync(h_cnt + R, w.tot_leaves, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, s));
+  KDS_CK(cudaMemcpyAsync(h_cnt + 2 * R, w.ucnt, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, s));
+  KDS_CK(cudaMemcpyAsync(h_dbl, w.ts0, sizeof(double) * R, cudaMemcpyDeviceToHost, s));
+  KDS_CK(cudaMemcpyAsync(h_dbl + R, w.root_frame, sizeof(double) * kRootFrame * R, cudaMemcpyDeviceToHost, s));
   KDS_CK(cudaStreamSynchronize(s));
+  const std::vector<int32_t> tn(h_cnt, h_cnt + R), tl(h_cnt + R, h_cnt + 2 * R), tu(h_cnt + 2 * R, h_cnt + 3 * R);
+  const std::vector<double> ts0(h_dbl, h_dbl + R), rf(h_dbl + R, h_dbl + R + (size_t)kRootFrame * R);
   std::vector<TreeDev> td(R);
   std::vector<kds_tree*> made(R, nullptr);
   for (int r = 0; r < R; ++r) {

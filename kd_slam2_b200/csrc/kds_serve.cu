@@ -1056,7 +1056,7 @@ void kds_server_params_default(kds_server_params* p) {
   p->max_build_points = 16 << 20;
   p->max_tiles = 32768;
   p->iters_per_tick = 3;
-  p->build_threads = 2;
+  p->build_threads = 1;
   kds_tree_params_default(&p->tree);
   kds_aligner_params_default(&p->icp);
   kds_aligner_params_default(&p->ct);

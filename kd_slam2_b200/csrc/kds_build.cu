@@ -561,6 +561,9 @@ struct PointBufs {
 // parent's minus the smaller's (exact integer arithmetic).  So below the roots each point
 // is summed once per level only when it lands in the smaller child of its parent.
 
+// L1 prefetch of the line holding p (no register, no effect on results).
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 // Warp-cooperative exact sums of points [b, e) of one point buffer.
 // Warp total of the 11 sums in reduce-scatter form: the 16 slots (11 used) are halved
 // over lane bits 4..1 (8 + 4 + 2 + 1 exchanges instead of 5 x 11), then added with
@@ -706,6 +709,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelS
     }
     const int K = (e - s + 31) >> 5;
     const bool one = K <= kUnroll;  // the whole node fits one round of loads: keep it
+    // every round of the node in flight at once (into L1), instead of one dependent
+    // round trip per kUnroll rounds
+    for (int k = kUnroll; k < K; ++k) {
+      const int i = s + (k << 5) + lane;
+      if (i < e) prefetch_l1(pin + i);
+    }
     unsigned bits = 0u;
     float4 pv[kUnroll];
     for (int k0 = 0; k0 < K; k0 += kUnroll) {
@@ -717,7 +726,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelS
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) {
         int i = s + ((k0 + u) << 5) + lane;
-        if (i < e && which_side_f(mean, dir, pv[u])) bits |= 1u << (k0 + u);
+        if (i < e) {
+          prefetch_l1(sts + __float_as_int(pv[u].w));  // the stamp, if this point lands in the smaller child
+          if (which_side_f(mean, dir, pv[u])) bits |= 1u << (k0 + u);
+        }
       }
     }
     int nl = __popc(bits);

@@ -150,6 +150,37 @@ __device__ __forceinline__ U128 fx_d(double d) {
   return fx_parts(s, m, e);
 }
 
+// floor(d * 2^64) for a non-negative double below 2^52 (the stamp terms dt and dt^2: dt >= 0
+// by construction, dt < 2^16 checked): two clamped shifts instead of fx_parts' branches,
+// the same bits.
+__device__ __forceinline__ unsigned long long shl_c(unsigned long long v, unsigned n) {
+  unsigned long long r;
+  asm("shl.b64 %0, %1, %2;" : "=l"(r) : "l"(v), "r"(n));  // n >= 64 gives 0
+  return r;
+}
+__device__ __forceinline__ unsigned long long shr_c(unsigned long long v, unsigned n) {
+  unsigned long long r;
+  asm("shr.u64 %0, %1, %2;" : "=l"(r) : "l"(v), "r"(n));  // n >= 64 gives 0
+  return r;
+}
+__device__ __forceinline__ U128 fx_d_nonneg(double d) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(d);
+  const int E = (int)((b >> 52) & 0x7ffull);
+  if ((b >> 63) || E >= 1075) return fx_d(d);  // negative, >= 2^52 or not finite: general path
+  unsigned long long m = b & ((1ull << 52) - 1ull);
+  int sh;  // d * 2^64 = m * 2^sh
+  if (E == 0) {
+    sh = -1074 + 64;
+  } else {
+    m |= 1ull << 52;
+    sh = E - 1075 + 64;
+  }
+  U128 r;  // sh < 64 here
+  r.lo = sh >= 0 ? shl_c(m, (unsigned)sh) : shr_c(m, (unsigned)(-sh));
+  r.hi = shr_c(m, (unsigned)(64 - sh));
+  return r;
+}
+
 struct Moments {
   U128 s[11];
 };
@@ -203,8 +234,8 @@ __device__ __forceinline__ void moments_add_point(Moments& M, float4 p, double s
     M.s[8] = u128_add(M.s[8], fx_f(p.z));
   }
   double dt = st - ts0;
-  M.s[9] = u128_add(M.s[9], fx_d(dt));
-  M.s[10] = u128_add(M.s[10], fx_d(dt * dt));
+  M.s[9] = u128_add(M.s[9], fx_d_nonneg(dt));
+  M.s[10] = u128_add(M.s[10], fx_d_nonneg(dt * dt));
 }
 
 // ---------------------------------------------------------------------------

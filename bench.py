@@ -52,7 +52,7 @@ MAP_EVERY = 5
 # DRAM bytes per point of a forest build pass: dram__bytes_read.sum + dram__bytes_write.sum
 # over all kernels of one ncu-captured pass of the trace's first 80 scans (bench.py
 # --forest-only); a step's build traffic scales with its points.  None: not captured.
-BUILD_TRAFFIC_PER_POINT = 931.0
+BUILD_TRAFFIC_PER_POINT = 939.0
 
 
 def pose_err(A, B):

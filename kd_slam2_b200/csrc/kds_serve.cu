@@ -219,6 +219,8 @@ struct kds_server {
   int device = 0;
   cudaStream_t sA = nullptr, sB = nullptr;  // Gauss-Newton (high priority), builds
   cudaStream_t sB2 = nullptr;               // the second build thread's stream
+  cudaStream_t sA2 = nullptr;               // a tick's ICP launches, beside the CT ones on sA
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::thread th_build, th_build2, th_gn;
   int thread_error = KDS_OK;
   char thread_error_text[256] = {0};
@@ -823,12 +825,27 @@ void gn_loop(kds_server* s) {
       }
       if (!rc && !active_cur.empty()) {
         if (s->P.profile) cudaEventRecord(s->ev_lin[buf][0], A);
+        // the two kinds touch disjoint jobs: with both present, the ICP iterations run on a
+        // second stream beside the CT ones (the profiling pass keeps them in one stream, so
+        // its events time the launches alone)
+        const bool fork = !s->P.profile && np0 > 0 && np1 > 0;
+        cudaStream_t A0 = fork ? s->sA2 : A;
+        if (fork) {
+          e = cudaEventRecord(s->ev_fork, A);
+          if (e == cudaSuccess) e = cudaStreamWaitEvent(A0, s->ev_fork, 0);
+          if (e != cudaSuccess) rc = cuda_status(e, "served tick fork", __FILE__, __LINE__);
+        }
         for (int it = 0; it < s->P.iters_per_tick && !rc; ++it) {
           rc = launch_linearize_pairs(0, np0, s->d_jobs, s->d_states, s->d_outs, s->d_lins, s->d_tiles[0],
-                                      s->d_pairs[0], s->d_partials[0], A);
+                                      s->d_pairs[0], s->d_partials[0], A0);
           if (!rc)
             rc = launch_linearize_pairs(1, np1, s->d_jobs, s->d_states, s->d_outs, s->d_lins, s->d_tiles[1],
                                         s->d_pairs[1], s->d_partials[1], A);
+        }
+        if (fork && !rc) {
+          e = cudaEventRecord(s->ev_join, A0);
+          if (e == cudaSuccess) e = cudaStreamWaitEvent(A, s->ev_join, 0);
+          if (e != cudaSuccess) rc = cuda_status(e, "served tick join", __FILE__, __LINE__);
         }
         if (s->P.profile) cudaEventRecord(s->ev_lin[buf][1], A);
         int nslots = 0;
@@ -1077,6 +1094,9 @@ int kds_server_create(const kds_server_params* params, kds_server** out) {
   int lo = 0, hi = 0;
   KDS_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
   KDS_CK(cudaStreamCreateWithPriority(&s->sA, cudaStreamNonBlocking, hi));
+  KDS_CK(cudaStreamCreateWithPriority(&s->sA2, cudaStreamNonBlocking, hi));
+  KDS_CK(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+  KDS_CK(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
   // both build streams at the lowest priority: a build stream above the other made the
   // two passes preempt each other's blocks (two overlapped passes took 35-55 ms instead of
   // 8-13 ms in some steps)
@@ -1371,7 +1391,11 @@ void kds_server_free(kds_server* s) {
     if (s->ev_lin[k][0]) cudaEventDestroy(s->ev_lin[k][0]);
     if (s->ev_lin[k][1]) cudaEventDestroy(s->ev_lin[k][1]);
   }
+  cudaStreamSynchronize(s->sA2);
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->ev_join) cudaEventDestroy(s->ev_join);
   cudaStreamDestroy(s->sA);
+  cudaStreamDestroy(s->sA2);
   cudaStreamDestroy(s->sB);
   cudaStreamDestroy(s->sB2);
   cudaGetLastError();

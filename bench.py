@@ -821,9 +821,11 @@ def tracker_streams(num_streams: int = 32, frames: int = 8):
             poses.append([r["pose_in_world"] for r in rs])
         return poses, ms
 
-    batched()  # warm-up (graph capture, pools)
+    for _ in range(3):  # warm-up (graph capture, pools, clocks)
+        batched()
     l0 = kds.lib().kds_launch_count()
-    pb, mb = batched()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        pb, mb = batched()
     l1 = kds.lib().kds_launch_count()
     ps, msq = one_at_a_time()
     l2 = kds.lib().kds_launch_count()
@@ -835,6 +837,8 @@ def tracker_streams(num_streams: int = 32, frames: int = 8):
             "batched_frames_per_s": fb, "batched_ms_per_step": float(np.mean(mb[1:])),
             "one_at_a_time_frames_per_s": fs, "one_at_a_time_ms_per_step": float(np.mean(msq[1:])),
             "speedup": fb / fs, "identical_poses": bool(same),
+            "batched_ms_all": [float(x) for x in mb], "one_at_a_time_ms_all": [float(x) for x in msq],
+            "batched_clocks": clk.summary(),
             "gpu_launches": {"batched": int(l1 - l0), "one_at_a_time": int(l2 - l1)},
             "note": "host-timed steps (one frame of every stream), first step excluded"}
 

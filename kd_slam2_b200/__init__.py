@@ -80,7 +80,8 @@ class Tree:
         return self._h
 
     def __del__(self):
-        self.free()
+        if _lib is not None:  # None once the interpreter tears the module down
+            self.free()
 
     def free(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -269,7 +270,7 @@ class _AlignerBase:
             _check(_lib.kds_aligner_set_params(self._h, C.byref(self.params)), "kds_aligner_set_params")
 
     def __del__(self):
-        if getattr(self, "_h", None) is not None and self._h.value:
+        if _lib is not None and getattr(self, "_h", None) is not None and self._h.value:
             _lib.kds_aligner_free(self._h)
             self._h = C.c_void_p(None)
 
@@ -491,7 +492,8 @@ class Tracker3D:
         self._h = h
 
     def __del__(self):
-        self.free()
+        if _lib is not None:  # None once the interpreter tears the module down
+            self.free()
 
     def free(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -584,7 +586,7 @@ class Batch:
         self._h = h
 
     def __del__(self):
-        if getattr(self, "_h", None) is not None and self._h.value:
+        if _lib is not None and getattr(self, "_h", None) is not None and self._h.value:
             _lib.kds_batch_free(self._h)
             self._h = C.c_void_p(None)
 
@@ -654,7 +656,8 @@ class Server:
         self._keep = []
 
     def __del__(self):
-        self.free()
+        if _lib is not None:  # None once the interpreter tears the module down
+            self.free()
 
     def free(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:

@@ -688,6 +688,43 @@ __global__ void k_decide(BNode* nodes, const LevelState* ls, const U128* mom, Bu
   }
 }
 
+// The level's split count from k_decide's per-block counts, then the next level (one
+// whole block).
+__device__ void level_advance_block(LevelState* ls, const int32_t* bsum, int nblocks, int32_t* level_begin) {
+  __shared__ int sm[32];
+  int v = 0;
+  for (int k = threadIdx.x; k < nblocks; k += blockDim.x) v += bsum[k];
+  int total;
+  block_scan(v, sm, &total);
+  if (threadIdx.x != 0 || ls->lb >= ls->le) return;
+  ls->lb = ls->le;
+  ls->le = ls->le + 2 * total;
+  ls->cur ^= 1;
+  ls->depth += 1;
+  if (ls->depth < kMaxDepth + 1) level_begin[ls->depth] = ls->lb;
+  ls->max_size = ls->max_next;
+  ls->max_next = 0;
+}
+
+// The last block of the level's last kernel advances the level (done: a counter that
+// starts at 0 and is left at 0; nullptr: not the last kernel).  Every block of the
+// calling kernel must reach this.
+__device__ __forceinline__ void advance_if_last(LevelState* ls, const int32_t* bsum, int nblocks,
+                                                int32_t* level_begin, unsigned* done) {
+  if (!done) return;
+  __shared__ int s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(done, 1u) == gridDim.x - 1 ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  level_advance_block(ls, bsum, nblocks, level_begin);
+  if (threadIdx.x == 0) *done = 0u;
+}
+
 // The first 18 words of a BNode (start .. dir): one coalesced load by lanes 0-17.
 constexpr int kNodeHeadWords = 18;
 static_assert(offsetof(BNode, dir) + 3 * sizeof(float) == kNodeHeadWords * 4, "BNode head layout");
@@ -701,7 +738,8 @@ static_assert(offsetof(BNode, start) == 0 && offsetof(BNode, end) == 4 && offset
 // Latency-bound at deep levels (many small nodes per warp), so each node's record
 // and sums are fetched in one round of loads, one node ahead.
 __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelState* ls, PointBufs B,
-                                                         const double* ts0, U128* mom) {
+                                                         const double* ts0, U128* mom, const int32_t* bsum,
+                                                         int nblocks, int32_t* level_begin, unsigned* done) {
   const int lb = ls->lb, le = ls->le, cur = ls->cur;
   const float4* pin = B.p[cur];
   const double* sts = B.st;
@@ -812,6 +850,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_small_part(BNode* nodes, LevelS
     }
   }
   if (lane == 0 && maxc > 0) atomicMax(&ls->max_next, maxc);
+  advance_if_last(ls, bsum, nblocks, level_begin, done);
 }
 
 // ---- large nodes ------------------------------------------------------------------
@@ -1083,8 +1122,8 @@ __global__ void __launch_bounds__(kThreads) k_big_scatter(const Chunk* chunks, c
 }
 
 // Children's sums of the large split nodes: the smaller from accl, the other = parent - it.
-__global__ void k_big_childmom(const BNode* nodes, const LevelState* ls, const int32_t* big_list, const U128* accl,
-                               U128* mom) {
+__global__ void k_big_childmom(const BNode* nodes, LevelState* ls, const int32_t* big_list, const U128* accl,
+                               U128* mom, const int32_t* bsum, int nblocks, int32_t* level_begin, unsigned* done) {
   const int nb = ls->num_big;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb * 11; t += gridDim.x * blockDim.x) {
     const int b = t / 11, k = t % 11;
@@ -1096,6 +1135,7 @@ __global__ void k_big_childmom(const BNode* nodes, const LevelState* ls, const i
     mom[(size_t)nodes[i].left * 11 + k] = small_left ? q : other;
     mom[(size_t)nodes[i].right * 11 + k] = small_left ? other : q;
   }
+  advance_if_last(ls, bsum, nblocks, level_begin, done);
 }
 
 // ---- children ------------------------------------------------------------------------
@@ -1148,23 +1188,6 @@ __global__ void k_level_children(BNode* nodes, LevelState* ls, const int32_t* bs
       }
     }
   }
-}
-
-// One block: the level's split count from the per-block counts, then the next level.
-__global__ void k_level_advance(LevelState* ls, const int32_t* bsum, int nblocks, int32_t* level_begin) {
-  __shared__ int sm[32];
-  int v = 0;
-  for (int k = threadIdx.x; k < nblocks; k += blockDim.x) v += bsum[k];
-  int total;
-  block_scan(v, sm, &total);
-  if (threadIdx.x != 0 || ls->lb >= ls->le) return;
-  ls->lb = ls->le;
-  ls->le = ls->le + 2 * total;
-  ls->cur ^= 1;
-  ls->depth += 1;
-  if (ls->depth < kMaxDepth + 1) level_begin[ls->depth] = ls->lb;
-  ls->max_size = ls->max_next;
-  ls->max_next = 0;
 }
 
 // ---- deep levels: whole subtrees in shared memory --------------------------------------
@@ -1639,6 +1662,7 @@ struct BuildWs {
   int64_t* off;
   LevelState* ls;
   int32_t* level_begin;
+  unsigned* done;  // last-block counter of the level's last kernel
   int32_t* bsum;
   int32_t* bbig;  // per-block (chunks, large nodes) of the level
   int32_t *cnt, *lcnt, *ucnt, *gp, *lgp, *to, *lto, *tot_nodes, *tot_leaves, *scan_tot;
@@ -1658,7 +1682,8 @@ size_t ws_bytes(int64_t n, int R) {
          carve_size<Chunk>(chunk_cap) + 4 * carve_size<int32_t>(chunk_cap) +
          2 * carve_size<U128>((size_t)11 * (n / kBig + 2)) + carve_size<U128>((size_t)11 * cn) + 2 * carve_size<double>(R) +
          carve_size<double>((size_t)kRootFrame * R) + carve_size<int64_t>(R + 1) +
-         carve_size<LevelState>(1) + carve_size<int32_t>(kMaxDepth + 2) + carve_size<int32_t>(kLevelBlocks) +
+         carve_size<LevelState>(1) + carve_size<int32_t>(kMaxDepth + 2) + carve_size<unsigned>(1) +
+         carve_size<int32_t>(kLevelBlocks) +
          carve_size<int32_t>(2 * kLevelBlocks) +
          7 * carve_size<int32_t>(G) + 3 * carve_size<int32_t>(R) + carve_size<int32_t>(8) + carve_size<TreeDev>(R) +
          256;
@@ -1703,6 +1728,7 @@ int ws_alloc(BuildWs& w, int64_t n, int R, cudaStream_t s) {
   w.off = carve<int64_t>(p, R + 1);
   w.ls = carve<LevelState>(p, 1);
   w.level_begin = carve<int32_t>(p, kMaxDepth + 2);
+  w.done = carve<unsigned>(p, 1);
   w.bsum = carve<int32_t>(p, kLevelBlocks);
   w.bbig = carve<int32_t>(p, 2 * kLevelBlocks);
   w.cnt = carve<int32_t>(p, G);
@@ -1873,6 +1899,7 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
     }
   }
   KDS_CK(cudaMemsetAsync(w.ls, 0, sizeof(LevelState), s));
+  KDS_CK(cudaMemsetAsync(w.done, 0, sizeof(unsigned), s));
   KDS_CK(cudaMemcpyAsync(w.off, off.data(), sizeof(int64_t) * (R + 1), cudaMemcpyHostToDevice, s));
   k_ingest<<<nblk(N, kThreads), kThreads, 0, s>>>(d_xyz, d_st, N, w.B.p[0], w.B.st, w.ls);
   count_launch();
@@ -1900,7 +1927,7 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
   const int cb = std::min<int>(w.chunk_cap, kGridBlocks * 2);
   // Grids of the level kernels sized to the level: a level has at most twice the nodes
   // of the one before, and the host learns the current level's size at each sync.  The
-  // node-range kernels (k_decide, k_level_children, k_big_plan, k_level_advance) share
+  // node-range kernels (k_decide, k_level_children, k_big_plan) share
   // one block count per level; every kernel's result is independent of its grid.
   int64_t level_nodes = R;
   int32_t global_levels = -1;  // levels built level by level; -1: no shared-memory pass
@@ -1947,9 +1974,11 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
       }
       k_decide<<<lvl_blocks, kThreads, 0, s>>>(w.nodes, w.ls, w.mom, P, w.bsum, w.bbig, w.root_frame);
       k_level_children<<<lvl_blocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bsum, (int32_t)w.cap_nodes);
-      k_small_part<<<small_blocks, kThreads, 0, s>>>(w.nodes, w.ls, w.B, w.ts0, w.mom);
+      const bool big = host_max > kBig;  // the large-node kernels run after the partition
+      k_small_part<<<small_blocks, kThreads, 0, s>>>(w.nodes, w.ls, w.B, w.ts0, w.mom, w.bsum, lvl_blocks,
+                                                     w.level_begin, big ? nullptr : w.done);
       for (int c = 0; c < 3; ++c) count_launch();
-      if (host_max > kBig) {
+      if (big) {
         if (!level0) {  // k_decide counted the large nodes per block
           k_big_plan<<<lvl_blocks, kThreads, 0, s>>>(w.nodes, w.ls, w.bbig, w.chunks, w.chunk_cap, w.big_list,
                                                      w.node_chunk0, w.acc, w.accl);
@@ -1959,11 +1988,10 @@ int tree_build_forest(const float* xyz, const double* stamps, const int64_t* off
         k_big_offsets<<<kGridBlocks, kThreads, 0, s>>>(w.nodes, w.ls, w.big_list, w.node_chunk0, w.chunk_nl,
                                                        w.chunk_loff);
         k_big_scatter<<<cb, kThreads, 0, s>>>(w.chunks, w.ls, w.nodes, w.B, w.chunk_loff, w.ts0, w.accl);
-        k_big_childmom<<<64, 256, 0, s>>>(w.nodes, w.ls, w.big_list, w.accl, w.mom);
+        k_big_childmom<<<64, 256, 0, s>>>(w.nodes, w.ls, w.big_list, w.accl, w.mom, w.bsum, lvl_blocks,
+                                          w.level_begin, w.done);
         for (int c = 0; c < 5; ++c) count_launch();
       }
-      k_level_advance<<<1, kThreads, 0, s>>>(w.ls, w.bsum, lvl_blocks, w.level_begin);
-      count_launch();
     }
     KDS_CK(cudaGetLastError());
     KDS_CK(cudaMemcpyAsync(&hls, w.ls, sizeof(LevelState), cudaMemcpyDeviceToHost, s));
